@@ -1,0 +1,376 @@
+"""Benchmark: edges traversed per second and ms to a maximal matching on B200.
+
+Workload (default): weighted maximal greedy matching (reference type 9) of an
+R-MAT power-law graph with 2^23 vertices, edge factor 16,
+(a, b, c, d) = (0.57, 0.19, 0.19, 0.05), symmetrised, self-loops and
+duplicates removed, FP32 weights in (0, 1], graph seed 1, colouring seeds from
+srand(12345) as the reference CLI draws them (bin/match.cpp:382), select
+barrier 0x88B81733 (bin/match.cpp:183).
+
+One step = one matching of the whole graph to maximality.
+
+  value     edges traversed / s with the graph resident in HBM (the round loop
+            only: the reference's t1 -> t2 "match time", bin/match.cpp:436-437).
+            Edges traversed = adjacency entries the reference's request and
+            respond loops inspect, summed over rounds (the same count the TBB
+            matcher does), measured by an instrumented run.
+  e2e       the same metric end to end through the C ABI with host buffers:
+            upload + validation + preparation + matching + download + free per
+            step (the reference's t0 -> t3 "total time").
+  roofline  the dominant kernel (phase A: blue scan + proposal) timed per
+            launch with CUDA events in a host-stepped run of the same kernels;
+            achieved = its algorithmic bytes / its duration, against the
+            measured HBM copy bandwidth.
+  cpu_baseline  the reference's own GraphMatchingTBBWeighted (same algorithm,
+            src/matchtbb.cu:567-623) compiled from its sources into
+            oracle/_ref, on all host cores, on the same graph and seeds; its
+            match[] is also compared with the GPU result ("parity").
+
+--impl reference runs only that CPU matcher, on the same metric.
+Multi-GPU (torchrun): every rank matches its own replica of the graph
+(replicas only: one graph does not shard); value is the sum over ranks divided
+by the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+from __graft_entry__ import load_package  # noqa: E402
+
+METRIC = "edges traversed/s and ms to maximal matching, 1 B200, plain vs learned/batched"
+BARRIER = 0x88B81733
+MATCH_SEED = 12345
+
+WORKLOADS = {
+    "rmat23_weighted_maximal": dict(kind="rmat", scale=23, ef=16, seed=1, type=9),
+    "rgg20_weighted_maximal": dict(kind="rgg", n=1 << 20, deg=13.0, seed=7, type=9),
+    "grid512_random_maximal": dict(kind="grid", w=512, h=512, type=7),
+    "rmat20_weighted_maximal": dict(kind="rmat", scale=20, ef=16, seed=1, type=9),
+}
+
+
+def make_graph(mm, spec):
+    if spec["kind"] == "rmat":
+        return mm.Graph.rmat(spec["scale"], spec["ef"], 0.57, 0.19, 0.19, seed=spec["seed"])
+    if spec["kind"] == "rgg":
+        return mm.Graph.rgg(spec["n"], spec["deg"], seed=spec["seed"])
+    if spec["kind"] == "grid":
+        return mm.Graph.grid(spec["w"], spec["h"])
+    raise KeyError(spec["kind"])
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args, spec, workload):
+    """--impl reference: the reference's own CPU matcher on this machine's cores."""
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    mm = load_package()
+    import oracle  # the CPU baseline leg is the one place bench.py runs oracle/
+
+    g = make_graph(mm, spec)
+    t = spec["type"]
+    ref_type = {6: 10, 7: 10, 8: 11, 9: 11}[t]
+    fixed = t in (6, 8)
+    cores = os.cpu_count() or 1
+    seeds = oracle.rand_seeds(MATCH_SEED, 256)
+    kind = "reference" if oracle.ref_available() else "port"
+    times, edges = [], None
+    _, _, ost = oracle.match(g, t, seeds, BARRIER, nthreads=cores)
+    edges = float(ost[:, oracle.ST_REQ_ENTRIES].sum() + ost[:, oracle.ST_RESP_ENTRIES].sum())
+    for i in range(args.warmup + args.steps):
+        if kind == "reference":
+            _, ms, _ = oracle.ref_run(g, ref_type, BARRIER, MATCH_SEED, nthreads=cores, fixed_rounds=fixed)
+        else:
+            t0 = time.perf_counter()
+            oracle.match(g, t, seeds, BARRIER, nthreads=cores)
+            ms = (time.perf_counter() - t0) * 1e3
+        if i >= args.warmup:
+            times.append(ms)
+    ms = statistics.mean(times)
+    value = edges / (ms / 1e3)
+    sample = f"full {workload} graph, one maximal matching per step"
+    line = {"metric": METRIC, "value": value, "unit": "edges/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+int32", "data": "synthetic",
+            "config": {"workload": workload, "n": g.n, "nnz": g.nnz, "type": t, "barrier": BARRIER,
+                       "srand": MATCH_SEED, "parallelism": "host cores", "l2": "n/a (CPU)"},
+            "cpu_baseline": {"value": value, "unit": "edges/s", "cores": cores, "kind": kind, "sample": sample,
+                             "matcher": f"GraphMatchingTBB{'Weighted' if ref_type == 11 else 'Random'}"
+                                        f"{' (20-round cap)' if fixed else ''}"},
+            "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_baseline(mm, g, t, gpu_match, workload):
+    """Reference TBB matcher on all host cores + parity of the GPU result (rank 0, N=1 only)."""
+    import oracle  # the CPU baseline leg is the one place bench.py runs oracle/
+
+    cores = os.cpu_count() or 1
+    ref_type = {6: 10, 7: 10, 8: 11, 9: 11}[t]
+    fixed = t in (6, 8)
+    if oracle.ref_available():
+        kind = "reference"
+        ref_m, ms, _ = oracle.ref_run(g, ref_type, BARRIER, MATCH_SEED, nthreads=cores, fixed_rounds=fixed)
+    else:
+        kind = "port"
+        seeds = oracle.rand_seeds(MATCH_SEED, 256)
+        t0 = time.perf_counter()
+        ref_m, _, _ = oracle.match(g, t, seeds, BARRIER, nthreads=cores)
+        ms = (time.perf_counter() - t0) * 1e3
+    # sequential weighted greedy (type 4) on one core: the reference's quality yardstick
+    seq = None
+    if oracle.ref_available() and t in (8, 9):
+        seq_m, seq_ms, _ = oracle.ref_run(g, 4, BARRIER, MATCH_SEED, nthreads=1)
+        w_seq, s_seq = oracle.weight(g, seq_m)
+        seq = {"type": 4, "ms": seq_ms, "weight": w_seq, "size": s_seq}
+    parity = bool(np.array_equal(ref_m, gpu_match))
+    chk = oracle.check(g, gpu_match)
+    w_gpu, s_gpu = oracle.weight(g, gpu_match)
+    return {"kind": kind, "cores": cores, "ms": ms,
+            "sample": f"full {workload} graph, one matching", "parity": parity,
+            "valid": chk["valid"], "maximal": chk["matchable"] == 0,
+            "gpu_weight": w_gpu, "gpu_size": s_gpu, "sequential": seq}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="rmat23_weighted_maximal", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    spec = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference(args, spec, args.workload)
+
+    world, rank, local = dist_setup()
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    mm = load_package()
+    t = spec["type"]
+    weighted = t in (8, 9)
+    g = make_graph(mm, spec)
+    seeds = mm.rand_seeds(MATCH_SEED, 255)
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+
+    dg = mm.DeviceGraph(g, device=local)
+    dg.prepare(t)
+    out = torch.empty(g.n, dtype=torch.int32, device="cuda")
+    # instrumented run: rounds and the work each round does
+    rounds, st = dg.stats(t, seeds, out.data_ptr(), stream=sptr)
+    work = mm.roofline_bytes(st, weighted)
+    edges = work["edges"]
+
+    # L2 is 126 MB; the CSR alone is > 1 GB, and a 512 MB write flushes L2 between steps.
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        dg.match_device(t, seeds, out.data_ptr(), stream=sptr)
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        with torch.cuda.stream(stream):
+            for i in range(args.steps):
+                flush.fill_(i & 0xFF)
+                evs[i][0].record(stream)
+                r = dg.match_device(t, seeds, out.data_ptr(), stream=sptr)
+                evs[i][1].record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    ms = statistics.mean(step_ms)
+    if dist:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = edges * world / (ms / 1e3)
+    gpu_launches = args.steps * (2 + 2 * (rounds if t in (7, 9) else 20))
+
+    # dominant kernel, timed per launch (host-stepped run of the same kernels)
+    prof_a, prof_b = [], []
+    for _ in range(3):
+        flush.fill_(1)
+        pr, ms_a, ms_b, _ = dg.profile(t, seeds, out.data_ptr(), stream=sptr)
+        prof_a.append(ms_a)
+        prof_b.append(ms_b)
+    ms_a = np.mean(np.stack(prof_a), axis=0)
+    ms_b = np.mean(np.stack(prof_b), axis=0)
+    ew = 8 if weighted else 4
+    nr = len(ms_a)
+    bytes_a = (ew * st[:nr, mm.ST_BLUE_DEG] + 28 * st[:nr, mm.ST_BLUE]).astype(np.float64)
+    achieved_a = bytes_a.sum() / (ms_a.sum() / 1e3) / 1e9
+    peak, peak_kind = load_peaks()
+    traffic = None
+    tfile = ROOT / "profiles" / f"traffic_{args.workload}.json"
+    if tfile.exists():
+        traffic = json.loads(tfile.read_text()).get("phase_a_bytes_per_launch")
+
+    # end to end through the C ABI with host buffers (pinned)
+    ranges_h = torch.from_numpy(np.ascontiguousarray(g.ranges, dtype=np.int32)).pin_memory()
+    nbrs_h = torch.from_numpy(g.nbrs).pin_memory()
+    w_h = torch.from_numpy(g.weights).pin_memory() if weighted else None
+    match_h = torch.empty(g.n, dtype=torch.int32).pin_memory()
+    lib = mm.lib()
+    import ctypes
+
+    e2e_ms = []
+    for i in range(args.e2e_steps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        h = ctypes.c_void_p()
+        mm._check(lib.mm_graph_create(g.n, ranges_h.data_ptr(), g.nnz, nbrs_h.data_ptr(),
+                                      None if w_h is None else w_h.data_ptr(), local, ctypes.byref(h)))
+        rr = ctypes.c_int()
+        sd = np.ascontiguousarray(seeds)
+        mm._check(lib.mm_match(h, t, BARRIER, sd.ctypes.data, len(sd), match_h.data_ptr(), ctypes.byref(rr), None))
+        lib.mm_graph_destroy(h)
+        dt = (time.perf_counter() - t0) * 1e3
+        if i > 0:
+            e2e_ms.append(dt)
+    e2e = statistics.mean(e2e_ms)
+    h2d = g.n * 8 + g.nnz * 4 + (g.nnz * 4 if weighted else 0) + 255 * 4
+    d2h = g.n * 4
+    e2e_value = edges * world / (e2e / 1e3)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        gpu_m = torch.empty(g.n, dtype=torch.int32, device="cuda")
+        dg.match_device(t, seeds, gpu_m.data_ptr(), stream=sptr)
+        torch.cuda.synchronize()
+        cpu = cpu_baseline(mm, g, t, gpu_m.cpu().numpy(), args.workload)
+    dg.close()
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "edges/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+int32", "data": "synthetic",
+            "config": {"workload": args.workload, "n": g.n, "nnz": g.nnz, "type": t, "barrier": BARRIER,
+                       "srand": MATCH_SEED, "rounds": rounds, "parallelism": f"replicas x{world}",
+                       "l2": "inputs > L2 (CSR > 1 GB) and a 512 MB L2 flush between steps"},
+            "ms_to_maximal": ms, "edges_per_step": edges,
+            "e2e": {"value": e2e_value, "unit": "edges/s", "ms_per_step": e2e, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "kernel": "k_phase_a (blue scan + proposal)",
+                         "achieved": achieved_a, "peak": peak, "unit": "GB/s", "frac": achieved_a / peak,
+                         "traffic": traffic, "peak_kind": peak_kind,
+                         "bytes_per_launch": float(bytes_a.mean()), "launches": int(nr),
+                         "ms_phase_a": float(ms_a.sum()), "ms_phase_b": float(ms_b.sum()),
+                         "reference_formula_gbs": work["reference_bytes"] / (ms / 1e3) / 1e9},
+            "gpu_launches": gpu_launches,
+            "clocks": clocks.summary(),
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = {"value": edges / (cpu["ms"] / 1e3), "unit": "edges/s", "cores": cpu["cores"],
+                                    "kind": cpu["kind"], "sample": cpu["sample"], "ms": cpu["ms"]}
+            line["parity"] = {"bit_exact_vs_reference": cpu["parity"], "valid": cpu["valid"],
+                              "maximal": cpu["maximal"], "weight": cpu["gpu_weight"], "size": cpu["gpu_size"],
+                              "sequential_greedy": cpu["sequential"]}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

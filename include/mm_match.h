@@ -1,0 +1,166 @@
+/*
+ * mm_match.h -- C ABI of the B200 greedy graph matching library (libmmatch.so).
+ *
+ * The reference (Multicore-Matching) exposes its GPU matcher only as C++
+ * classes (src/matchgpu.h:29-84).  This header is the plain-C boundary those
+ * classes sit on here (include/mtc/matchgpu.h implements them over it), and
+ * what an FFI (ctypes, cgo, JNI, N-API) binds.  No CUDA or C++ types appear
+ * in the signatures: graphs are plain arrays, streams are opaque pointers.
+ *
+ * Graph layout (the reference's mtc::Graph CSR, src/graph.h:41-60):
+ *   ranges[2*v], ranges[2*v+1]  begin / end of vertex v's neighbour list
+ *                               (std::vector<int2> neighbourRanges); lists
+ *                               need not be contiguous, sorted or disjoint;
+ *                               an empty or reversed range means degree 0
+ *   neighbours[j]               neighbour id, 0 <= id < n, for j in a range
+ *   weights[j]                  float edge weight (NULL: unit weights)
+ *
+ * Match encoding (src/matchgpu.cu:157-164, src/matchcpu.h:40-41): 0 blue,
+ * 1 red, 2 unmatchable, >= 4 matched with value 4 + min(v, partner).
+ *
+ * Matching types (bin/match.cpp:145-148): 6 random, 7 random maximal,
+ * 8 weighted, 9 weighted maximal.  The fixed types run exactly 20 rounds
+ * (NR_MATCH_ROUNDS, src/matchcpu.h:24); the maximal types run until a round
+ * finds no vertex left to colour, at most 255 rounds (src/matchgpu.cu:604).
+ * Round r colours with seeds[r], the value the reference draws from the host
+ * rand() at the start of that round (src/matchgpu.cu:509, 609, 707, 816).
+ *
+ * All functions are thread-compatible (one call per graph at a time) and
+ * report failures through their status; mm_last_error() gives the message of
+ * the calling thread's last failure.  Nothing aborts or traps.
+ */
+#ifndef MM_MATCH_H
+#define MM_MATCH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum mm_status {
+    MM_OK = 0,
+    MM_ERR_ARG = 1,          /* bad argument: null pointer, unknown type, n < 0 */
+    MM_ERR_GRAPH = 2,        /* CSR rejected: a range outside [0, nnz) or a neighbour id outside [0, n) */
+    MM_ERR_CUDA = 3,         /* CUDA runtime error; see mm_last_error() */
+    MM_ERR_NOMEM = 4,        /* device allocation failed */
+    MM_ERR_UNSUPPORTED = 5,  /* size beyond the library's limits */
+    MM_ERR_SEEDS = 6,        /* fewer seeds than rounds the matching needs */
+    MM_ERR_DEVICE = 7        /* a device-side step reported failure (status word) */
+} mm_status;
+
+enum {
+    MM_TYPE_RANDOM = 6,
+    MM_TYPE_RANDOM_MAXIMAL = 7,
+    MM_TYPE_WEIGHTED = 8,
+    MM_TYPE_WEIGHTED_MAXIMAL = 9
+};
+
+/* Kernel families for mm_match_ex (the default, MM_PATH_AUTO, is the push path). */
+enum {
+    MM_PATH_AUTO = 0,
+    MM_PATH_PULL = 1,  /* reference-structured select/request/respond/commit kernels */
+    MM_PATH_PUSH = 2   /* reverse-index proposals, device-resident round loop */
+};
+
+/* Number of int64 counters per round written by mm_match_stats. */
+#define MM_STATS_COLS 8
+enum {
+    MM_ST_ACTIVE = 0,     /* vertices that could still be matched at the round's colouring */
+    MM_ST_BLUE = 1,       /* of those, coloured blue */
+    MM_ST_RED = 2,        /* of those, coloured red */
+    MM_ST_REQ_ENTRIES = 3,  /* adjacency entries the reference's request loop inspects */
+    MM_ST_RESP_ENTRIES = 4, /* adjacency entries the reference's respond loop inspects */
+    MM_ST_BLUE_DEG = 5,   /* sum of degrees of blue vertices */
+    MM_ST_RED_DEG = 6,    /* sum of degrees of red vertices */
+    MM_ST_MATCHED = 7     /* vertices matched in the round */
+};
+
+typedef struct mm_graph mm_graph;
+
+/*
+ * Upload a CSR graph to `device` (-1: the current device) and validate it on
+ * the device.  Replaces the GraphMatchingGPU constructor (src/matchgpu.cu:39-66)
+ * and the weighted constructors' weight upload (src/matchgpu.cu:97-147).
+ * Host arrays are read only during the call.
+ */
+mm_status mm_graph_create(int n, const int *ranges, long long nnz, const int *neighbours,
+                          const float *weights, int device, mm_graph **out);
+
+/* Same, from arrays already in device memory of the current device (copied). */
+mm_status mm_graph_create_device(int n, const int *d_ranges, long long nnz, const int *d_neighbours,
+                                 const float *d_weights, mm_graph **out);
+
+/*
+ * Build the per-type device structures a matching type needs (the reverse
+ * proposal index of the push path) ahead of the first mm_match call, so that
+ * their cost lands in set-up rather than in the timed round loop.  Optional.
+ */
+mm_status mm_graph_prepare(mm_graph *g, int type);
+
+/* Free all device memory of g.  Replaces ~GraphMatchingGPU (src/matchgpu.cu:68-73, 117-121). */
+void mm_graph_destroy(mm_graph *g);
+
+int mm_graph_n(const mm_graph *g);
+long long mm_graph_nnz(const mm_graph *g);
+int mm_graph_weighted(const mm_graph *g);
+/* Device copies of the CSR (the reference's dneighbourRanges / dneighbours / dweights). */
+const void *mm_graph_device_ranges(const mm_graph *g);
+const int *mm_graph_device_neighbours(const mm_graph *g);
+const float *mm_graph_device_weights(const mm_graph *g);
+
+/* Round cap of a type: 20 (types 6, 8) or 255 (types 7, 9); -1 if unknown. */
+int mm_max_rounds(int type);
+
+/*
+ * Run one matching of `type` and copy match[n] to the HOST array match_out.
+ * Replaces GraphMatchingGPU*::performMatching (src/matchgpu.cu:453-851).
+ * seeds[0..nseeds) are the per-round colouring seeds; *rounds_out receives the
+ * number of rounds executed, which is the number of seeds the reference would
+ * have drawn.  stream: a cudaStream_t, or NULL for the legacy default stream.
+ * Weighted types on a graph created without weights use unit weights.
+ */
+mm_status mm_match(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds,
+                   int *match_out, int *rounds_out, void *stream);
+
+/* As mm_match, but match_out is a DEVICE array of n ints on g's device. */
+mm_status mm_match_device(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds,
+                          int nseeds, int *d_match_out, int *rounds_out, void *stream);
+
+/* As mm_match_device with an explicit kernel family (MM_PATH_*). */
+mm_status mm_match_ex(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds,
+                      int *d_match_out, int *rounds_out, int path, void *stream);
+
+/*
+ * As mm_match_ex, additionally filling stats[r * MM_STATS_COLS + c] for the
+ * first min(rounds, stats_rounds) rounds (counters of MM_ST_*).  Slower than
+ * mm_match_device; meant for instrumentation, not for timing.
+ */
+mm_status mm_match_stats(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds,
+                         int nseeds, int *d_match_out, int *rounds_out, long long *stats,
+                         int stats_rounds, int path, void *stream);
+
+/*
+ * Measurement entry: the push path's kernels launched one by one from the host
+ * with CUDA events on `stream` around each launch (it synchronises once per
+ * round, so it is slower than mm_match_device and only meant for timing the
+ * individual kernels).  ms_phase_a[r] / ms_phase_b[r] receive the durations of
+ * round r's scan/propose and commit/recolour launches for r < cap_rounds;
+ * *launches receives the number of kernels launched.  Same matching result.
+ */
+mm_status mm_match_profile(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds,
+                           int *d_match_out, int *rounds_out, float *ms_phase_a, float *ms_phase_b,
+                           int cap_rounds, int *launches, void *stream);
+
+/* Message of the calling thread's most recent failure ("" if none). */
+const char *mm_last_error(void);
+
+/* Library version string. */
+const char *mm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MM_MATCH_H */

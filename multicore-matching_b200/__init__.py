@@ -1,0 +1,323 @@
+"""B200 greedy graph matching: Python host bindings.
+
+Thin ctypes layer over the in-tree native libraries:
+
+  * ``libmmatch.so`` -- the product: sm_100a kernels behind the C ABI of
+    ``include/mm_match.h`` (GraphMatchingGPU* of the reference,
+    src/matchgpu.h:29-84, as plain C).
+  * ``libmmgen.so`` -- deterministic synthetic graphs in the reference's CSR
+    layout (``mtc::Graph``, src/graph.h:41-60).
+
+There is no CPU fallback: if ``libmmatch.so`` is missing or fails to load,
+every matching call raises.  Build with ``build.build_all()``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+
+# Match encoding (src/matchgpu.cu:157-164, src/matchcpu.h:40-41).
+BLUE, RED, DEAD = 0, 1, 2
+
+# Matching types (bin/match.cpp:145-148).
+RANDOM, RANDOM_MAXIMAL, WEIGHTED, WEIGHTED_MAXIMAL = 6, 7, 8, 9
+TYPES = (RANDOM, RANDOM_MAXIMAL, WEIGHTED, WEIGHTED_MAXIMAL)
+
+# Kernel families of mm_match_ex.
+PATH_AUTO, PATH_PULL, PATH_PUSH = 0, 1, 2
+
+# Default select barrier of the reference CLI (bin/match.cpp:183): p(blue) ~ 0.534.
+DEFAULT_BARRIER = 0x88B81733
+
+STATS_COLS = 8
+ST_ACTIVE, ST_BLUE, ST_RED, ST_REQ_ENTRIES, ST_RESP_ENTRIES, ST_BLUE_DEG, ST_RED_DEG, ST_MATCHED = range(8)
+
+STATUS = {0: "MM_OK", 1: "MM_ERR_ARG", 2: "MM_ERR_GRAPH", 3: "MM_ERR_CUDA", 4: "MM_ERR_NOMEM",
+          5: "MM_ERR_UNSUPPORTED", 6: "MM_ERR_SEEDS", 7: "MM_ERR_DEVICE"}
+
+
+class MatchError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+def max_rounds(type_: int) -> int:
+    """Round cap: NR_MATCH_ROUNDS = 20 for types 6/8, 255 for 7/9 (src/matchcpu.h:24-25)."""
+    return 20 if type_ in (RANDOM, WEIGHTED) else 255
+
+
+# --------------------------------------------------------------------------
+# library loading
+
+_LIBS: dict[str, ctypes.CDLL] = {}
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_LL = ctypes.c_longlong
+_U = ctypes.c_uint32
+
+_MM_SIGS = {
+    "mm_graph_create": (_I, [_I, _P, _LL, _P, _P, _I, ctypes.POINTER(_P)]),
+    "mm_graph_create_device": (_I, [_I, _P, _LL, _P, _P, ctypes.POINTER(_P)]),
+    "mm_graph_prepare": (_I, [_P, _I]),
+    "mm_graph_destroy": (None, [_P]),
+    "mm_graph_n": (_I, [_P]),
+    "mm_graph_nnz": (_LL, [_P]),
+    "mm_graph_weighted": (_I, [_P]),
+    "mm_graph_device_ranges": (_P, [_P]),
+    "mm_graph_device_neighbours": (_P, [_P]),
+    "mm_graph_device_weights": (_P, [_P]),
+    "mm_max_rounds": (_I, [_I]),
+    "mm_match": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P]),
+    "mm_match_device": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P]),
+    "mm_match_ex": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _I, _P]),
+    "mm_match_stats": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P, _I, _I, _P]),
+    "mm_match_profile": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P, _P, _I, ctypes.POINTER(_I), _P]),
+    "mm_last_error": (ctypes.c_char_p, []),
+    "mm_version": (ctypes.c_char_p, []),
+}
+
+_GEN_SIGS = {
+    "mmg_grid": (_P, [_I, _I]),
+    "mmg_rgg": (_P, [_I, ctypes.c_double, ctypes.c_ulonglong, _I]),
+    "mmg_rmat": (_P, [_I, _I, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_ulonglong, _I]),
+    "mmg_er": (_P, [_I, ctypes.c_double, ctypes.c_ulonglong, _I]),
+    "mmg_n": (_I, [_P]),
+    "mmg_nnz": (_LL, [_P]),
+    "mmg_ranges": (_P, [_P]),
+    "mmg_nbrs": (_P, [_P]),
+    "mmg_weights": (_P, [_P]),
+    "mmg_free": (None, [_P]),
+}
+
+
+def _load(name: str, sigs: dict) -> ctypes.CDLL:
+    if name in _LIBS:
+        return _LIBS[name]
+    path = PKG / name
+    if not path.exists():
+        raise OSError(f"{path} is not built; run multicore-matching_b200/build.py")
+    lib = ctypes.CDLL(str(path))
+    for fn, (res, args) in sigs.items():
+        f = getattr(lib, fn)
+        f.restype = res
+        f.argtypes = args
+    _LIBS[name] = lib
+    return lib
+
+
+def lib() -> ctypes.CDLL:
+    """The product library (libmmatch.so)."""
+    return _load("libmmatch.so", _MM_SIGS)
+
+
+def genlib() -> ctypes.CDLL:
+    return _load("libmmgen.so", _GEN_SIGS)
+
+
+def mm_symbols() -> list[str]:
+    """Every function include/mm_match.h declares (for the export check)."""
+    return list(_MM_SIGS)
+
+
+def _check(status: int) -> None:
+    if status != 0:
+        raise MatchError(status, lib().mm_last_error().decode(errors="replace"))
+
+
+def _ptr(a: Optional[np.ndarray]) -> Optional[int]:
+    return None if a is None else a.ctypes.data
+
+
+# --------------------------------------------------------------------------
+# host-side graphs
+
+
+@dataclass
+class Graph:
+    """CSR graph in the reference's layout: ranges[v] = (begin, end) into nbrs/weights."""
+
+    n: int
+    ranges: np.ndarray   # int32 [n, 2]
+    nbrs: np.ndarray     # int32 [nnz]
+    weights: Optional[np.ndarray] = None  # float32 [nnz] or None (unit)
+    name: str = ""
+
+    @property
+    def nnz(self) -> int:
+        return int(self.nbrs.shape[0])
+
+    def degrees(self) -> np.ndarray:
+        d = self.ranges[:, 1].astype(np.int64) - self.ranges[:, 0]
+        return np.maximum(d, 0)
+
+    def contiguous_arrays(self):
+        return (np.ascontiguousarray(self.ranges, dtype=np.int32),
+                np.ascontiguousarray(self.nbrs, dtype=np.int32),
+                None if self.weights is None else np.ascontiguousarray(self.weights, dtype=np.float32))
+
+    @staticmethod
+    def from_generated(handle: int, name: str) -> "Graph":
+        g = genlib()
+        if not handle:
+            raise ValueError(f"graph generator failed for {name}")
+        try:
+            n = g.mmg_n(handle)
+            nnz = g.mmg_nnz(handle)
+            ranges = np.ctypeslib.as_array(ctypes.cast(g.mmg_ranges(handle), ctypes.POINTER(ctypes.c_int32)),
+                                           shape=(max(n, 1) * 2,))[: 2 * n].copy().reshape(n, 2)
+            if nnz:
+                nbrs = np.ctypeslib.as_array(ctypes.cast(g.mmg_nbrs(handle), ctypes.POINTER(ctypes.c_int32)),
+                                             shape=(nnz,)).copy()
+                w = np.ctypeslib.as_array(ctypes.cast(g.mmg_weights(handle), ctypes.POINTER(ctypes.c_float)),
+                                          shape=(nnz,)).copy()
+            else:
+                nbrs = np.zeros(0, np.int32)
+                w = np.zeros(0, np.float32)
+        finally:
+            g.mmg_free(handle)
+        return Graph(n, ranges, nbrs, w, name)
+
+    @staticmethod
+    def grid(width: int, height: int) -> "Graph":
+        return Graph.from_generated(genlib().mmg_grid(width, height), f"grid{width}x{height}")
+
+    @staticmethod
+    def rgg(n: int, avg_deg: float = 13.0, seed: int = 7, unit: bool = False) -> "Graph":
+        return Graph.from_generated(genlib().mmg_rgg(n, avg_deg, seed, int(unit)), f"rgg{n}")
+
+    @staticmethod
+    def rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+             seed: int = 1, unit: bool = False) -> "Graph":
+        return Graph.from_generated(genlib().mmg_rmat(scale, edge_factor, a, b, c, seed, int(unit)),
+                                    f"rmat{scale}")
+
+    @staticmethod
+    def er(n: int, avg_deg: float = 8.0, seed: int = 1, unit: bool = False) -> "Graph":
+        return Graph.from_generated(genlib().mmg_er(n, avg_deg, seed, int(unit)), f"er{n}")
+
+
+def rand_seeds(seed: int, count: int = 255) -> np.ndarray:
+    """The host rand() values the reference draws per round after srand(seed)
+    (bin/match.cpp:382; src/matchgpu.cu:609, 816)."""
+    libc = ctypes.CDLL(None)
+    libc.srand(ctypes.c_uint(seed))
+    libc.rand.restype = ctypes.c_int
+    return np.array([libc.rand() for _ in range(count)], dtype=np.uint32)
+
+
+# --------------------------------------------------------------------------
+# device graphs
+
+
+class DeviceGraph:
+    """A graph uploaded to the GPU (mm_graph); the object the GPU matchers own."""
+
+    def __init__(self, g, device: int = -1, with_weights: bool = True):
+        ranges = np.ascontiguousarray(np.asarray(g.ranges).reshape(-1, 2), dtype=np.int32)
+        nbrs = np.ascontiguousarray(g.nbrs, dtype=np.int32)
+        w = None if (g.weights is None or not with_weights) else np.ascontiguousarray(g.weights, dtype=np.float32)
+        self._lib = lib()
+        h = ctypes.c_void_p()
+        _check(self._lib.mm_graph_create(int(g.n), _ptr(ranges), int(nbrs.shape[0]), _ptr(nbrs), _ptr(w), device,
+                                         ctypes.byref(h)))
+        self.handle = h.value
+        self.n = int(g.n)
+        self.nnz = int(nbrs.shape[0])
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self._lib.mm_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def prepare(self, type_: int) -> None:
+        _check(self._lib.mm_graph_prepare(self.handle, type_))
+
+    def match(self, type_: int, seeds: np.ndarray, barrier: int = DEFAULT_BARRIER, stream: int = 0):
+        """Host-output matching (mm_match): returns (match int32[n], rounds)."""
+        seeds = np.ascontiguousarray(seeds, dtype=np.uint32)
+        out = np.empty(max(self.n, 1), dtype=np.int32)
+        rounds = ctypes.c_int(0)
+        _check(self._lib.mm_match(self.handle, type_, barrier, _ptr(seeds), len(seeds), _ptr(out),
+                                  ctypes.byref(rounds), stream or None))
+        return out[: self.n], rounds.value
+
+    def match_device(self, type_: int, seeds: np.ndarray, d_out: int, barrier: int = DEFAULT_BARRIER,
+                     path: int = PATH_AUTO, stream: int = 0) -> int:
+        """Device-output matching into the device pointer d_out; returns rounds."""
+        seeds = np.ascontiguousarray(seeds, dtype=np.uint32)
+        rounds = ctypes.c_int(0)
+        _check(self._lib.mm_match_ex(self.handle, type_, barrier, _ptr(seeds), len(seeds), d_out,
+                                     ctypes.byref(rounds), path, stream or None))
+        return rounds.value
+
+    def stats(self, type_: int, seeds: np.ndarray, d_out: int, barrier: int = DEFAULT_BARRIER,
+              path: int = PATH_AUTO, stream: int = 0):
+        """Instrumented run: returns (rounds, int64[rounds, STATS_COLS])."""
+        seeds = np.ascontiguousarray(seeds, dtype=np.uint32)
+        rounds = ctypes.c_int(0)
+        st = np.zeros((255, STATS_COLS), dtype=np.int64)
+        _check(self._lib.mm_match_stats(self.handle, type_, barrier, _ptr(seeds), len(seeds), d_out,
+                                        ctypes.byref(rounds), _ptr(st), 255, path, stream or None))
+        return rounds.value, st[: rounds.value]
+
+
+    def profile(self, type_: int, seeds: np.ndarray, d_out: int, barrier: int = DEFAULT_BARRIER, stream: int = 0):
+        """Host-stepped run with CUDA events per launch: (rounds, ms_a[r], ms_b[r], launches)."""
+        seeds = np.ascontiguousarray(seeds, dtype=np.uint32)
+        rounds = ctypes.c_int(0)
+        launches = ctypes.c_int(0)
+        ms_a = np.zeros(255, np.float32)
+        ms_b = np.zeros(255, np.float32)
+        _check(self._lib.mm_match_profile(self.handle, type_, barrier, _ptr(seeds), len(seeds), d_out,
+                                          ctypes.byref(rounds), _ptr(ms_a), _ptr(ms_b), 255,
+                                          ctypes.byref(launches), stream or None))
+        executed = (launches.value - 2) // 2
+        return rounds.value, ms_a[:executed], ms_b[:executed], launches.value
+
+
+def roofline_bytes(stats: np.ndarray, weighted: bool) -> dict:
+    """Algorithmic work of one matching from its per-round counters.
+
+    reference_bytes: the bytes the reference's round loop must move,
+        sum_r [24 |A_r| + (4 + 4 w) E_r] with E_r the entries its request and
+        respond loops inspect (gathers of match/requests assumed L2-resident).
+    push_bytes: the bytes the push path must move: blue lists only,
+        sum_r [(4 + 4 w) blue_deg_r + 40 |blue_r| + 24 |red_r|].
+    edges: sum_r E_r (edges traversed, for TEPS).
+    """
+    ew = 8 if weighted else 4
+    act = stats[:, ST_ACTIVE].astype(np.float64)
+    e = stats[:, ST_REQ_ENTRIES].astype(np.float64) + stats[:, ST_RESP_ENTRIES]
+    blue = stats[:, ST_BLUE].astype(np.float64)
+    red = stats[:, ST_RED].astype(np.float64)
+    bdeg = stats[:, ST_BLUE_DEG].astype(np.float64)
+    return {
+        "edges": float(e.sum()),
+        "reference_bytes": float((24 * act + ew * e).sum()),
+        "push_bytes": float((ew * bdeg + 40 * blue + 24 * red).sum()),
+    }
+
+
+def version() -> str:
+    return lib().mm_version().decode()

@@ -1,0 +1,129 @@
+"""Sequential Python model of the push-path round loop (design check only).
+
+It restates, one vertex at a time, what the CUDA kernels of
+multicore-matching_b200/csrc/mm_push.cu compute: reverse proposal keys,
+blue-only scans with atomic-max proposals, commit by key comparison and the
+select of the next round fused into the commit.  tests/test_push_model.py runs
+it against the oracle on small adversarial graphs, so the reformulation is
+checked on the CPU before any kernel runs.
+"""
+from __future__ import annotations
+
+import struct
+
+import numpy as np
+
+M32 = 0xFFFFFFFF
+
+
+def weight_order(w: float) -> int:
+    u = struct.unpack("<I", struct.pack("<f", w))[0]
+    if u == 0x80000000:
+        u = 0
+    return (~u & M32) if (u & 0x80000000) else (u | 0x80000000)
+
+
+def cand_key(j: int, w: float, weighted: bool) -> int:
+    if weighted:
+        return ((weight_order(w) << 32) | (~j & M32)) if w > -1.0 else 0
+    return ~j & M32
+
+
+def reverse_keys(n, ranges, nbrs, w, weighted):
+    """revkey[(v, j)] for every adjacency slot of every owner v."""
+    rk = {}
+    for v in range(n):
+        b, e = int(ranges[v, 0]), int(ranges[v, 1])
+        for j in range(b, e):
+            t = int(nbrs[j])
+            if t == v:
+                rk[(v, j)] = 0
+                continue
+            best = 0
+            tb, te = int(ranges[t, 0]), int(ranges[t, 1])
+            for p in range(tb, te):
+                if int(nbrs[p]) == v:
+                    best = max(best, cand_key(p, float(w[p]), weighted))
+            rk[(v, j)] = best
+    return rk
+
+
+def push_match(g, type_, seeds, barrier, colour_hash):
+    n = g.n
+    ranges = np.asarray(g.ranges)
+    nbrs = np.asarray(g.nbrs)
+    w = np.ones(len(nbrs), np.float32) if g.weights is None else np.asarray(g.weights, np.float32)
+    weighted = type_ in (8, 9)
+    maximal = type_ in (7, 9)
+    cap = 255 if maximal else 20
+    rk = reverse_keys(n, ranges, nbrs, w, weighted)
+    BLUE, RED, DEAD, MATCHED = 0, 1, 2, 3
+    col = [BLUE if colour_hash(v, int(seeds[0])) < barrier else RED for v in range(n)]
+    match = [None] * n
+    active = list(range(n))
+    best = [0] * n
+    rounds = None
+    t = 0
+    while True:
+        # phase A: blue vertices scan and propose
+        req = {}
+        dead = set()
+        for v in active:
+            if col[v] != BLUE:
+                continue
+            b, e = int(ranges[v, 0]), int(ranges[v, 1])
+            alive = 0
+            key = 0
+            for j in range(b, e):
+                c = col[int(nbrs[j])]
+                alive |= c != MATCHED
+                if c == RED:
+                    key = max(key, cand_key(j, float(w[j]), weighted))
+                    if not weighted:
+                        break
+            if not alive:
+                col[v] = DEAD
+                match[v] = 2
+                dead.add(v)
+            elif key == 0:
+                req[v] = (-2, 0)
+            else:
+                j = ~key & M32
+                tgt = int(nbrs[j])
+                r = rk[(v, j)]
+                if r:
+                    best[tgt] = max(best[tgt], r)
+                req[v] = (tgt, r & M32)
+        # phase B: commit, recolour, compact
+        has_next = t + 1 < cap
+        nxt = []
+        for v in active:
+            if v in dead:
+                continue
+            if col[v] == BLUE:
+                tgt, lo = req[v]
+                if lo and (best[tgt] & M32) == lo:
+                    match[v] = 4 + min(v, tgt)
+                    col[v] = MATCHED
+                    continue
+            else:  # red
+                k = best[v]
+                if k:
+                    u = int(nbrs[~k & M32])
+                    match[v] = 4 + min(v, u)
+                    col[v] = MATCHED
+                    continue
+            nxt.append(v)
+        # colours of the next round only after every commit of this round
+        if has_next:
+            for v in nxt:
+                col[v] = BLUE if colour_hash(v, int(seeds[t + 1])) < barrier else RED
+        active = nxt
+        if not (has_next and active):
+            rounds = min(t + 2, cap) if (maximal and not active) else cap
+            break
+        t += 1
+    out = np.zeros(n, np.int32)
+    for v in range(n):
+        out[v] = match[v] if match[v] is not None else col[v]
+    return out, rounds

@@ -1,0 +1,93 @@
+"""CPU tests of the boundary and host logic: the C ABI library loads and exports
+every function include/mm_match.h declares; argument errors come back as
+statuses without touching the device; the workload generators are
+deterministic and produce the CSR shape the configurations name."""
+from __future__ import annotations
+
+import ctypes
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared_functions(header: Path) -> set[str]:
+    text = header.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return set(re.findall(r"^\s*(?:const\s+)?(?:(?:unsigned|long|signed)\s+)*\w+\s*\*?\s*(mm_\w+)\s*\(",
+                          text, flags=re.M))
+
+
+def exported(lib: Path) -> set[str]:
+    out = subprocess.run(["nm", "-D", "--defined-only", str(lib)], capture_output=True, text=True, check=True)
+    return {line.split()[-1] for line in out.stdout.splitlines() if line.strip()}
+
+
+def test_library_exports_every_declared_symbol(mm):
+    mm.lib()  # loads, or raises
+    decl = declared_functions(ROOT / "include" / "mm_match.h")
+    assert len(decl) >= 15
+    syms = exported(mm.PKG / "libmmatch.so")
+    missing = decl - syms
+    assert not missing, missing
+    # nothing but the mm_* API leaks out (static cudart is hidden)
+    assert all(s.startswith("mm_") for s in syms), sorted(s for s in syms if not s.startswith("mm_"))[:5]
+    assert set(mm.mm_symbols()) == decl
+
+
+def test_argument_errors_need_no_device(mm):
+    lib = mm.lib()
+    assert lib.mm_graph_create(4, None, 0, None, None, -1, None) == 1  # out is null
+    h = ctypes.c_void_p()
+    assert lib.mm_graph_create(-1, None, 0, None, None, -1, ctypes.byref(h)) == 1
+    assert lib.mm_graph_create(3, None, 0, None, None, -1, ctypes.byref(h)) == 1  # ranges null
+    assert lib.mm_graph_create(1, None, 1 << 31, None, None, -1, ctypes.byref(h)) in (1, 5)
+    r = ctypes.c_int()
+    assert lib.mm_match(None, 7, 0, None, 0, None, ctypes.byref(r), None) == 1
+    assert lib.mm_max_rounds(6) == 20 and lib.mm_max_rounds(8) == 20
+    assert lib.mm_max_rounds(7) == 255 and lib.mm_max_rounds(9) == 255
+    assert lib.mm_max_rounds(3) == -1
+    assert b"mm_graph_create" in lib.mm_last_error() or lib.mm_last_error() != b""
+    assert mm.version().startswith("mmatch")
+
+
+def csr_properties(g):
+    r = g.ranges
+    assert r[0, 0] == 0 and np.all(r[1:, 0] == r[:-1, 1]) and r[-1, 1] == g.nnz
+    owners = np.repeat(np.arange(g.n), g.degrees())
+    # no self loops, sorted strictly increasing within each list (no duplicates)
+    assert np.all(owners != g.nbrs)
+    same = owners[1:] == owners[:-1]
+    assert np.all(g.nbrs[1:][same] > g.nbrs[:-1][same])
+    # symmetric with equal weights both ways
+    fwd = owners.astype(np.int64) * g.n + g.nbrs
+    rev = g.nbrs.astype(np.int64) * g.n + owners
+    order_f, order_r = np.argsort(fwd), np.argsort(rev)
+    assert np.array_equal(fwd[order_f], rev[order_r])
+    assert np.array_equal(g.weights[order_f], g.weights[order_r])
+
+
+def test_generators_deterministic_and_well_formed(mm):
+    for make in (lambda: mm.Graph.grid(37, 21), lambda: mm.Graph.rgg(5000, 13.0, seed=7),
+                 lambda: mm.Graph.rmat(12, 16, seed=3), lambda: mm.Graph.er(5000, 8.0, seed=3)):
+        a, b = make(), make()
+        assert np.array_equal(a.ranges, b.ranges) and np.array_equal(a.nbrs, b.nbrs)
+        assert np.array_equal(a.weights, b.weights)
+        csr_properties(a)
+        assert a.weights.min() > 0 and a.weights.max() <= 1.0
+
+
+def test_generator_shapes(mm):
+    g = mm.Graph.grid(512, 512)
+    assert g.n == 262144 and g.nnz == 2 * (512 * 511 * 2)
+    assert np.all(g.weights == 1.0)
+    r = mm.Graph.rgg(1 << 16, 13.0, seed=7)
+    assert 12.0 < r.nnz / r.n < 13.5  # pi r^2 n = 13 minus the boundary
+    e = mm.Graph.er(1 << 14, 8.0, seed=1)
+    assert 7.5 < e.nnz / e.n <= 8.0
+    m = mm.Graph.rmat(14, 16, seed=1)
+    deg = m.degrees()
+    assert deg.max() > 50 * max(1.0, deg.mean())  # power-law skew

@@ -1,0 +1,27 @@
+"""CPU design check: the push-path reformulation equals the oracle on
+adversarial inputs (see tests/push_model.py)."""
+from __future__ import annotations
+
+import numpy as np
+
+from graphs_small import random_graph
+from push_model import push_match
+
+
+def test_push_model_equals_oracle(orc):
+    rng = np.random.default_rng(12)
+    total = 0
+    for it in range(120):
+        n = int(rng.integers(1, 40))
+        g = random_graph(rng, n, avg_deg=float(rng.uniform(0.5, 6)), symmetric=bool(rng.random() < 0.6),
+                         gaps=bool(rng.random() < 0.3), shuffle_ranges=bool(rng.random() < 0.3),
+                         empty_reversed=0.2 if rng.random() < 0.3 else 0.0, dup=0.1, loops=0.1)
+        seeds = orc.rand_seeds(int(rng.integers(1, 1000)))
+        for barrier in (0x88B81733, 0x40000000, 0, 0xFFFFFFFF):
+            for t in (6, 7, 8, 9):
+                want, rounds, _ = orc.match(g, t, seeds, barrier)
+                got, got_rounds = push_match(g, t, seeds, barrier, orc.colour_hash)
+                assert got_rounds == rounds
+                assert np.array_equal(got, want), (it, t, hex(barrier))
+                total += 1
+    assert total == 120 * 16
