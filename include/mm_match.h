@@ -153,6 +153,25 @@ mm_status mm_match_profile(mm_graph *g, int type, uint32_t barrier, const uint32
                            int *d_match_out, int *rounds_out, float *ms_phase_a, float *ms_phase_b,
                            int cap_rounds, int *launches, void *stream);
 
+/*
+ * Allocation-free matching.  No counterpart in the reference: it exists for
+ * callers that must not allocate device memory while they run -- cudaMalloc and
+ * cudaFree synchronise the whole device, which a process sharing the GPU with
+ * latency-sensitive streams cannot afford, and a caller whose device memory is
+ * reserved up front by a framework or pool is not allowed to allocate at all.
+ * The graph (d_ranges as int2 pairs, d_neighbours, d_weights or NULL for unit
+ * weights) and d_match_out are the caller's own DEVICE arrays on the current
+ * device; seeds are host values.  Same result and round count as mm_match.
+ * Scratch lives in a fixed device array inside the library: at most 1048576
+ * vertices (larger n returns MM_ERR_UNSUPPORTED), held on every GPU that loads
+ * the library until the process exits.  The first call on a device looks up
+ * that array (make it before any stream capture).  All calls share the array:
+ * calls that overlap on the GPU race.  Calls no cudaMalloc / cudaFree.
+ */
+mm_status mm_match_noalloc(int n, const int *d_ranges, long long nnz, const int *d_neighbours,
+                           const float *d_weights, int type, uint32_t barrier, const uint32_t *seeds,
+                           int nseeds, int *d_match_out, int *rounds_out, void *stream);
+
 /* Message of the calling thread's most recent failure ("" if none). */
 const char *mm_last_error(void);
 

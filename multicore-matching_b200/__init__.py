@@ -81,6 +81,7 @@ _MM_SIGS = {
     "mm_match_ex": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _I, _P]),
     "mm_match_stats": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P, _I, _I, _P]),
     "mm_match_profile": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P, _P, _I, ctypes.POINTER(_I), _P]),
+    "mm_match_noalloc": (_I, [_I, _P, _LL, _P, _P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P]),
     "mm_last_error": (ctypes.c_char_p, []),
     "mm_version": (ctypes.c_char_p, []),
 }
