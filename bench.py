@@ -224,6 +224,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="rmat23_weighted_maximal", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ncu-case", action="store_true",
+                    help="build + prepare, then one host-stepped matching only (for ncu captures of the kernels)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     spec = WORKLOADS[args.workload]
@@ -252,6 +254,16 @@ def main():
     dg = mm.DeviceGraph(g, device=local)
     dg.prepare(t)
     out = torch.empty(g.n, dtype=torch.int32, device="cuda")
+    if args.ncu_case:
+        r, ms_k, launches = dg.profile(t, seeds, out.data_ptr(), stream=sptr)
+        torch.cuda.synchronize()
+        print(json.dumps({"ncu_case": args.workload, "rounds": r, "launches": launches,
+                          "ms_short_scan": [round(float(x), 4) for x in ms_k[:-1, 0]],
+                          "ms_staged_scan": [round(float(x), 4) for x in ms_k[:-1, 1]],
+                          "ms_commit": [round(float(x), 4) for x in ms_k[:-1, 2]],
+                          "ms_tail": round(float(ms_k[-1, 3]), 4)}))
+        dg.close()
+        return 0
     # instrumented run: rounds and the work each round does
     rounds, st = dg.stats(t, seeds, out.data_ptr(), stream=sptr)
     work = mm.roofline_bytes(st, weighted)
@@ -283,26 +295,32 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
     value = edges * world / (ms / 1e3)
-    gpu_launches = args.steps * (2 + 2 * (rounds if t in (7, 9) else 20))
-
-    # dominant kernel, timed per launch (host-stepped run of the same kernels)
-    prof_a, prof_b = [], []
+    # the scan kernels, timed per launch (host-stepped run of the same kernels)
+    prof = []
     for _ in range(3):
         flush.fill_(1)
-        pr, ms_a, ms_b, _ = dg.profile(t, seeds, out.data_ptr(), stream=sptr)
-        prof_a.append(ms_a)
-        prof_b.append(ms_b)
-    ms_a = np.mean(np.stack(prof_a), axis=0)
-    ms_b = np.mean(np.stack(prof_b), axis=0)
+        _, ms_k, _ = dg.profile(t, seeds, out.data_ptr(), stream=sptr)
+        prof.append(ms_k)
+    ms_k = np.mean(np.stack(prof), axis=0)  # [grid rounds + 1, (short scan, staged scan, commit, tail)]
+    ms_tail = float(ms_k[-1, 3])
+    ms_k = ms_k[:-1]
+    nr = ms_k.shape[0]
+    gpu_launches = args.steps * (3 + 3 * nr)
     ew = 8 if weighted else 4
-    nr = len(ms_a)
-    bytes_a = (ew * st[:nr, mm.ST_BLUE_DEG] + 28 * st[:nr, mm.ST_BLUE]).astype(np.float64)
-    achieved_a = bytes_a.sum() / (ms_a.sum() / 1e3) / 1e9
+    stn = st[:nr].astype(np.float64)
+    staged_bytes = ew * stn[:, mm.ST_STAGED_DEG] + 36 * stn[:, mm.ST_STAGED_ITEMS]
+    short_bytes = (ew * (stn[:, mm.ST_BLUE_DEG] - stn[:, mm.ST_STAGED_DEG])
+                   + 36 * np.maximum(stn[:, mm.ST_BLUE] - stn[:, mm.ST_STAGED_ITEMS], 0))
+    kernels = {"k_phase_a_stream (staged long-list scan)": (staged_bytes, ms_k[:, 1]),
+               "k_phase_a_short (short-list scan)": (short_bytes, ms_k[:, 0])}
+    dom = max(kernels, key=lambda k: kernels[k][1].sum())
+    dom_bytes, dom_ms = kernels[dom]
+    achieved = dom_bytes.sum() / (dom_ms.sum() / 1e3) / 1e9
     peak, peak_kind = load_peaks()
     traffic = None
     tfile = ROOT / "profiles" / f"traffic_{args.workload}.json"
     if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get("phase_a_bytes_per_launch")
+        traffic = json.loads(tfile.read_text()).get("dominant_bytes_per_launch")
 
     # end to end through the C ABI with host buffers (pinned)
     ranges_h = torch.from_numpy(np.ascontiguousarray(g.ranges, dtype=np.int32)).pin_memory()
@@ -350,11 +368,12 @@ def main():
             "ms_to_maximal": ms, "edges_per_step": edges,
             "e2e": {"value": e2e_value, "unit": "edges/s", "ms_per_step": e2e, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
-            "roofline": {"bound": "hbm", "kernel": "k_phase_a (blue scan + proposal)",
-                         "achieved": achieved_a, "peak": peak, "unit": "GB/s", "frac": achieved_a / peak,
+            "roofline": {"bound": "hbm", "kernel": dom,
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_kind": peak_kind,
-                         "bytes_per_launch": float(bytes_a.mean()), "launches": int(nr),
-                         "ms_phase_a": float(ms_a.sum()), "ms_phase_b": float(ms_b.sum()),
+                         "bytes_per_launch": float(dom_bytes.mean()), "launches": int(nr),
+                         "ms_short_scan": float(ms_k[:, 0].sum()), "ms_staged_scan": float(ms_k[:, 1].sum()),
+                         "ms_commit": float(ms_k[:, 2].sum()), "ms_tail": ms_tail,
                          "reference_formula_gbs": work["reference_bytes"] / (ms / 1e3) / 1e9},
             "gpu_launches": gpu_launches,
             "clocks": clocks.summary(),

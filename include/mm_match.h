@@ -65,7 +65,7 @@ enum {
 };
 
 /* Number of int64 counters per round written by mm_match_stats. */
-#define MM_STATS_COLS 8
+#define MM_STATS_COLS 10
 enum {
     MM_ST_ACTIVE = 0,     /* vertices that could still be matched at the round's colouring */
     MM_ST_BLUE = 1,       /* of those, coloured blue */
@@ -74,7 +74,9 @@ enum {
     MM_ST_RESP_ENTRIES = 4, /* adjacency entries the reference's respond loop inspects */
     MM_ST_BLUE_DEG = 5,   /* sum of degrees of blue vertices */
     MM_ST_RED_DEG = 6,    /* sum of degrees of red vertices */
-    MM_ST_MATCHED = 7     /* vertices matched in the round */
+    MM_ST_MATCHED = 7,    /* vertices matched in the round */
+    MM_ST_STAGED_DEG = 8,   /* push path: entries its staged long-list scan read */
+    MM_ST_STAGED_ITEMS = 9  /* push path: lists and chunks that scan handled */
 };
 
 typedef struct mm_graph mm_graph;
@@ -145,13 +147,17 @@ mm_status mm_match_stats(mm_graph *g, int type, uint32_t barrier, const uint32_t
  * Measurement entry: the push path's kernels launched one by one from the host
  * with CUDA events on `stream` around each launch (it synchronises once per
  * round, so it is slower than mm_match_device and only meant for timing the
- * individual kernels).  ms_phase_a[r] / ms_phase_b[r] receive the durations of
- * round r's scan/propose and commit/recolour launches for r < cap_rounds;
- * *launches receives the number of kernels launched.  Same matching result.
+ * individual kernels).  ms_per_kernel[r * MM_PROFILE_KERNELS + k] receives the
+ * duration of round r's kernel k for r < cap_rounds: k = 0 short-list scan,
+ * 1 staged long-list scan, 2 commit/recolour; the row after the last such
+ * round holds in k = 3 the single-block tail kernel that runs the remaining
+ * small rounds.  *launches receives the number of kernels launched (init,
+ * 3 per grid round, tail, finish).  Same matching result.
  */
+#define MM_PROFILE_KERNELS 4
 mm_status mm_match_profile(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds,
-                           int *d_match_out, int *rounds_out, float *ms_phase_a, float *ms_phase_b,
-                           int cap_rounds, int *launches, void *stream);
+                           int *d_match_out, int *rounds_out, float *ms_per_kernel, int cap_rounds,
+                           int *launches, void *stream);
 
 /*
  * Allocation-free matching.  No counterpart in the reference: it exists for

@@ -36,8 +36,10 @@ PATH_AUTO, PATH_PULL, PATH_PUSH = 0, 1, 2
 # Default select barrier of the reference CLI (bin/match.cpp:183): p(blue) ~ 0.534.
 DEFAULT_BARRIER = 0x88B81733
 
-STATS_COLS = 8
-ST_ACTIVE, ST_BLUE, ST_RED, ST_REQ_ENTRIES, ST_RESP_ENTRIES, ST_BLUE_DEG, ST_RED_DEG, ST_MATCHED = range(8)
+STATS_COLS = 10
+PROFILE_KERNELS = 4  # short-list scan, staged long-list scan, commit/recolour, tail
+(ST_ACTIVE, ST_BLUE, ST_RED, ST_REQ_ENTRIES, ST_RESP_ENTRIES, ST_BLUE_DEG, ST_RED_DEG, ST_MATCHED,
+ ST_STAGED_DEG, ST_STAGED_ITEMS) = range(10)
 
 STATUS = {0: "MM_OK", 1: "MM_ERR_ARG", 2: "MM_ERR_GRAPH", 3: "MM_ERR_CUDA", 4: "MM_ERR_NOMEM",
           5: "MM_ERR_UNSUPPORTED", 6: "MM_ERR_SEEDS", 7: "MM_ERR_DEVICE"}
@@ -80,7 +82,7 @@ _MM_SIGS = {
     "mm_match_device": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P]),
     "mm_match_ex": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _I, _P]),
     "mm_match_stats": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P, _I, _I, _P]),
-    "mm_match_profile": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P, _P, _I, ctypes.POINTER(_I), _P]),
+    "mm_match_profile": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P, _I, ctypes.POINTER(_I), _P]),
     "mm_match_noalloc": (_I, [_I, _P, _LL, _P, _P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P]),
     "mm_last_error": (ctypes.c_char_p, []),
     "mm_version": (ctypes.c_char_p, []),
@@ -284,17 +286,20 @@ class DeviceGraph:
 
 
     def profile(self, type_: int, seeds: np.ndarray, d_out: int, barrier: int = DEFAULT_BARRIER, stream: int = 0):
-        """Host-stepped run with CUDA events per launch: (rounds, ms_a[r], ms_b[r], launches)."""
+        """Host-stepped run with CUDA events per launch.
+
+        Returns (rounds, ms[r, k], launches) with k = 0 short-list scan,
+        1 staged long-list scan, 2 commit/recolour (one row per grid round),
+        then a last row with the single-block tail kernel's time in k = 3."""
         seeds = np.ascontiguousarray(seeds, dtype=np.uint32)
         rounds = ctypes.c_int(0)
         launches = ctypes.c_int(0)
-        ms_a = np.zeros(255, np.float32)
-        ms_b = np.zeros(255, np.float32)
+        ms = np.zeros((255, PROFILE_KERNELS), np.float32)
         _check(self._lib.mm_match_profile(self.handle, type_, barrier, _ptr(seeds), len(seeds), d_out,
-                                          ctypes.byref(rounds), _ptr(ms_a), _ptr(ms_b), 255,
-                                          ctypes.byref(launches), stream or None))
-        executed = (launches.value - 2) // 2
-        return rounds.value, ms_a[:executed], ms_b[:executed], launches.value
+                                          ctypes.byref(rounds), _ptr(ms), 255, ctypes.byref(launches),
+                                          stream or None))
+        grid_rounds = (launches.value - 3) // 3
+        return rounds.value, ms[: grid_rounds + 1], launches.value
 
 
 def roofline_bytes(stats: np.ndarray, weighted: bool) -> dict:

@@ -146,11 +146,15 @@ mm_status create_common(int n, const int *ranges, long long nnz, const int *nbrs
     cudaGetDevice(&g->device);
     g->n = n;
     g->nnz = nnz;
-    const size_t nv = (size_t)(n > 0 ? n : 1), ne = (size_t)(nnz > 0 ? nnz : 1);
+    // Neighbour and weight arrays are padded to a multiple of 4 entries plus 4 so
+    // that 16-byte vector loads starting at any in-range, 4-aligned slot stay inside.
+    const size_t nv = (size_t)(n > 0 ? n : 1), ne = ((size_t)nnz + 3) / 4 * 4 + 4;
     const cudaMemcpyKind kind = from_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     cudaError_t e = cudaMalloc(&g->d_ranges, nv * sizeof(int2));
     if (e == cudaSuccess) e = cudaMalloc(&g->d_nbrs, ne * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&g->d_w, ne * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemset(g->d_nbrs + nnz, 0, (ne - (size_t)nnz) * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(g->d_w + nnz, 0, (ne - (size_t)nnz) * sizeof(float));
     if (e == cudaSuccess && n > 0) e = cudaMemcpy(g->d_ranges, ranges, (size_t)n * sizeof(int2), kind);
     if (e == cudaSuccess && nnz > 0) e = cudaMemcpy(g->d_nbrs, nbrs, (size_t)nnz * sizeof(int), kind);
     if (e == cudaSuccess && nnz > 0 && w) e = cudaMemcpy(g->d_w, w, (size_t)nnz * sizeof(float), kind);
@@ -295,14 +299,14 @@ MM_API mm_status mm_match_stats(mm_graph *g, int type, uint32_t barrier, const u
 }
 
 MM_API mm_status mm_match_profile(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds,
-                                  int *d_match_out, int *rounds_out, float *ms_phase_a, float *ms_phase_b,
-                                  int cap_rounds, int *launches, void *stream)
+                                  int *d_match_out, int *rounds_out, float *ms_per_kernel, int cap_rounds,
+                                  int *launches, void *stream)
 {
     mm_status s = check_match_args(g, type, seeds, nseeds, d_match_out, rounds_out);
     if (s != MM_OK) return s;
     DeviceGuard guard(g->device);
-    return push_profile(g, type, barrier, seeds, nseeds, d_match_out, rounds_out, ms_phase_a, ms_phase_b,
-                        cap_rounds, launches, (cudaStream_t)stream);
+    return push_profile(g, type, barrier, seeds, nseeds, d_match_out, rounds_out, ms_per_kernel, cap_rounds, launches,
+                        (cudaStream_t)stream);
 }
 
 MM_API const char *mm_last_error(void) { return g_last_error.c_str(); }

@@ -81,6 +81,10 @@ struct mm_graph {
     float *d_w = nullptr;     // unit weights when the graph came without any
     long long max_degree = 0;
     long long sum_degree = 0;
+    bool scanned = false;          // degree classes below are valid
+    long long short_count = 0;     // vertices with at most 32 neighbour entries
+    long long long_count = 0;      // vertices with more
+    long long long_entries = 0;    // entries in those longer lists
 
     // device buffer for host-output calls (mm_match)
     int *d_out = nullptr;
@@ -119,8 +123,7 @@ mm_status push_match(mm_graph *g, int type, uint32_t barrier, const uint32_t *se
                      int *d_match, int *rounds_out, long long *stats, int stats_rounds,
                      cudaStream_t stream);
 mm_status push_profile(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds, int *d_match,
-                       int *rounds_out, float *ms_a, float *ms_b, int cap_rounds, int *launched,
-                       cudaStream_t stream);
+                       int *rounds_out, float *ms_kernels, int cap_rounds, int *launched, cudaStream_t stream);
 void push_release(mm_graph *g);
 
 inline int max_rounds_of(int type)

@@ -13,28 +13,44 @@
 //     restricted to entries pointing at proposers.  For every adjacency slot
 //     (v -> r) the preparation step stores revkey = the best such key among
 //     r's entries pointing back at v (0 if none can ever be picked).  A blue
-//     proposer then atomicMax-es its revkey into slot_best[r]; the maximum over
+//     proposer then atomicMax-es its revkey into best[r]; the maximum over
 //     proposers equals the maximum over r's list.  Red vertices never scan.
-//   * Commit (gMatch, matchgpu.cu:260-283): red r is matched iff slot_best[r]
-//     is non-zero (its partner is neighbours[~low32(key)]); blue u is matched
-//     iff the low 32 bits of slot_best[its target] equal the low 32 bits of its
-//     own revkey (positions in r's list are unique).
+//   * Commit (gMatch, matchgpu.cu:260-283): red r is matched iff best[r] is
+//     non-zero (its partner is neighbours[~low32(key)]); blue u is matched iff
+//     the low 32 bits of best[its target] equal the low 32 bits of its own
+//     revkey (positions in r's list are unique).
 //   * Select (gaSelect, matchgpu.cu:220-258) of round t+1 is fused into the
 //     commit pass of round t: a survivor recolours itself with seed t+1.
 //   * Dead marking (requests == n+1) happens as soon as the blue scan finds no
 //     unmatched neighbour; readers of that colour byte see "unmatched, not red"
 //     either way, so their outcome is unchanged.
 //
-// Round t is two kernels: phase A (blue scan + proposal) and phase B
-// (commit + recolour + worklist compaction).  They form the body of a CUDA
-// graph WHILE node; the last block of phase B decides whether another round
-// runs (cudaGraphSetConditional), so there is no host synchronisation inside
-// the loop.  Worklists hold only vertices that can still be matched, split
-// by colour and by degree class (long lists are scanned by a whole block).
+// Work layout.  Vertices that can still be matched sit in worklists; an item
+// carries the vertex and its neighbour range, so the scans never read
+// neighbourRanges again.
+//   short lists (deg <= 32)   a warp walks the concatenated lists of 32 blue
+//                             vertices, loading entries directly
+//                             (k_phase_a_short)
+//   long lists  (deg  > 32)   blue ones are appended with their offset in the
+//                             round's concatenated long-list entry space; that
+//                             space is cut into 960-entry segments, each staged
+//                             into shared memory by bulk copies (TMA) and
+//                             scanned from there (k_phase_a_stream).  A list
+//                             cut by segment edges is combined by atomics and
+//                             its last piece proposes.  Every warp claims equal
+//                             amounts of work whatever the degree skew.
+// The two scans run concurrently.
+//
+// Round t is three kernels: the two phase-A scans (blue scan + proposal) and
+// phase B (commit + recolour + worklist compaction).  They form the body of a
+// CUDA graph WHILE node; the last block of phase B decides whether another
+// round runs (cudaGraphSetConditional), so there is no host synchronisation
+// inside the loop.
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
+#include <cstddef>
 #include <cstring>
 #include <new>
 
@@ -45,13 +61,13 @@ namespace {
 
 constexpr int kBlockA = 256;
 constexpr int kBlockB = 256;
-constexpr int kWarpsA = kBlockA / 32;
-constexpr int kLargeDegree = 1024;  // lists longer than this are scanned by a whole block
 constexpr unsigned kFull = 0xffffffffu;
+constexpr int kSmallMax = 32;       // short lists: degree <= 32
+constexpr int kSegEntries = 416;    // entries per staged segment (at most 15 pieces of lists > 32)
+constexpr int kSegCap = 512;        // slot capacity: a segment plus 16-byte alignment slack per piece
 
-// Worklists: [colour][degree class] -> index 0 blue-short, 1 blue-long,
-// 2 red-short, 3 red-long.
-constexpr int kLists = 4;
+// Worklists.  kStaged holds blue long lists with their entry offsets.
+enum : int { kBlueS = 0, kRedS, kRedLong, kStaged, kLists };
 
 struct Ctl {
     int *match;            // output array of this call
@@ -61,10 +77,15 @@ struct Ctl {
     int nseeds;
     int t;                 // 0-based index of the round being executed
     int rounds;            // rounds the reference executes (set at loop exit)
-    int status;            // 0 ok, 1 seeds exhausted
+    int status;            // 0 ok, 1 seeds exhausted, 2 a bounded device wait gave up
     int cont;              // 1 while another round follows (read by the stepped driver)
     unsigned ticket;       // phase-B block arrivals
-    int cnt[2][kLists];    // worklist lengths by round parity
+    int task_short[2];     // phase-A cursors by round parity: short-list batches
+    int task_stream[2];    //   and staged segments
+    int cnt[2][kLists];    // worklist lengths by round parity (kStaged unused)
+    unsigned long long staged_pack[2];  // kStaged: (items << 32) | entries, by parity
+    int retired[2];        // vertices of the round that were unmatchable as soon as coloured
+    int tail;              // 1: the remaining rounds run in the single-block tail kernel
 };
 
 struct Params {
@@ -77,35 +98,29 @@ struct Params {
     const long long *slot_off;
     uint8_t *col;
     int2 *req;
-    unsigned long long *best;  // per red vertex: max proposal key this round
-    int *lists;                // [2][kLists][n]
+    unsigned long long *best;       // per red vertex: max proposal key this round
+    unsigned long long *part_key;   // per cut long list: max over finished pieces
+    int *part_cnt;                  // per cut long list: finished pieces
+    int4 *lists[2][kLists];         // items {v, begin, end, offset} by parity and list id
+    int *seg_first[2];              // per staged segment: item holding its first entry
     const uint32_t *seeds;
     Ctl *ctl;
-    unsigned long long *stats; // [kMaxRounds][MM_STATS_COLS] or null
+    unsigned long long *stats;      // [kMaxRounds][MM_STATS_COLS] or null
     cudaGraphConditionalHandle loop;
 };
 
-__device__ __forceinline__ int *list_ptr(const Params &p, int parity, int which)
-{
-    return p.lists + ((size_t)parity * kLists + which) * (size_t)p.n;
-}
-
 __device__ __forceinline__ int degree_of(int2 r) { return r.y > r.x ? r.y - r.x : 0; }
+__device__ __forceinline__ int degree_of(int4 it) { return it.z > it.y ? it.z - it.y : 0; }
 
-// Append v to worklist `which` of `parity`, one atomic per warp and list.
-__device__ __forceinline__ void append(const Params &p, int parity, int which, int v, bool take)
+__device__ __forceinline__ int warp_incl_scan(int v)
 {
     const int lane = threadIdx.x & 31;
 #pragma unroll
-    for (int l = 0; l < kLists; ++l) {
-        const unsigned m = __ballot_sync(kFull, take && which == l);
-        if (!m) continue;
-        const int leader = __ffs(m) - 1;
-        int base = 0;
-        if (lane == leader) base = atomicAdd(&p.ctl->cnt[parity][l], __popc(m));
-        base = __shfl_sync(kFull, base, leader);
-        if (take && which == l) list_ptr(p, parity, l)[base + __popc(m & ((1u << lane) - 1))] = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, v, o);
+        if (lane >= o) v += y;
     }
+    return v;
 }
 
 __device__ __forceinline__ void stat_add(const Params &p, int round, int col, unsigned long long v)
@@ -117,306 +132,762 @@ __device__ __forceinline__ void stat_add(const Params &p, int round, int col, un
 
 // Key under which a blue vertex ranks a red neighbour at position j
 // (gwRequest: strict > from -1, earliest j on ties; grRequest: earliest j).
+// Every candidate key is >= 2^31, so the value 1 can stand for "an unmatched
+// neighbour that is not a candidate" and a single max-reduction carries both
+// the choice and the dead flag (0 = nothing unmatched seen).
 template <bool kW>
 __device__ __forceinline__ unsigned long long cand_key(int j, float w)
 {
-    if (kW) return w > -1.0f ? (((unsigned long long)weight_order(w) << 32) | (uint32_t)~j) : 0ull;
+    if (kW) return w > -1.0f ? (((unsigned long long)weight_order(w) << 32) | (uint32_t)~j) : 1ull;
     return (unsigned long long)(uint32_t)~j;
 }
 
-// Finish blue vertex v after its scan: dead, no proposal, or propose.
-template <bool kStats>
-__device__ __forceinline__ void propose(const Params &p, int v, int2 r, unsigned long long key, int alive,
-                                        int t, bool weighted)
+// Scan result of one adjacency entry with neighbour colour c.
+template <bool kW>
+__device__ __forceinline__ unsigned long long entry_key(uint8_t c, int j, float w)
 {
-    if (!alive) {
+    if (c == kRed) return cand_key<kW>(j, w);
+    return c == kMatched ? 0ull : 1ull;
+}
+
+// Finish blue vertex v after its scan: dead, no proposal, or propose.
+__device__ __forceinline__ void propose(const Params &p, int v, int begin, unsigned long long key)
+{
+    if (key == 0) {  // no unmatched neighbour: unmatchable (requests == n + 1)
         p.col[v] = kDead;
         p.ctl->match[v] = 2;
         p.req[v] = make_int2(-1, 0);
         return;
     }
-    if (key == 0) {
+    if (key == 1) {  // unmatched neighbours but no red one to propose to
         p.req[v] = make_int2(-2, 0);
         return;
     }
     const int j = (int)~(uint32_t)key;
     const int target = p.nbrs[j];
-    const long long slot = p.contiguous ? (long long)j : p.slot_off[v] + (j - r.x);
+    const long long slot = p.contiguous ? (long long)j : p.slot_off[v] + (j - begin);
     const unsigned long long rk = p.revkey[slot];
     if (rk) atomicMax(&p.best[target], rk);
     p.req[v] = make_int2(target, (int)(uint32_t)rk);
 }
 
-// Phase A for one long list: the whole block scans, then thread 0 proposes.
-template <bool kW, bool kStats>
-__device__ void scan_long(const Params &p, int v, int t)
+// Adjacency entries the reference's request loop inspects for this vertex
+// (random mode stops at the first red neighbour).
+template <bool kW>
+__device__ __forceinline__ unsigned long long request_seen(int begin, int deg, unsigned long long key)
 {
-    __shared__ unsigned long long s_key[kWarpsA];
-    __shared__ int s_alive[kWarpsA];
-    const int2 r = p.ranges[v];
-    unsigned long long key = 0;
-    int alive = 0;
-    for (int base = r.x; base < r.y; base += kBlockA) {
-        const int j = base + threadIdx.x;
-        if (j < r.y) {
-            const uint8_t c = p.col[p.nbrs[j]];
-            alive |= c != kMatched;
-            if (c == kRed) {
-                const unsigned long long k = cand_key<kW>(j, kW ? p.w[j] : 0.0f);
-                key = k > key ? k : key;
-            }
-        }
-        // Random mode stops at the first red neighbour (grRequest returns there).
-        if (!kW && __syncthreads_or(key != 0)) break;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long k2 = __shfl_down_sync(kFull, key, o);
-        key = k2 > key ? k2 : key;
-        alive |= __shfl_down_sync(kFull, alive, o);
-    }
-    const int warp = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) {
-        s_key[warp] = key;
-        s_alive[warp] = alive;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int i = 1; i < kWarpsA; ++i) {
-            key = s_key[i] > key ? s_key[i] : key;
-            alive |= s_alive[i];
-        }
-        if (kStats) {
-            const int deg = degree_of(r);
-            const long long seen = kW ? deg : (key ? (long long)((int)~(uint32_t)key - r.x + 1) : deg);
-            atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_REQ_ENTRIES], (unsigned long long)seen);
-            atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_BLUE_DEG], (unsigned long long)deg);
-        }
-        propose<kStats>(p, v, r, key, alive, t, kW);
-    }
-    __syncthreads();
+    if (kW || key < 2) return (unsigned long long)deg;
+    return (unsigned long long)((int)~(uint32_t)key - begin + 1);
 }
 
-// Phase A for 32 short lists: the warp walks their concatenated entries, 32 at
-// a time, and reduces per vertex with a segmented shuffle.
 template <bool kW, bool kStats>
-__device__ void scan_short_batch(const Params &p, const int *list, int begin, int count, int t)
+__device__ __forceinline__ void propose_counted(const Params &p, int4 it, unsigned long long key, int t)
 {
-    const int lane = threadIdx.x & 31;
-    const int idx = begin + lane;
-    int v = -1;
-    int2 r = make_int2(0, 0);
-    int deg = 0;
-    if (idx < count) {
-        v = list[idx];
-        r = p.ranges[v];
-        deg = degree_of(r);
+    if (kStats) {
+        atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_REQ_ENTRIES], request_seen<kW>(it.y, degree_of(it), key));
+        atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_BLUE_DEG], (unsigned long long)degree_of(it));
     }
-    int incl = deg;
+    propose(p, it.x, it.y, key);
+}
+
+// Key of a scan's best entry: weight order and position of its best red
+// neighbour (the reference's rule: strict > from -1 in list order), else 1 if
+// an unmatched neighbour was seen, else 0.
+template <bool kW>
+__device__ __forceinline__ unsigned long long strip_key(float bw, int bj, bool alive)
+{
+    if (bw > -1.0f) return kW ? (((unsigned long long)weight_order(bw) << 32) | (uint32_t)~bj)
+                              : (unsigned long long)(uint32_t)~bj;
+    return alive ? 1ull : 0ull;
+}
+
+constexpr int kShortStep = 8;  // entries a lane loads (and gathers) at once
+
+// Phase A for up to 32 short lists, one per lane: each lane walks its own list
+// (at most 32 entries) kShortStep entries at a time, keeping the reference's
+// choice with a running float compare.  Random mode ranks every red neighbour
+// with weight 0, so the first one wins and the walk stops there.
+template <bool kW, bool kStats>
+__device__ void scan_short_lanes(const Params &p, const int4 *list, int begin, int count, int t)
+{
+    const int idx = begin + (threadIdx.x & 31);
+    if (idx >= count) return;
+    const int4 it = list[idx];
+    float bw = -1.0f;
+    int bj = 0;
+    bool alive = false;
+    for (int b = it.y; b < it.z; b += kShortStep) {
+        int nb[kShortStep];
+        float wv[kShortStep];
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(kFull, incl, o);
-        if (lane >= o) incl += y;
-    }
-    const int excl = incl - deg;
-    const int total = __shfl_sync(kFull, incl, 31);
-    unsigned long long acc = 0;
-    int alive = 0;
-    for (int e0 = 0; e0 < total; e0 += 32) {
-        const int e = e0 + lane;
-        const bool valid = e < total;
-        // owner = first lane whose inclusive prefix exceeds e
-        int o = 0;
-#pragma unroll
-        for (int step = 16; step >= 1; step >>= 1) {
-            const int probe = __shfl_sync(kFull, incl, o + step - 1);
-            if (probe <= e) o += step;
+        for (int k = 0; k < kShortStep; ++k) {
+            const bool in = b + k < it.z;
+            nb[k] = in ? __ldcs(p.nbrs + b + k) : 0;
+            wv[k] = kW && in ? __ldcs(p.w + b + k) : 0.0f;
         }
-        const int ox = __shfl_sync(kFull, r.x, o);
-        const int oexcl = __shfl_sync(kFull, excl, o);
-        unsigned long long k = 0;
-        int a = 0;
-        if (valid) {
-            const int j = ox + (e - oexcl);
-            const uint8_t c = p.col[p.nbrs[j]];
-            a = c != kMatched;
-            if (c == kRed) k = cand_key<kW>(j, kW ? p.w[j] : 0.0f);
-        }
-        const int owner = valid ? o : 32 + lane;
-        // segmented suffix max / or over runs of equal owner
+        uint8_t c[kShortStep];
 #pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const unsigned long long k2 = __shfl_down_sync(kFull, k, d);
-            const int a2 = __shfl_down_sync(kFull, a, d);
-            const int o2 = __shfl_down_sync(kFull, owner, d);
-            if (lane + d < 32 && o2 == owner) {
-                k = k2 > k ? k2 : k;
-                a |= a2;
+        for (int k = 0; k < kShortStep; ++k) c[k] = p.col[nb[k]];
+#pragma unroll
+        for (int k = 0; k < kShortStep; ++k) {
+            if (b + k >= it.z) break;
+            alive |= c[k] != kMatched;
+            if (c[k] == kRed && wv[k] > bw) {
+                bw = wv[k];
+                bj = b + k;
             }
         }
-        // each vertex lane pulls the value from the head of its run in this chunk
-        const bool hit = deg > 0 && excl < e0 + 32 && incl > e0;
-        const int head = excl > e0 ? excl - e0 : 0;
-        const unsigned long long hk = __shfl_sync(kFull, k, head & 31);
-        const int ha = __shfl_sync(kFull, a, head & 31);
-        if (hit) {
-            acc = hk > acc ? hk : acc;
-            alive |= ha;
+        if (!kW && bw > -1.0f) break;  // grRequest returns at the first red neighbour
+    }
+    propose_counted<kW, kStats>(p, it, strip_key<kW>(bw, bj, alive), t);
+}
+
+// ---- worklist compaction for the set-up and commit passes ----
+//
+// A block handles tiles of kTileItems vertices, kPer per thread.  Each thread
+// decides the next list of its vertices; the block counts them per list with
+// warp scans, takes one atomic per list and tile (the staged list's item and
+// entry counts in one 64-bit atomic), and writes its items.
+
+constexpr int kBlockT = 512;
+constexpr int kPer = 4;
+constexpr int kTileItems = kBlockT * kPer;
+constexpr int kWarpsT = kBlockT / 32;
+
+// dest[k]: -1 (drop) or the list id kBlueS, kRedS, kRedLong, kStaged.
+__device__ __forceinline__ void compact_tile(const Params &p, int parity, const int (&dest)[kPer],
+                                             const int4 (&item)[kPer])
+{
+    __shared__ int s_warp[kWarpsT][5];  // per-warp counts, then per-warp offsets within the tile
+    __shared__ int s_base[5];           // tile bases: 4 list indices, then the staged entry offset
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int c[4] = {0, 0, 0, 0}, ent = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+#pragma unroll
+        for (int l = 0; l < 4; ++l) c[l] += dest[k] == l;
+        if (dest[k] == kStaged) ent += degree_of(item[k]);
+    }
+    int ex[5];
+#pragma unroll
+    for (int l = 0; l < 5; ++l) {
+        const int v = l < 4 ? c[l] : ent;
+        const int incl = warp_incl_scan(v);
+        ex[l] = incl - v;
+        if (lane == 31) s_warp[warp][l] = incl;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        const int l = threadIdx.x;
+        int run = 0;
+        for (int w = 0; w < kWarpsT; ++w) {
+            const int x = s_warp[w][l];
+            s_warp[w][l] = run;
+            run += x;
+        }
+        if (l < kStaged) {
+            s_base[l] = run ? atomicAdd(&p.ctl->cnt[parity][l], run) : 0;
+        } else {
+            int run_e = 0;
+            for (int w = 0; w < kWarpsT; ++w) {
+                const int x = s_warp[w][4];
+                s_warp[w][4] = run_e;
+                run_e += x;
+            }
+            unsigned long long old = 0;
+            if (run) old = atomicAdd(&p.ctl->staged_pack[parity], ((unsigned long long)run << 32) | (unsigned)run_e);
+            s_base[3] = (int)(old >> 32);
+            s_base[4] = (int)(old & 0xffffffffull);
         }
     }
-    if (v >= 0) {
-        if (kStats) {
-            const long long seen = kW ? deg : (acc ? (long long)((int)~(uint32_t)acc - r.x + 1) : deg);
-            atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_REQ_ENTRIES], (unsigned long long)seen);
-            atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_BLUE_DEG], (unsigned long long)deg);
+    __syncthreads();
+    int rc[4] = {0, 0, 0, 0}, re = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        const int l = dest[k];
+        if (l < 0) continue;
+        int idx = 0;
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+            if (l == m) idx = s_base[m] + s_warp[warp][m] + ex[m] + rc[m]++;
+        if (l != kStaged) {
+            p.lists[parity][l][idx] = item[k];
+        } else {
+            const int deg = degree_of(item[k]);
+            const int off = s_base[4] + s_warp[warp][4] + ex[4] + re;
+            re += deg;
+            p.lists[parity][kStaged][idx] = make_int4(item[k].x, item[k].y, item[k].z, off);
+            for (int s = (off + kSegEntries - 1) / kSegEntries; s * kSegEntries < off + deg; ++s)
+                p.seg_first[parity][s] = idx;
         }
-        propose<kStats>(p, v, r, acc, alive, t, kW);
     }
+    __syncthreads();  // s_warp / s_base are reused by the next tile
+}
+
+__device__ __forceinline__ int next_list(bool blue, int deg)
+{
+    if (deg > kSmallMax) return blue ? kStaged : kRedLong;
+    return blue ? kBlueS : kRedS;
 }
 
 // Round set-up: colour every vertex with seeds[0], clear proposal slots, and
 // fill the first worklists.
 template <bool kStats>
-__global__ void __launch_bounds__(kBlockB) k_init(Params p)
+__global__ void __launch_bounds__(kBlockT) k_init(Params p)
 {
     const Ctl *ctl = p.ctl;
     const uint32_t seed = p.seeds[0], barrier = ctl->barrier;
     const int n = p.n;
-    const int nloop = (n + blockDim.x - 1) / blockDim.x * blockDim.x;
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nloop; v += gridDim.x * blockDim.x) {
-        const bool in = v < n;
-        int which = 0;
-        unsigned long long blue = 0;
-        if (in) {
-            const uint8_t c = colour_of((uint32_t)v, seed, barrier);
-            p.col[v] = c;
-            p.best[v] = 0ull;
-            const bool longl = degree_of(p.ranges[v]) > kLargeDegree;
-            which = (c == kRed ? 2 : 0) + (longl ? 1 : 0);
-            blue = c == kBlue;
+    const int ntiles = (n + kTileItems - 1) / kTileItems;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        int dest[kPer];
+        int4 item[kPer];
+        unsigned long long act = 0, blue_n = 0;
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            const int v = tile * kTileItems + k * kBlockT + threadIdx.x;
+            dest[k] = -1;
+            item[k] = make_int4(v, 0, 0, 0);
+            if (v < n) {
+                const int2 r = p.ranges[v];
+                item[k].y = r.x;
+                item[k].z = r.y;
+                const int deg = degree_of(r);
+                const bool blue = colour_of((uint32_t)v, seed, barrier) == kBlue;
+                p.best[v] = 0ull;
+                if (deg > kSmallMax) {
+                    p.part_key[v] = 0ull;
+                    p.part_cnt[v] = 0;
+                }
+                ++act;
+                blue_n += blue;
+                if (blue && deg == 0) {  // no neighbours: unmatchable as soon as it is blue
+                    p.col[v] = kDead;
+                    p.ctl->match[v] = 2;
+                } else {
+                    p.col[v] = blue ? kBlue : kRed;
+                    dest[k] = next_list(blue, deg);
+                }
+            }
         }
-        append(p, 0, which, v, in);
         if (kStats) {
-            stat_add(p, 0, MM_ST_ACTIVE, in ? 1ull : 0ull);
-            stat_add(p, 0, MM_ST_BLUE, blue);
-            stat_add(p, 0, MM_ST_RED, in && !blue ? 1ull : 0ull);
+            stat_add(p, 0, MM_ST_ACTIVE, act);
+            stat_add(p, 0, MM_ST_BLUE, blue_n);
+            stat_add(p, 0, MM_ST_RED, act - blue_n);
         }
+        compact_tile(p, 0, dest, item);
     }
 }
 
-// Phase A: every blue vertex scans its list and proposes.
+// Phase A, short lists: warps claim batches of 32 blue short-list vertices.
+// Block 0 also resets the next round's list counters and cursors.
 template <bool kW, bool kStats>
-__global__ void __launch_bounds__(kBlockA) k_phase_a(Params p)
+__global__ void __launch_bounds__(kBlockA) k_phase_a_short(Params p)
 {
     Ctl *ctl = p.ctl;
     const int t = ctl->t;
     const int par = t & 1;
-    const int n_short = ctl->cnt[par][0];
-    const int n_long = ctl->cnt[par][1];
+    const int n_short = ctl->cnt[par][kBlueS];
     if (blockIdx.x == 0 && threadIdx.x < kLists) ctl->cnt[par ^ 1][threadIdx.x] = 0;
-    const int per_block = kBlockA;  // short lists per block unit (32 per warp)
-    const long long units = (long long)n_long + (n_short + per_block - 1) / per_block;
-    const int *longs = list_ptr(p, par, 1);
-    const int *shorts = list_ptr(p, par, 0);
-    const int warp = threadIdx.x >> 5;
-    for (long long u = blockIdx.x; u < units; u += gridDim.x) {
-        if (u < n_long) {
-            scan_long<kW, kStats>(p, longs[u], t);
-        } else {
-            const int b = (int)(u - n_long) * per_block + warp * 32;
-            if (b < n_short) scan_short_batch<kW, kStats>(p, shorts, b, n_short, t);
+    if (blockIdx.x == 0 && threadIdx.x == 32) {
+        ctl->task_short[par ^ 1] = 0;
+        ctl->task_stream[par ^ 1] = 0;
+        ctl->staged_pack[par ^ 1] = 0ull;
+        ctl->retired[par ^ 1] = 0;
+    }
+    const int units = (n_short + 31) / 32;
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int u = 0;
+        if (lane == 0) u = atomicAdd(&ctl->task_short[par], 1);
+        u = __shfl_sync(kFull, u, 0);
+        if (u >= units) break;
+        scan_short_lanes<kW, kStats>(p, p.lists[par][kBlueS], u * 32, n_short, t);
+    }
+}
+
+// ---- staged scans of long lists (Blackwell bulk copies into shared memory) ----
+
+constexpr int kWarpsStream = 4;    // warps per staged-scan block, each an independent pipeline
+constexpr int kStages = 2;         // slots per warp: one being scanned, one in flight
+constexpr int kStep = 17;          // entries per lane per pass: a whole strip of a full slot
+
+// Bulk-copy destinations must be 16-byte aligned: every slot row is a multiple
+// of 16 bytes and the per-warp struct (laid out back to back) is 16-aligned.
+struct __align__(16) StreamWarpSmem {
+    int nb[kStages][kSegCap];           // neighbour ids
+    float w[kStages][kSegCap];          // weights
+    unsigned long long acc[32];         // per-piece running max of the segment being scanned
+    unsigned long long bar[kStages];    // one mbarrier per slot
+    int span_end[32];                   // one past each piece's copied span in the slot
+    int first[32];                      // slot index of each piece's first real entry
+    int last[32];                       // one past its last real entry
+    int delta[32];                      // global position of a slot entry = slot index + delta
+};
+static_assert(sizeof(StreamWarpSmem) % 16 == 0, "per-warp staging area must keep 16-byte alignment");
+static_assert((kSegCap * sizeof(int)) % 16 == 0, "slot rows must be multiples of 16 bytes");
+static_assert(offsetof(StreamWarpSmem, w) % 16 == 0, "weight slots must be 16-byte aligned");
+static_assert(offsetof(StreamWarpSmem, bar) % 8 == 0, "mbarriers must be 8-byte aligned");
+
+__device__ __forceinline__ uint32_t smem_addr(const void *ptr) { return (uint32_t)__cvta_generic_to_shared(ptr); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect(unsigned long long *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// try_wait that lets the hardware suspend the warp for up to ~1 us while the
+// phase is incomplete, instead of spinning on issue slots.
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(1000u)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Wait for a slot's copies; false if the wait gave up.  Each try suspends the
+// warp for up to ~1 us, and the clock is read only every 1024 tries, so the
+// bound (~2 s) costs nothing while copies land normally.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, uint32_t parity)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    for (unsigned tries = 1;; ++tries) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((tries & 1023u) == 0 && global_ns() - t0 > 2000000000ull) return false;
+    }
+}
+
+// Bulk copy global -> shared, completing on `bar`; the source is streamed
+// (L2 evict-first) so it does not displace the colour and proposal arrays.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, unsigned long long *bar,
+                                          unsigned long long policy)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;"
+        ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(policy)
+        : "memory");
+}
+
+__device__ __forceinline__ unsigned long long evict_first_policy()
+{
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+// One staged segment as held by a warp: lane i holds the i-th list piece.
+struct StageSeg {
+    int4 it;      // the list's item {v, begin, end, offset}; it.x < 0 if none
+    int lo, hi;   // piece = list entries [lo, hi) (list-relative)
+    int off;      // slot offset (entries) of the piece's 16-byte-aligned copy
+    int plen;     // copied entries (aligned span)
+    int pieces;   // segments the whole list spans
+    int valid;    // warp-uniform: a segment was claimed
+};
+
+// Claim the next segment and start its bulk copies into `slot`.  The slot's
+// previous contents were only read by this warp and those reads completed
+// before the __syncwarp that ended its scan, so the copies may overwrite it.
+template <bool kW>
+__device__ __forceinline__ void claim_and_issue(const Params &p, StreamWarpSmem &sm, int par, int nseg, int nitems,
+                                                int slot, unsigned long long policy, StageSeg &g)
+{
+    const int lane = threadIdx.x & 31;
+    int s = 0;
+    if (lane == 0) s = atomicAdd(&p.ctl->task_stream[par], 1);
+    s = __shfl_sync(kFull, s, 0);
+    g.valid = s < nseg;
+    g.it = make_int4(-1, 0, 0, 0);
+    g.plen = 0;
+    g.lo = g.hi = 0;
+    g.pieces = 1;
+    if (!g.valid) return;
+    const int s_lo = s * kSegEntries, s_hi = s_lo + kSegEntries;
+    const int idx = p.seg_first[par][s] + lane;
+    if (idx < nitems) {
+        const int4 it = p.lists[par][kStaged][idx];
+        const int deg = degree_of(it);
+        if (it.w < s_hi && it.w + deg > s_lo) {
+            g.it = it;
+            g.lo = max(it.w, s_lo) - it.w;
+            g.hi = min(it.w + deg, s_hi) - it.w;
+            g.plen = ((it.y + g.hi + 3) & ~3) - ((it.y + g.lo) & ~3);
+            g.pieces = (it.w + deg - 1) / kSegEntries - it.w / kSegEntries + 1;
         }
     }
+    g.off = warp_incl_scan(g.plen) - g.plen;
+    uint32_t bytes = (uint32_t)g.plen * 4u * (kW ? 2u : 1u);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(kFull, bytes, o);
+    if (lane == 0) mbar_expect(&sm.bar[slot], bytes);
+    if (g.plen > 0) {
+        const int a = (g.it.y + g.lo) & ~3;
+        bulk_load(&sm.nb[slot][g.off], p.nbrs + a, (uint32_t)g.plen * 4u, &sm.bar[slot], policy);
+        if (kW) bulk_load(&sm.w[slot][g.off], p.w + a, (uint32_t)g.plen * 4u, &sm.bar[slot], policy);
+    }
+}
+
+// Scan a staged segment from its slot.  Lane l walks the contiguous strip
+// [l*S, (l+1)*S) of the slot, S odd so the 32 lanes hit 32 banks.  Within a
+// strip entries come in increasing list position, so a running float compare
+// (strict >) keeps exactly the entry the reference's loop would; the piece an
+// entry belongs to is tracked in registers (alignment junk around a piece is
+// skipped), and the lane folds its key into sm.acc with a shared atomic max
+// where its strip leaves a piece.  Random mode ranks every red neighbour with
+// weight 0, so the first one seen wins.
+template <bool kW>
+__device__ __forceinline__ bool scan_segment(const Params &p, StreamWarpSmem &sm, const StageSeg &g, int slot,
+                                             uint32_t parity)
+{
+    const int lane = threadIdx.x & 31;
+    if (!mbar_wait_bounded(&sm.bar[slot], parity)) return false;
+    const int *snb = sm.nb[slot];
+    const float *sw = sm.w[slot];
+    const int first = g.off + ((g.it.y + g.lo) & 3);  // slot index of the piece's first entry
+    sm.span_end[lane] = g.off + g.plen;
+    sm.first[lane] = first;
+    sm.last[lane] = first + (g.hi - g.lo);
+    sm.delta[lane] = (g.it.y + g.lo) - first;
+    const int used = __shfl_sync(kFull, g.off + g.plen, 31);
+    __syncwarp();
+    const int stride = ((used + 31) / 32) | 1;
+    const int p0 = lane * stride, p1 = min(p0 + stride, used);
+    if (p0 < p1) {
+        // piece holding p0: first lane whose span ends after it
+        int lo = 0, hi = 31;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (sm.span_end[mid] <= p0) lo = mid + 1;
+            else hi = mid;
+        }
+        int own = lo, own_end = sm.span_end[lo], own_first = sm.first[lo], own_last = sm.last[lo];
+        int own_delta = sm.delta[lo];
+        float bw = -1.0f;
+        int bj = 0;
+        bool alive = false;
+        for (int base = p0; base < p1; base += kStep) {
+            int nbv[kStep];
+            float wv[kStep];
+#pragma unroll
+            for (int k = 0; k < kStep; ++k) {
+                const bool in = base + k < p1;
+                nbv[k] = in ? snb[base + k] : 0;
+                wv[k] = kW && in ? sw[base + k] : 0.0f;
+            }
+            // alignment junk can hold anything (gaps of a non-contiguous CSR are
+            // never validated): clamp the index; those entries are ignored below
+            uint8_t c[kStep];
+#pragma unroll
+            for (int k = 0; k < kStep; ++k) c[k] = p.col[min((unsigned)nbv[k], (unsigned)(p.n - 1))];
+#pragma unroll
+            for (int k = 0; k < kStep; ++k) {
+                const int q = base + k;
+                if (q >= p1) break;
+                if (q >= own_end) {  // strip leaves the piece: fold it and move on
+                    const unsigned long long key = strip_key<kW>(bw, bj, alive);
+                    if (key) atomicMax(&sm.acc[own], key);
+                    bw = -1.0f;
+                    alive = false;
+                    do {
+                        ++own;
+                        own_end = sm.span_end[own];
+                    } while (q >= own_end);
+                    own_first = sm.first[own];
+                    own_last = sm.last[own];
+                    own_delta = sm.delta[own];
+                }
+                const bool real = q >= own_first && q < own_last;
+                alive |= real && c[k] != kMatched;
+                if (real && c[k] == kRed && wv[k] > bw) {
+                    bw = wv[k];
+                    bj = q + own_delta;
+                }
+            }
+        }
+        const unsigned long long key = strip_key<kW>(bw, bj, alive);
+        if (key) atomicMax(&sm.acc[own], key);
+    }
+    __syncwarp();
+    return true;
+}
+
+// Proposal of a whole list whose two loads (target id and reverse key) are in
+// flight; it is completed after the warp has scanned its next segment.
+struct PendingProposal {
+    int v;                  // -1: nothing pending
+    int target;
+    unsigned long long rk;
+};
+
+__device__ __forceinline__ void finish_proposal(const Params &p, const PendingProposal &q)
+{
+    if (q.v < 0) return;
+    if (q.rk) atomicMax(&p.best[q.target], q.rk);
+    p.req[q.v] = make_int2(q.target, (int)(uint32_t)q.rk);
+}
+
+// Fold a scanned segment.  A whole list that proposes only issues its loads
+// here (finish_proposal completes it later); dead / non-proposing lists are
+// finished at once; a list cut by segment edges folds its piece into part_key
+// and its last piece to arrive proposes.
+template <bool kW, bool kStats>
+__device__ __forceinline__ PendingProposal finish_segment(const Params &p, StreamWarpSmem &sm, const StageSeg &g,
+                                                          int t)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned long long key = sm.acc[lane];
+    sm.acc[lane] = 0ull;
+    __syncwarp();
+    PendingProposal q;
+    q.v = -1;
+    if (g.it.x < 0) return q;
+    if (kStats) {
+        atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_STAGED_DEG], (unsigned long long)(g.hi - g.lo));
+        atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_STAGED_ITEMS], 1ull);
+    }
+    if (g.pieces == 1) {
+        if (key < 2) {
+            propose_counted<kW, kStats>(p, g.it, key, t);
+            return q;
+        }
+        if (kStats) {
+            atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_REQ_ENTRIES],
+                      request_seen<kW>(g.it.y, degree_of(g.it), key));
+            atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_BLUE_DEG], (unsigned long long)degree_of(g.it));
+        }
+        const int j = (int)~(uint32_t)key;
+        const long long slot = p.contiguous ? (long long)j : p.slot_off[g.it.x] + (j - g.it.y);
+        q.v = g.it.x;
+        q.target = p.nbrs[j];
+        q.rk = p.revkey[slot];
+        return q;
+    }
+    const int v = g.it.x;
+    if (key) atomicMax(&p.part_key[v], key);
+    // acq_rel: this piece's max is visible before its arrival counts, and the
+    // last arrival sees every other piece's max
+    int done;
+    asm volatile("atom.add.acq_rel.gpu.s32 %0, [%1], 1;" : "=r"(done) : "l"(p.part_cnt + v) : "memory");
+    if (done == g.pieces - 1) {
+        const unsigned long long all = atomicExch(&p.part_key[v], 0ull);
+        p.part_cnt[v] = 0;
+        propose_counted<kW, kStats>(p, g.it, all, t);
+    }
+    return q;
+}
+
+// Phase A, long lists: each warp runs a two-slot pipeline -- while it scans
+// one segment from shared memory, the bulk copies of the next are in flight.
+template <bool kW, bool kStats>
+__global__ void __launch_bounds__(kWarpsStream * 32) k_phase_a_stream(Params p)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    StreamWarpSmem &sm = reinterpret_cast<StreamWarpSmem *>(smem_raw)[threadIdx.x >> 5];
+    Ctl *ctl = p.ctl;
+    const int t = ctl->t;
+    const int par = t & 1;
+    const unsigned long long pack = ctl->staged_pack[par];
+    const int nitems = (int)(pack >> 32);
+    const int nseg = (int)(((pack & 0xffffffffull) + kSegEntries - 1) / kSegEntries);
+    if (nseg == 0) return;
+    const int lane = threadIdx.x & 31;
+    if (lane == 0) {
+        for (int q = 0; q < kStages; ++q) mbar_init(&sm.bar[q], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    sm.acc[lane] = 0ull;
+    __syncwarp();
+    const unsigned long long policy = evict_first_policy();
+    uint32_t parity = 0u;  // bit q: phase parity of slot q's barrier
+    StageSeg cur, nxt;
+    PendingProposal pending;
+    pending.v = -1;
+    int s_cur = 0;
+    claim_and_issue<kW>(p, sm, par, nseg, nitems, s_cur, policy, cur);
+    while (cur.valid) {
+        claim_and_issue<kW>(p, sm, par, nseg, nitems, s_cur ^ 1, policy, nxt);
+        const bool ok = scan_segment<kW>(p, sm, cur, s_cur, (parity >> s_cur) & 1u);
+        parity ^= 1u << s_cur;
+        if (!ok) {
+            if (lane == 0) atomicExch(&ctl->status, 2);
+            return;
+        }
+        finish_proposal(p, pending);  // the previous segment's loads had this scan to land
+        pending = finish_segment<kW, kStats>(p, sm, cur, t);
+        cur = nxt;
+        s_cur ^= 1;
+    }
+    finish_proposal(p, pending);
+    // claims beyond the last segment armed nothing: no copy is in flight
+}
+
+// Rounds small enough for one block run in the tail kernel.
+constexpr int kTailThreads = 1024;
+constexpr long long kTailItems = 4096;        // vertices that can still be matched
+constexpr unsigned kTailEntries = 32768;      // entries of blue long lists
+
+// Close round t (one thread): record the outcome and decide what runs next.
+// Returns true if another round runs in the caller's loop.
+__device__ __forceinline__ bool close_round(Ctl *ctl, int t, int cap, bool has_next, bool seeds_short, long long next,
+                                            unsigned staged_entries, int retired, bool in_tail)
+{
+    const bool more = has_next && next > 0;
+    if (!more) {
+        if (seeds_short) ctl->status = 1;
+        // Vertices retired while being coloured for round t+1 are still active
+        // in that round for the reference, so it runs round t+1 and only finds
+        // nothing left at round t+2.
+        if (!ctl->maximal || next > 0) ctl->rounds = cap;
+        else ctl->rounds = min(retired > 0 ? t + 3 : t + 2, cap);
+    }
+    ctl->t = t + 1;
+    const bool to_tail = more && !in_tail && next <= kTailItems && staged_entries <= kTailEntries;
+    if (to_tail) ctl->tail = 1;
+    const bool loop = more && !to_tail;
+    ctl->cont = loop ? 1 : 0;
+    return loop;
 }
 
 // Phase B: commit proposals, recolour survivors with the next seed, compact
 // the worklists; the last block closes the round.
 template <bool kW, bool kStats>
-__global__ void __launch_bounds__(kBlockB) k_phase_b(Params p)
+__global__ void __launch_bounds__(kBlockT) k_phase_b(Params p)
 {
     Ctl *ctl = p.ctl;
     const int t = ctl->t;
     const int par = t & 1;
     const int cap = ctl->cap;
     bool has_next = t + 1 < cap;
-    bool seeds_short = has_next && t + 1 >= ctl->nseeds;
+    const bool seeds_short = has_next && t + 1 >= ctl->nseeds;
     if (seeds_short) has_next = false;
     const uint32_t next_seed = has_next ? p.seeds[t + 1] : 0u;
     const uint32_t barrier = ctl->barrier;
-    int cnt[kLists];
-    long long total = 0;
-#pragma unroll
-    for (int l = 0; l < kLists; ++l) {
-        cnt[l] = ctl->cnt[par][l];
-        total += cnt[l];
-    }
+    // lists in the order: blue short, blue long (staged), red short, red long
+    const int c0 = ctl->cnt[par][kBlueS], c1 = (int)(ctl->staged_pack[par] >> 32), c2 = ctl->cnt[par][kRedS],
+              c3 = ctl->cnt[par][kRedLong];
+    const long long total = (long long)c0 + c1 + c2 + c3;
+    const long long ntiles = (total + kTileItems - 1) / kTileItems;
     int *match = ctl->match;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    const long long loop_end = (total + blockDim.x - 1) / blockDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < loop_end; i += stride) {
-        bool in = i < total;
-        int which = 0;
-        long long k = i;
-        if (in) {
-            while (which < kLists - 1 && k >= cnt[which]) {
-                k -= cnt[which];
-                ++which;
-            }
-        }
-        int v = in ? list_ptr(p, par, which)[k] : 0;
-        bool survive = false;
-        unsigned long long matched = 0, seen = 0, rdeg = 0;
-        if (in) {
-            if (which < 2) {  // blue
-                const int2 q = p.req[v];
-                if (q.x != -1) {
-                    bool won = false;
-                    if (q.y != 0) won = (uint32_t)p.best[q.x] == (uint32_t)q.y;
-                    if (won) {
-                        match[v] = 4 + min(v, q.x);
-                        p.col[v] = kMatched;
-                        matched = 1;
-                    } else {
-                        survive = true;
-                    }
-                }
-            } else {  // red
-                const unsigned long long key = p.best[v];
-                if (kStats) {
-                    const int2 r = p.ranges[v];
-                    const int deg = degree_of(r);
-                    rdeg = deg;
-                    seen = kW ? deg : (key ? (long long)((int)~(uint32_t)key - r.x + 1) : deg);
-                }
-                if (key) {
-                    const int u = p.nbrs[(int)~(uint32_t)key];
-                    match[v] = 4 + min(v, u);
-                    p.col[v] = kMatched;
-                    matched = 1;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        int4 it[kPer];
+        bool in[kPer], blue[kPer];
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            long long i = tile * kTileItems + k * kBlockT + threadIdx.x;
+            in[k] = i < total;
+            blue[k] = true;
+            it[k] = make_int4(0, 0, 0, 0);
+            if (in[k]) {
+                if (i < c0) {
+                    it[k] = p.lists[par][kBlueS][i];
+                } else if ((i -= c0) < c1) {
+                    it[k] = p.lists[par][kStaged][i];
+                } else if ((i -= c1) < c2) {
+                    it[k] = p.lists[par][kRedS][i];
+                    blue[k] = false;
                 } else {
-                    survive = true;
+                    it[k] = p.lists[par][kRedLong][i - c2];
+                    blue[k] = false;
                 }
             }
         }
-        int next_which = which;
-        unsigned long long nb = 0;
-        if (survive && has_next) {
-            const uint8_t c = colour_of((uint32_t)v, next_seed, barrier);
-            p.col[v] = c;
-            next_which = (c == kRed ? 2 : 0) + (which & 1);
-            nb = c == kBlue;
+        // proposal state: blue -> its request, red -> the best proposal it received
+        int2 q[kPer];
+        unsigned long long key[kPer];
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            q[k] = make_int2(-1, 0);
+            key[k] = 0ull;
+            if (in[k]) {
+                if (blue[k]) q[k] = p.req[it[k].x];
+                else key[k] = p.best[it[k].x];
+            }
         }
-        append(p, par ^ 1, next_which, v, survive);
+#pragma unroll
+        for (int k = 0; k < kPer; ++k)
+            if (in[k] && blue[k] && q[k].y != 0) key[k] = p.best[q[k].x];
+        int partner[kPer];
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            partner[k] = -1;
+            if (!in[k]) continue;
+            if (blue[k]) {
+                if (q[k].y != 0 && (uint32_t)key[k] == (uint32_t)q[k].y) partner[k] = q[k].x;
+            } else if (key[k]) {
+                partner[k] = p.nbrs[(int)~(uint32_t)key[k]];
+            }
+        }
+        int dest[kPer];
+        unsigned long long matched = 0, seen = 0, rdeg = 0, act = 0, nblue = 0;
+        int retired = 0;
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            dest[k] = -1;
+            if (!in[k]) continue;
+            const int v = it[k].x;
+            const int deg = degree_of(it[k]);
+            if (kStats && !blue[k]) {
+                rdeg += deg;
+                seen += kW ? deg : (key[k] ? (unsigned long long)((int)~(uint32_t)key[k] - it[k].y + 1) : deg);
+            }
+            if (partner[k] >= 0) {
+                match[v] = 4 + min(v, partner[k]);
+                p.col[v] = kMatched;
+                ++matched;
+                continue;
+            }
+            if (blue[k] && q[k].x == -1) continue;  // unmatchable (marked in phase A)
+            // survivor
+            if (!has_next) {
+                dest[k] = next_list(blue[k], deg);
+                continue;
+            }
+            const bool nb = colour_of((uint32_t)v, next_seed, barrier) == kBlue;
+            ++act;
+            nblue += nb;
+            if (nb && deg == 0) {  // no neighbours: unmatchable as soon as it is blue
+                p.col[v] = kDead;
+                match[v] = 2;
+                ++retired;
+            } else {
+                p.col[v] = nb ? kBlue : kRed;
+                dest[k] = next_list(nb, deg);
+            }
+        }
         if (kStats) {
             stat_add(p, t, MM_ST_MATCHED, matched);
             stat_add(p, t, MM_ST_RESP_ENTRIES, seen);
             stat_add(p, t, MM_ST_RED_DEG, rdeg);
             if (has_next) {
-                stat_add(p, t + 1, MM_ST_ACTIVE, survive ? 1ull : 0ull);
-                stat_add(p, t + 1, MM_ST_BLUE, nb);
-                stat_add(p, t + 1, MM_ST_RED, survive && !nb ? 1ull : 0ull);
+                stat_add(p, t + 1, MM_ST_ACTIVE, act);
+                stat_add(p, t + 1, MM_ST_BLUE, nblue);
+                stat_add(p, t + 1, MM_ST_RED, act - nblue);
             }
         }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) retired += __shfl_xor_sync(kFull, retired, o);
+        if ((threadIdx.x & 31) == 0 && retired) atomicAdd(&ctl->retired[par ^ 1], retired);
+        compact_tile(p, par ^ 1, dest, it);
     }
     // Round bookkeeping by the last block to arrive.
     __syncthreads();
@@ -425,21 +896,204 @@ __global__ void __launch_bounds__(kBlockB) k_phase_b(Params p)
         const unsigned ticket = atomicAdd(&ctl->ticket, 1u);
         if (ticket == gridDim.x - 1) {
             __threadfence();
-            long long next = 0;
+            long long next = (long long)(atomicAdd(&ctl->staged_pack[par ^ 1], 0ull) >> 32);
 #pragma unroll
-            for (int l = 0; l < kLists; ++l) next += atomicAdd(&ctl->cnt[par ^ 1][l], 0);
-            const bool cont = has_next && next > 0;
-            if (!cont) {
-                if (seeds_short) ctl->status = 1;
-                ctl->rounds = (ctl->maximal && next == 0) ? min(t + 2, cap) : cap;
-            }
-            ctl->t = t + 1;
+            for (int l = 0; l < kStaged; ++l) next += atomicAdd(&ctl->cnt[par ^ 1][l], 0);
+            const int retired_all = atomicAdd(&ctl->retired[par ^ 1], 0);
+            const unsigned staged_entries =
+                (unsigned)(atomicAdd(&ctl->staged_pack[par ^ 1], 0ull) & 0xffffffffull);
             ctl->ticket = 0u;
-            ctl->cont = cont ? 1 : 0;
+            const bool cont = close_round(ctl, t, cap, has_next, seeds_short, next, staged_entries, retired_all, false);
             // Outside a graph (the stepped profiling driver) the host reads ctl->cont instead.
             if (p.loop) cudaGraphSetConditional(p.loop, cont ? 1u : 0u);
         }
     }
+}
+
+// ---- tail: the last, small rounds in one block ----
+//
+// Same round as the grid kernels (scan + propose, commit + recolour), with
+// block barriers between the phases instead of kernel launches.  Values that
+// other threads of the block changed by atomics (best, counters) are read
+// from L2 (__ldcg), never from this SM's L1.
+
+// One short list scanned by one thread, kShortStep loads and gathers at a time.
+template <bool kW, bool kStats>
+__device__ void tail_scan_thread(const Params &p, int4 it, int t)
+{
+    float bw = -1.0f;
+    int bj = 0;
+    bool alive = false;
+    for (int b = it.y; b < it.z; b += kShortStep) {
+        int nb[kShortStep];
+        float wv[kShortStep];
+#pragma unroll
+        for (int k = 0; k < kShortStep; ++k) {
+            const bool in = b + k < it.z;
+            nb[k] = in ? p.nbrs[b + k] : 0;
+            wv[k] = kW && in ? p.w[b + k] : 0.0f;
+        }
+        uint8_t c[kShortStep];
+#pragma unroll
+        for (int k = 0; k < kShortStep; ++k) c[k] = __ldcg(p.col + nb[k]);
+#pragma unroll
+        for (int k = 0; k < kShortStep; ++k) {
+            if (b + k >= it.z) break;
+            alive |= c[k] != kMatched;
+            if (c[k] == kRed && wv[k] > bw) {
+                bw = wv[k];
+                bj = b + k;
+            }
+        }
+        if (!kW && bw > -1.0f) break;  // grRequest returns at the first red neighbour
+    }
+    propose_counted<kW, kStats>(p, it, strip_key<kW>(bw, bj, alive), t);
+}
+
+// One long list scanned by one warp: 4 entries per lane per step, 32 apart.
+template <bool kW, bool kStats>
+__device__ void tail_scan_warp(const Params &p, int4 it, int t)
+{
+    const int lane = threadIdx.x & 31;
+    float bw = -1.0f;
+    int bj = 0;
+    bool alive = false;
+    for (int base = it.y; base < it.z; base += 128) {
+        int nb[4];
+        float wv[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int j = base + k * 32 + lane;
+            nb[k] = j < it.z ? p.nbrs[j] : 0;
+            wv[k] = kW && j < it.z ? p.w[j] : 0.0f;
+        }
+        uint8_t c[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) c[k] = __ldcg(p.col + nb[k]);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int j = base + k * 32 + lane;
+            if (j >= it.z) break;
+            alive |= c[k] != kMatched;
+            if (c[k] == kRed && wv[k] > bw) {
+                bw = wv[k];
+                bj = j;
+            }
+        }
+        if (!kW && __any_sync(kFull, bw > -1.0f)) break;
+    }
+    unsigned long long key = strip_key<kW>(bw, bj, alive);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long k2 = __shfl_xor_sync(kFull, key, o);
+        key = k2 > key ? k2 : key;
+    }
+    if (lane == 0) propose_counted<kW, kStats>(p, it, key, t);
+}
+
+template <bool kW, bool kStats>
+__global__ void __launch_bounds__(kTailThreads) k_tail(Params p)
+{
+    Ctl *ctl = p.ctl;
+    if (!__ldcg(&ctl->tail)) return;
+    __shared__ int s_t, s_more;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (;;) {
+        if (tid == 0) {
+            const int t = ctl->t;
+            s_t = t;
+            const int nx = (t & 1) ^ 1;
+            for (int l = 0; l < kLists; ++l) ctl->cnt[nx][l] = 0;
+            ctl->staged_pack[nx] = 0ull;
+            ctl->retired[nx] = 0;
+        }
+        __syncthreads();
+        const int t = s_t, par = t & 1, nx = par ^ 1;
+        const int cap = ctl->cap;
+        const int c_bs = __ldcg(&ctl->cnt[par][kBlueS]);
+        const int c_st = (int)(__ldcg(&ctl->staged_pack[par]) >> 32);
+        const int c_rs = __ldcg(&ctl->cnt[par][kRedS]);
+        const int c_rl = __ldcg(&ctl->cnt[par][kRedLong]);
+        // scan + propose
+        for (int i = tid; i < c_bs; i += kTailThreads) tail_scan_thread<kW, kStats>(p, p.lists[par][kBlueS][i], t);
+        for (int i = warp; i < c_st; i += kTailThreads / 32) tail_scan_warp<kW, kStats>(p, p.lists[par][kStaged][i], t);
+        __syncthreads();
+        // commit + recolour + compact
+        bool has_next = t + 1 < cap;
+        const bool seeds_short = has_next && t + 1 >= ctl->nseeds;
+        if (seeds_short) has_next = false;
+        const uint32_t next_seed = has_next ? p.seeds[t + 1] : 0u;
+        const uint32_t barrier = ctl->barrier;
+        int *match = ctl->match;
+        const int total = c_bs + c_st + c_rs + c_rl;
+        for (int i = tid; i < total; i += kTailThreads) {
+            int4 it;
+            bool blue = true;
+            if (i < c_bs) it = p.lists[par][kBlueS][i];
+            else if (i < c_bs + c_st) it = p.lists[par][kStaged][i - c_bs];
+            else if (i < c_bs + c_st + c_rs) { it = p.lists[par][kRedS][i - c_bs - c_st]; blue = false; }
+            else { it = p.lists[par][kRedLong][i - c_bs - c_st - c_rs]; blue = false; }
+            const int v = it.x;
+            const int deg = degree_of(it);
+            int partner = -1;
+            bool dead = false;
+            if (blue) {
+                const int2 q = __ldcg(&p.req[v]);
+                dead = q.x == -1;
+                if (q.y != 0 && (uint32_t)__ldcg(&p.best[q.x]) == (uint32_t)q.y) partner = q.x;
+            } else {
+                const unsigned long long key = __ldcg(&p.best[v]);
+                if (key) partner = p.nbrs[(int)~(uint32_t)key];
+                if (kStats) {
+                    atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_RED_DEG], (unsigned long long)deg);
+                    atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_RESP_ENTRIES],
+                              kW ? (unsigned long long)deg
+                                 : (key ? (unsigned long long)((int)~(uint32_t)key - it.y + 1) : (unsigned long long)deg));
+                }
+            }
+            if (partner >= 0) {
+                match[v] = 4 + min(v, partner);
+                p.col[v] = kMatched;
+                if (kStats) atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_MATCHED], 1ull);
+                continue;
+            }
+            if (dead) continue;
+            int dest;
+            if (!has_next) {
+                dest = next_list(blue, deg);
+            } else {
+                const bool nb = colour_of((uint32_t)v, next_seed, barrier) == kBlue;
+                if (kStats) {
+                    atomicAdd(&p.stats[(size_t)(t + 1) * MM_STATS_COLS + MM_ST_ACTIVE], 1ull);
+                    atomicAdd(&p.stats[(size_t)(t + 1) * MM_STATS_COLS + (nb ? MM_ST_BLUE : MM_ST_RED)], 1ull);
+                }
+                if (nb && deg == 0) {  // no neighbours: unmatchable as soon as it is blue
+                    p.col[v] = kDead;
+                    match[v] = 2;
+                    atomicAdd(&ctl->retired[nx], 1);
+                    continue;
+                }
+                p.col[v] = nb ? kBlue : kRed;
+                dest = next_list(nb, deg);
+            }
+            if (dest == kStaged) {
+                const unsigned long long old =
+                    atomicAdd(&ctl->staged_pack[nx], (1ull << 32) | (unsigned long long)(unsigned)deg);
+                p.lists[nx][kStaged][(int)(old >> 32)] = make_int4(it.x, it.y, it.z, (int)(old & 0xffffffffull));
+            } else {
+                p.lists[nx][dest][atomicAdd(&ctl->cnt[nx][dest], 1)] = it;
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            long long next = (long long)(__ldcg(&ctl->staged_pack[nx]) >> 32);
+            for (int l = 0; l < kStaged; ++l) next += __ldcg(&ctl->cnt[nx][l]);
+            s_more = close_round(ctl, t, cap, has_next, seeds_short, next, 0u, __ldcg(&ctl->retired[nx]), true);
+        }
+        __syncthreads();
+        if (!s_more) break;
+    }
+    (void)lane;
 }
 
 // After the loop: vertices still able to match keep their last colour as
@@ -448,11 +1102,11 @@ __global__ void __launch_bounds__(kBlockB) k_finish(Params p)
 {
     const Ctl *ctl = p.ctl;
     const int par = ctl->t & 1;
-    long long total = 0;
     int cnt[kLists];
+    long long total = 0;
 #pragma unroll
     for (int l = 0; l < kLists; ++l) {
-        cnt[l] = ctl->cnt[par][l];
+        cnt[l] = l == kStaged ? (int)(ctl->staged_pack[par] >> 32) : ctl->cnt[par][l];
         total += cnt[l];
     }
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
@@ -463,30 +1117,39 @@ __global__ void __launch_bounds__(kBlockB) k_finish(Params p)
             k -= cnt[which];
             ++which;
         }
-        const int v = list_ptr(p, par, which)[k];
+        const int v = p.lists[par][which][k].x;
         ctl->match[v] = p.col[v];
     }
 }
 
 // ---------------------------------------------------------------------------
-// Preparation: reverse proposal keys.
+// Preparation: degree classes and reverse proposal keys.
 
 struct PrepInfo {
     unsigned long long sum_deg;
     unsigned long long max_deg;
+    unsigned long long short_count;   // lists of at most kSmallMax entries
+    unsigned long long long_count;    // longer lists
+    unsigned long long long_entries;  // entries in longer lists
     int noncontig;
-    int bad;
+    int pad;
 };
 
 __global__ void k_scan_ranges(const int2 *ranges, int n, long long nnz, PrepInfo *info, long long *deg_out)
 {
-    unsigned long long sum = 0, mx = 0;
+    unsigned long long sum = 0, mx = 0, nshort = 0, nlong = 0, elong = 0;
     int nc = 0;
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
         const int2 r = ranges[v];
         const int d = degree_of(r);
         sum += d;
         mx = d > (long long)mx ? d : mx;
+        if (d > kSmallMax) {
+            nlong += 1;
+            elong += d;
+        } else {
+            nshort += 1;
+        }
         if (deg_out) deg_out[v] = d;
         if (r.y < r.x) nc = 1;
         if (v == 0 && r.x != 0) nc = 1;
@@ -498,11 +1161,17 @@ __global__ void k_scan_ranges(const int2 *ranges, int n, long long nnz, PrepInfo
         sum += __shfl_down_sync(kFull, sum, o);
         const unsigned long long m2 = __shfl_down_sync(kFull, mx, o);
         mx = m2 > mx ? m2 : mx;
+        nshort += __shfl_down_sync(kFull, nshort, o);
+        nlong += __shfl_down_sync(kFull, nlong, o);
+        elong += __shfl_down_sync(kFull, elong, o);
         nc |= __shfl_down_sync(kFull, nc, o);
     }
     if ((threadIdx.x & 31) == 0) {
         if (sum) atomicAdd(&info->sum_deg, sum);
         if (mx) atomicMax(&info->max_deg, mx);
+        if (nshort) atomicAdd(&info->short_count, nshort);
+        if (nlong) atomicAdd(&info->long_count, nlong);
+        if (elong) atomicAdd(&info->long_entries, elong);
         if (nc) atomicOr(&info->noncontig, 1);
     }
 }
@@ -527,13 +1196,18 @@ __global__ void k_pair_items(const int2 *ranges, const int *nbrs, int n, int bit
     }
 }
 
-// Key red `owner` gives the entry at `slot` (its own list).
+// Key red `owner` gives the entry at `slot` of its own list (the revkey form:
+// 0 for weights the reference can never pick).
 template <bool kW>
 __device__ __forceinline__ unsigned long long red_key(const int2 *ranges, const float *w, int contiguous,
                                                       const long long *slot_off, long long owner, long long slot)
 {
     const long long pos = contiguous ? slot : (long long)ranges[owner].x + (slot - slot_off[owner]);
-    return cand_key<kW>((int)pos, kW ? w[pos] : 0.0f);
+    if (kW) {
+        const float x = w[pos];
+        return x > -1.0f ? (((unsigned long long)weight_order(x) << 32) | (uint32_t)~(int)pos) : 0ull;
+    }
+    return (unsigned long long)(uint32_t)~(int)pos;
 }
 
 // For each group of equal unordered pair, give every item the best key of the
@@ -565,6 +1239,9 @@ __global__ void k_pair_groups(const unsigned long long *keys, const int *vals, l
     }
 }
 
+// Control block rounded to 256 bytes so the seeds that follow it stay aligned.
+constexpr size_t kCtlBytes = (sizeof(Ctl) + 255) / 256 * 256;
+
 // Captured round loop of one (graph, type, stats) combination.
 struct Plan {
     int type = 0;
@@ -574,17 +1251,23 @@ struct Plan {
 };
 
 struct PushState {
-    // scratch owned by the push path
     uint8_t *col = nullptr;
     int2 *req = nullptr;
     unsigned long long *best = nullptr;
-    int *lists = nullptr;
-    uint32_t *seeds = nullptr;
+    unsigned long long *part_key = nullptr;
+    int *part_cnt = nullptr;
+    int4 *list_mem = nullptr;
+    int4 *lists[2][kLists] = {};
+    int *seg_mem = nullptr;
+    int *seg_first[2] = {};
+    uint32_t *seeds = nullptr;        // device: right after ctl in one allocation
     Ctl *ctl = nullptr;
+    unsigned char *host_stage = nullptr;  // pinned: control block + seeds, uploaded in one copy
+    unsigned char *host_back = nullptr;   // pinned: control block read back
     unsigned long long *stats = nullptr;
     Plan plans[8];
     int nplans = 0;
-    int blocks_a = 0, blocks_b = 0;
+    int blocks_a = 0, blocks_b = 0, blocks_stream = 0, stream_smem = 0;
 };
 
 int bits_for(long long n)
@@ -592,6 +1275,26 @@ int bits_for(long long n)
     int b = 1;
     while ((1ll << b) < n) ++b;
     return b;
+}
+
+void free_state(PushState *s)
+{
+    for (int i = 0; i < s->nplans; ++i) {
+        if (s->plans[i].exec) cudaGraphExecDestroy(s->plans[i].exec);
+        if (s->plans[i].graph) cudaGraphDestroy(s->plans[i].graph);
+    }
+    cudaFree(s->col);
+    cudaFree(s->req);
+    cudaFree(s->best);
+    cudaFree(s->part_key);
+    cudaFree(s->part_cnt);
+    cudaFree(s->list_mem);
+    cudaFree(s->seg_mem);
+    cudaFree(s->ctl);
+    cudaFreeHost(s->host_stage);
+    cudaFreeHost(s->host_back);
+    cudaFree(s->stats);
+    delete s;
 }
 
 mm_status alloc_state(mm_graph *g, PushState **out)
@@ -602,30 +1305,61 @@ mm_status alloc_state(mm_graph *g, PushState **out)
         return MM_ERR_NOMEM;
     }
     const size_t n = (size_t)(g->n > 0 ? g->n : 1);
+    // list capacities: every vertex is in at most one list per parity
+    const size_t cap[kLists] = {(size_t)g->short_count, (size_t)g->short_count, (size_t)g->long_count,
+                                (size_t)g->long_count};
+    size_t per_parity = 0;
+    for (int l = 0; l < kLists; ++l) per_parity += cap[l];
+    const size_t nseg_cap = (size_t)(g->long_entries / kSegEntries) + 2;
     cudaError_t e = cudaSuccess;
     if (e == cudaSuccess) e = cudaMalloc(&s->col, n);
     if (e == cudaSuccess) e = cudaMalloc(&s->req, n * sizeof(int2));
     if (e == cudaSuccess) e = cudaMalloc(&s->best, n * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMalloc(&s->lists, n * 2 * kLists * sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc(&s->seeds, 256 * sizeof(uint32_t));
-    if (e == cudaSuccess) e = cudaMalloc(&s->ctl, sizeof(Ctl));
+    if (e == cudaSuccess) e = cudaMalloc(&s->part_key, n * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&s->part_cnt, n * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&s->list_mem, (2 * per_parity + 1) * sizeof(int4));
+    if (e == cudaSuccess) e = cudaMalloc(&s->seg_mem, 2 * nseg_cap * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&s->ctl, kCtlBytes + 256 * sizeof(uint32_t));
+    if (e == cudaSuccess) s->seeds = reinterpret_cast<uint32_t *>(reinterpret_cast<unsigned char *>(s->ctl) + kCtlBytes);
+    if (e == cudaSuccess) e = cudaHostAlloc(&s->host_stage, kCtlBytes + 256 * sizeof(uint32_t), cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaHostAlloc(&s->host_back, kCtlBytes, cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaMalloc(&s->stats, sizeof(unsigned long long) * kMaxRounds * MM_STATS_COLS);
     if (e != cudaSuccess) {
-        cudaFree(s->col); cudaFree(s->req); cudaFree(s->best); cudaFree(s->lists);
-        cudaFree(s->seeds); cudaFree(s->ctl); cudaFree(s->stats);
-        delete s;
+        free_state(s);
         cudaGetLastError();
         set_error(std::string("push: device allocation failed: ") + cudaGetErrorString(e));
         return MM_ERR_NOMEM;
     }
+    size_t off = 0;
+    for (int par = 0; par < 2; ++par) {
+        for (int l = 0; l < kLists; ++l) {
+            s->lists[par][l] = s->list_mem + off;
+            off += cap[l];
+        }
+        s->seg_first[par] = s->seg_mem + par * nseg_cap;
+    }
     int sms = 148, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int occ_a = 0, occ_b = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_phase_a<true, false>, kBlockA, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_phase_b<true, false>, kBlockB, 0);
+    // the staged scan keeps two slots per warp in dynamic shared memory
+    const int stream_smem = (int)(sizeof(StreamWarpSmem) * kWarpsStream);
+    cudaFuncSetAttribute(k_phase_a_stream<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, stream_smem);
+    cudaFuncSetAttribute(k_phase_a_stream<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, stream_smem);
+    cudaFuncSetAttribute(k_phase_a_stream<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, stream_smem);
+    cudaFuncSetAttribute(k_phase_a_stream<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, stream_smem);
+    int occ_a = 0, occ_s = 0, occ_b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_phase_a_short<true, false>, kBlockA, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, k_phase_a_stream<true, false>, kWarpsStream * 32, stream_smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_phase_b<true, false>, kBlockT, 0);
     s->blocks_a = sms * (occ_a > 0 ? occ_a : 4);
+    s->blocks_stream = sms * (occ_s > 0 ? occ_s : 1);
+    s->stream_smem = stream_smem;
     s->blocks_b = sms * (occ_b > 0 ? occ_b : 4);
+    cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) {
+        free_state(s);
+        return cuda_fail(le, "push: kernel attributes");
+    }
     *out = s;
     return MM_OK;
 }
@@ -643,7 +1377,12 @@ Params make_params(mm_graph *g, PushState *s, bool weighted, bool stats, cudaGra
     p.col = s->col;
     p.req = s->req;
     p.best = s->best;
-    p.lists = s->lists;
+    p.part_key = s->part_key;
+    p.part_cnt = s->part_cnt;
+    for (int par = 0; par < 2; ++par) {
+        for (int l = 0; l < kLists; ++l) p.lists[par][l] = s->lists[par][l];
+        p.seg_first[par] = s->seg_first[par];
+    }
     p.seeds = s->seeds;
     p.ctl = s->ctl;
     p.stats = stats ? s->stats : nullptr;
@@ -664,14 +1403,14 @@ mm_status build_plan(mm_graph *g, PushState *s, Plan *plan)
     }
     Params prm = make_params(g, s, kW, kStats, h);
     void *args[] = {&prm};
-    const int blocks_init = grid_for(g->n, kBlockB, s->blocks_b);
+    const int blocks_init = grid_for(g->n, kTileItems, s->blocks_b);
 
     cudaKernelNodeParams kp = {};
     kp.func = (void *)k_init<kStats>;
     kp.gridDim = dim3(blocks_init);
-    kp.blockDim = dim3(kBlockB);
+    kp.blockDim = dim3(kBlockT);
     kp.kernelParams = args;
-    cudaGraphNode_t n_init, n_loop, n_fin, n_a, n_b;
+    cudaGraphNode_t n_init, n_loop, n_fin, n_a, n_l, n_b;
     e = cudaGraphAddKernelNode(&n_init, graph, nullptr, 0, &kp);
 
     cudaGraphNodeParams cp = {};
@@ -681,21 +1420,41 @@ mm_status build_plan(mm_graph *g, PushState *s, Plan *plan)
     cp.conditional.size = 1;
     if (e == cudaSuccess) e = cudaGraphAddNode(&n_loop, graph, &n_init, 1, &cp);
     if (e == cudaSuccess) {
+        // loop body: the two phase-A scans run side by side, then phase B
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         cudaKernelNodeParams ka = {};
-        ka.func = (void *)k_phase_a<kW, kStats>;
+        ka.func = (void *)k_phase_a_short<kW, kStats>;
         ka.gridDim = dim3(s->blocks_a);
         ka.blockDim = dim3(kBlockA);
         ka.kernelParams = args;
         e = cudaGraphAddKernelNode(&n_a, body, nullptr, 0, &ka);
         if (e == cudaSuccess) {
+            cudaKernelNodeParams kl = {};
+            kl.func = (void *)k_phase_a_stream<kW, kStats>;
+            kl.gridDim = dim3(s->blocks_stream);
+            kl.blockDim = dim3(kWarpsStream * 32);
+            kl.sharedMemBytes = (unsigned)s->stream_smem;
+            kl.kernelParams = args;
+            e = cudaGraphAddKernelNode(&n_l, body, nullptr, 0, &kl);
+        }
+        if (e == cudaSuccess) {
             cudaKernelNodeParams kb = {};
             kb.func = (void *)k_phase_b<kW, kStats>;
             kb.gridDim = dim3(s->blocks_b);
-            kb.blockDim = dim3(kBlockB);
+            kb.blockDim = dim3(kBlockT);
             kb.kernelParams = args;
-            e = cudaGraphAddKernelNode(&n_b, body, &n_a, 1, &kb);
+            const cudaGraphNode_t deps[2] = {n_a, n_l};
+            e = cudaGraphAddKernelNode(&n_b, body, deps, 2, &kb);
         }
+    }
+    cudaGraphNode_t n_tail;
+    if (e == cudaSuccess) {
+        cudaKernelNodeParams kt = {};
+        kt.func = (void *)k_tail<kW, kStats>;
+        kt.gridDim = dim3(1);
+        kt.blockDim = dim3(kTailThreads);
+        kt.kernelParams = args;
+        e = cudaGraphAddKernelNode(&n_tail, graph, &n_loop, 1, &kt);
     }
     if (e == cudaSuccess) {
         cudaKernelNodeParams kf = {};
@@ -703,7 +1462,7 @@ mm_status build_plan(mm_graph *g, PushState *s, Plan *plan)
         kf.gridDim = dim3(grid_for(g->n, kBlockB, s->blocks_b));
         kf.blockDim = dim3(kBlockB);
         kf.kernelParams = args;
-        e = cudaGraphAddKernelNode(&n_fin, graph, &n_loop, 1, &kf);
+        e = cudaGraphAddKernelNode(&n_fin, graph, &n_tail, 1, &kf);
     }
     cudaGraphExec_t exec = nullptr;
     if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
@@ -716,6 +1475,121 @@ mm_status build_plan(mm_graph *g, PushState *s, Plan *plan)
     return MM_OK;
 }
 
+// Shared set-up of one matching call: preparation, state, control block.
+mm_status begin_call(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds, int *d_match,
+                     cudaStream_t stream, PushState **out)
+{
+    mm_status st = push_prepare(g, is_weighted(type) ? 1 : 0, stream);
+    if (st != MM_OK) return st;
+    PushState *s = (PushState *)g->push_exec;
+    if (!s) {
+        st = alloc_state(g, &s);
+        if (st != MM_OK) return st;
+        g->push_exec = s;
+    }
+    // One pinned upload of control block + seeds.  The previous call on this
+    // graph synchronised its stream before returning, so the staging buffer is free.
+    Ctl *ctl = reinterpret_cast<Ctl *>(s->host_stage);
+    std::memset(ctl, 0, kCtlBytes);
+    ctl->match = d_match;
+    ctl->barrier = barrier;
+    ctl->cap = max_rounds_of(type);
+    ctl->maximal = is_maximal(type) ? 1 : 0;
+    ctl->nseeds = nseeds < 256 ? nseeds : 256;
+    std::memcpy(s->host_stage + kCtlBytes, seeds, sizeof(uint32_t) * ctl->nseeds);
+    MM_CUDA_TRY(cudaMemcpyAsync(s->ctl, s->host_stage, kCtlBytes + sizeof(uint32_t) * ctl->nseeds,
+                                cudaMemcpyHostToDevice, stream),
+                "control block");
+    *out = s;
+    return MM_OK;
+}
+
+mm_status end_call(mm_graph *g, PushState *s, int nseeds, int *rounds_out, long long *stats, int stats_rounds,
+                   cudaStream_t stream)
+{
+    MM_CUDA_TRY(cudaMemcpyAsync(s->host_back, s->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, stream), "control read");
+    if (stats && stats_rounds > 0)
+        MM_CUDA_TRY(cudaMemcpyAsync(stats, s->stats,
+                                    sizeof(long long) * MM_STATS_COLS *
+                                        (size_t)(stats_rounds < kMaxRounds ? stats_rounds : kMaxRounds),
+                                    cudaMemcpyDeviceToHost, stream),
+                    "stats read");
+    MM_CUDA_TRY(cudaStreamSynchronize(stream), "round loop");
+    Ctl out;
+    std::memcpy(&out, s->host_back, sizeof out);
+    if (out.status == 2) {
+        set_error("mm_match: a bounded device wait gave up (staged copy did not complete)");
+        return MM_ERR_DEVICE;
+    }
+    if (out.status == 1 || out.rounds > nseeds) {
+        set_error("mm_match: fewer seeds than rounds");
+        return MM_ERR_SEEDS;
+    }
+    *rounds_out = out.rounds;
+    return MM_OK;
+}
+
+template <bool kW>
+mm_status stepped_rounds(mm_graph *g, PushState *s, int *rounds_done, float *ms_kernels, int cap_rounds,
+                         cudaStream_t stream)
+{
+    Params p = make_params(g, s, kW, false, 0);
+    const int blocks_init = grid_for(g->n, kTileItems, s->blocks_b);
+    cudaEvent_t ev[4];
+    for (int i = 0; i < 4; ++i) MM_CUDA_TRY(cudaEventCreate(&ev[i]), "event create");
+    mm_status st = MM_OK;
+    k_init<false><<<blocks_init, kBlockT, 0, stream>>>(p);
+    int r = 0;
+    for (;; ++r) {
+        cudaEventRecord(ev[0], stream);
+        k_phase_a_short<kW, false><<<s->blocks_a, kBlockA, 0, stream>>>(p);
+        cudaEventRecord(ev[1], stream);
+        k_phase_a_stream<kW, false><<<s->blocks_stream, kWarpsStream * 32, s->stream_smem, stream>>>(p);
+        cudaEventRecord(ev[2], stream);
+        k_phase_b<kW, false><<<s->blocks_b, kBlockT, 0, stream>>>(p);
+        cudaEventRecord(ev[3], stream);
+        int cont = 0;
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&cont, &s->ctl->cont, sizeof(int), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) {
+            st = cuda_fail(e, "stepped round");
+            break;
+        }
+        if (r < cap_rounds && ms_kernels) {
+            for (int k = 0; k < 3; ++k) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+                ms_kernels[(size_t)r * MM_PROFILE_KERNELS + k] = ms;
+            }
+            ms_kernels[(size_t)r * MM_PROFILE_KERNELS + 3] = 0.f;
+        }
+        if (!cont) {
+            ++r;
+            break;
+        }
+    }
+    if (st == MM_OK) {
+        cudaEventRecord(ev[0], stream);
+        k_tail<kW, false><<<1, kTailThreads, 0, stream>>>(p);
+        cudaEventRecord(ev[1], stream);
+        k_finish<<<grid_for(g->n, kBlockB, s->blocks_b), kBlockB, 0, stream>>>(p);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaEventSynchronize(ev[1]);
+        if (e != cudaSuccess) {
+            st = cuda_fail(e, "tail / finish");
+        } else if (r < cap_rounds && ms_kernels) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev[0], ev[1]);
+            for (int k = 0; k < MM_PROFILE_KERNELS; ++k) ms_kernels[(size_t)r * MM_PROFILE_KERNELS + k] = 0.f;
+            ms_kernels[(size_t)r * MM_PROFILE_KERNELS + 3] = ms;
+        }
+    }
+    for (int i = 0; i < 4; ++i) cudaEventDestroy(ev[i]);
+    *rounds_done = r;
+    return st;
+}
+
 }  // namespace
 
 mm_status push_prepare(mm_graph *g, int weighted, cudaStream_t stream)
@@ -725,52 +1599,58 @@ mm_status push_prepare(mm_graph *g, int weighted, cudaStream_t stream)
     const int n = g->n;
     if (n == 0) return MM_OK;
 
-    // Degrees, contiguity, slot offsets.
-    PrepInfo *d_info = nullptr;
-    long long *d_deg = nullptr;
-    MM_CUDA_TRY(cudaMalloc(&d_info, sizeof(PrepInfo)), "prep info");
-    MM_CUDA_TRY(cudaMemsetAsync(d_info, 0, sizeof(PrepInfo), stream), "prep info clear");
-    cudaError_t e = cudaMalloc(&d_deg, sizeof(long long) * (size_t)n);
-    if (e != cudaSuccess) {
-        cudaFree(d_info);
-        return cuda_fail(e, "prep degrees");
-    }
-    k_scan_ranges<<<grid_for(n, 256, 148 * 8), 256, 0, stream>>>(g->d_ranges, n, g->nnz, d_info, d_deg);
-    PrepInfo info;
-    e = cudaMemcpyAsync(&info, d_info, sizeof info, cudaMemcpyDeviceToHost, stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-    cudaFree(d_info);
-    if (e != cudaSuccess) {
-        cudaFree(d_deg);
-        return cuda_fail(e, "prep scan");
-    }
-    const long long S = (long long)info.sum_deg;
-    g->sum_degree = S;
-    g->max_degree = (long long)info.max_deg;
-    g->contiguous = info.noncontig == 0;
-    if (S >= (1ll << 31) - 1) {
-        cudaFree(d_deg);
-        set_error("push: more than 2^31 - 2 adjacency slots are not supported");
-        return MM_ERR_UNSUPPORTED;
-    }
-    if (!g->contiguous && !g->d_slot_off) {
-        e = cudaMalloc(&g->d_slot_off, sizeof(long long) * (size_t)n);
-        void *tmp = nullptr;
-        size_t tmp_bytes = 0;
-        if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_deg, g->d_slot_off, n, stream);
-        if (e == cudaSuccess) e = cudaMalloc(&tmp, tmp_bytes);
-        if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, d_deg, g->d_slot_off, n, stream);
+    // Degrees, classes, contiguity, slot offsets.
+    if (!g->scanned) {
+        PrepInfo *d_info = nullptr;
+        long long *d_deg = nullptr;
+        MM_CUDA_TRY(cudaMalloc(&d_info, sizeof(PrepInfo)), "prep info");
+        MM_CUDA_TRY(cudaMemsetAsync(d_info, 0, sizeof(PrepInfo), stream), "prep info clear");
+        cudaError_t e = cudaMalloc(&d_deg, sizeof(long long) * (size_t)n);
+        if (e != cudaSuccess) {
+            cudaFree(d_info);
+            return cuda_fail(e, "prep degrees");
+        }
+        k_scan_ranges<<<grid_for(n, 256, 148 * 8), 256, 0, stream>>>(g->d_ranges, n, g->nnz, d_info, d_deg);
+        PrepInfo info;
+        e = cudaMemcpyAsync(&info, d_info, sizeof info, cudaMemcpyDeviceToHost, stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-        cudaFree(tmp);
+        cudaFree(d_info);
         if (e != cudaSuccess) {
             cudaFree(d_deg);
-            return cuda_fail(e, "slot offsets");
+            return cuda_fail(e, "prep scan");
         }
+        g->sum_degree = (long long)info.sum_deg;
+        g->max_degree = (long long)info.max_deg;
+        g->short_count = (long long)info.short_count;
+        g->long_count = (long long)info.long_count;
+        g->long_entries = (long long)info.long_entries;
+        g->contiguous = info.noncontig == 0;
+        if (g->sum_degree >= (1ll << 31) - 1) {
+            cudaFree(d_deg);
+            set_error("push: more than 2^31 - 2 adjacency slots are not supported");
+            return MM_ERR_UNSUPPORTED;
+        }
+        if (!g->contiguous) {
+            e = cudaMalloc(&g->d_slot_off, sizeof(long long) * (size_t)n);
+            void *tmp = nullptr;
+            size_t tmp_bytes = 0;
+            if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_deg, g->d_slot_off, n, stream);
+            if (e == cudaSuccess) e = cudaMalloc(&tmp, tmp_bytes);
+            if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, d_deg, g->d_slot_off, n, stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+            cudaFree(tmp);
+            if (e != cudaSuccess) {
+                cudaFree(d_deg);
+                return cuda_fail(e, "slot offsets");
+            }
+        }
+        cudaFree(d_deg);
+        g->scanned = true;
     }
-    cudaFree(d_deg);
+    const long long S = g->sum_degree;
 
     unsigned long long *revkey = nullptr;
-    e = cudaMalloc(&revkey, sizeof(unsigned long long) * (size_t)(S > 0 ? S : 1));
+    cudaError_t e = cudaMalloc(&revkey, sizeof(unsigned long long) * (size_t)(S > 0 ? S : 1));
     if (e != cudaSuccess) return cuda_fail(e, "reverse keys");
     if (S == 0) {
         g->d_revkey[wi] = revkey;
@@ -824,24 +1704,18 @@ mm_status push_match(mm_graph *g, int type, uint32_t barrier, const uint32_t *se
                      int *rounds_out, long long *stats, int stats_rounds, cudaStream_t stream)
 {
     const bool weighted = is_weighted(type), maximal = is_maximal(type);
-    const int cap = max_rounds_of(type);
     if (g->n == 0) {
         // The reference still runs (and draws a seed for) its first round.
-        *rounds_out = maximal ? 1 : cap;
+        *rounds_out = maximal ? 1 : max_rounds_of(type);
         if (nseeds < *rounds_out) {
             set_error("mm_match: fewer seeds than rounds");
             return MM_ERR_SEEDS;
         }
         return MM_OK;
     }
-    mm_status st = push_prepare(g, weighted, stream);
+    PushState *s = nullptr;
+    mm_status st = begin_call(g, type, barrier, seeds, nseeds, d_match, stream, &s);
     if (st != MM_OK) return st;
-    PushState *s = (PushState *)g->push_exec;
-    if (!s) {
-        st = alloc_state(g, &s);
-        if (st != MM_OK) return st;
-        g->push_exec = s;
-    }
     const bool want_stats = stats != nullptr;
     Plan *plan = nullptr;
     for (int i = 0; i < s->nplans; ++i)
@@ -859,148 +1733,37 @@ mm_status push_match(mm_graph *g, int type, uint32_t barrier, const uint32_t *se
         plan->stats = want_stats;
         ++s->nplans;
     }
-    if (nseeds < 1) {
-        set_error("mm_match: no seeds");
-        return MM_ERR_SEEDS;
-    }
-    Ctl ctl;
-    std::memset(&ctl, 0, sizeof ctl);
-    ctl.match = d_match;
-    ctl.barrier = barrier;
-    ctl.cap = cap;
-    ctl.maximal = maximal ? 1 : 0;
-    ctl.nseeds = nseeds < 256 ? nseeds : 256;
-    const int nup = ctl.nseeds;
-    MM_CUDA_TRY(cudaMemcpyAsync(s->seeds, seeds, sizeof(uint32_t) * nup, cudaMemcpyHostToDevice, stream), "seeds");
-    MM_CUDA_TRY(cudaMemcpyAsync(s->ctl, &ctl, sizeof ctl, cudaMemcpyHostToDevice, stream), "control block");
     if (want_stats)
         MM_CUDA_TRY(cudaMemsetAsync(s->stats, 0, sizeof(unsigned long long) * kMaxRounds * MM_STATS_COLS, stream),
                     "stats clear");
     MM_CUDA_TRY(cudaGraphLaunch(plan->exec, stream), "round loop launch");
-    Ctl out;
-    MM_CUDA_TRY(cudaMemcpyAsync(&out, s->ctl, sizeof out, cudaMemcpyDeviceToHost, stream), "control read");
-    if (want_stats && stats_rounds > 0)
-        MM_CUDA_TRY(cudaMemcpyAsync(stats, s->stats, sizeof(long long) * MM_STATS_COLS *
-                                                         (size_t)(stats_rounds < kMaxRounds ? stats_rounds : kMaxRounds),
-                                    cudaMemcpyDeviceToHost, stream),
-                    "stats read");
-    MM_CUDA_TRY(cudaStreamSynchronize(stream), "round loop");
-    if (out.status == 1 || out.rounds > nseeds) {
-        set_error("mm_match: fewer seeds than rounds");
-        return MM_ERR_SEEDS;
-    }
-    *rounds_out = out.rounds;
-    return MM_OK;
+    return end_call(g, s, nseeds, rounds_out, stats, stats_rounds, stream);
 }
-
-namespace {
-
-template <bool kW>
-mm_status stepped_rounds(mm_graph *g, PushState *s, int *rounds_done, float *ms_a, float *ms_b, int cap_rounds,
-                         cudaStream_t stream)
-{
-    Params p = make_params(g, s, kW, false, 0);
-    const int blocks_init = grid_for(g->n, kBlockB, s->blocks_b);
-    cudaEvent_t ev[3];
-    for (int i = 0; i < 3; ++i) MM_CUDA_TRY(cudaEventCreate(&ev[i]), "event create");
-    mm_status st = MM_OK;
-    k_init<false><<<blocks_init, kBlockB, 0, stream>>>(p);
-    int r = 0;
-    for (;; ++r) {
-        cudaEventRecord(ev[0], stream);
-        k_phase_a<kW, false><<<s->blocks_a, kBlockA, 0, stream>>>(p);
-        cudaEventRecord(ev[1], stream);
-        k_phase_b<kW, false><<<s->blocks_b, kBlockB, 0, stream>>>(p);
-        cudaEventRecord(ev[2], stream);
-        int cont = 0;
-        cudaError_t e = cudaMemcpyAsync(&cont, &s->ctl->cont, sizeof(int), cudaMemcpyDeviceToHost, stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-        if (e != cudaSuccess) {
-            st = cuda_fail(e, "stepped round");
-            break;
-        }
-        float a = 0.f, b = 0.f;
-        cudaEventElapsedTime(&a, ev[0], ev[1]);
-        cudaEventElapsedTime(&b, ev[1], ev[2]);
-        if (r < cap_rounds) {
-            if (ms_a) ms_a[r] = a;
-            if (ms_b) ms_b[r] = b;
-        }
-        if (!cont) {
-            ++r;
-            break;
-        }
-    }
-    if (st == MM_OK) {
-        k_finish<<<grid_for(g->n, kBlockB, s->blocks_b), kBlockB, 0, stream>>>(p);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) st = cuda_fail(e, "finish");
-    }
-    for (int i = 0; i < 3; ++i) cudaEventDestroy(ev[i]);
-    *rounds_done = r;
-    return st;
-}
-
-}  // namespace
 
 // Same kernels as push_match, launched one by one from the host with CUDA
 // events around each phase, so the duration of every phase-A and phase-B
 // launch can be read.  For measurement only (it synchronises every round).
 mm_status push_profile(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds, int *d_match,
-                       int *rounds_out, float *ms_a, float *ms_b, int cap_rounds, int *launched,
-                       cudaStream_t stream)
+                       int *rounds_out, float *ms_kernels, int cap_rounds, int *launched, cudaStream_t stream)
 {
-    const bool weighted = is_weighted(type), maximal = is_maximal(type);
-    if (g->n == 0 || nseeds < 1) return push_match(g, type, barrier, seeds, nseeds, d_match, rounds_out, nullptr, 0, stream);
-    mm_status st = push_prepare(g, weighted, stream);
+    if (g->n == 0) return push_match(g, type, barrier, seeds, nseeds, d_match, rounds_out, nullptr, 0, stream);
+    PushState *s = nullptr;
+    mm_status st = begin_call(g, type, barrier, seeds, nseeds, d_match, stream, &s);
     if (st != MM_OK) return st;
-    PushState *s = (PushState *)g->push_exec;
-    if (!s) {
-        st = alloc_state(g, &s);
-        if (st != MM_OK) return st;
-        g->push_exec = s;
-    }
-    Ctl ctl;
-    std::memset(&ctl, 0, sizeof ctl);
-    ctl.match = d_match;
-    ctl.barrier = barrier;
-    ctl.cap = max_rounds_of(type);
-    ctl.maximal = maximal ? 1 : 0;
-    ctl.nseeds = nseeds < 256 ? nseeds : 256;
-    MM_CUDA_TRY(cudaMemcpyAsync(s->seeds, seeds, sizeof(uint32_t) * ctl.nseeds, cudaMemcpyHostToDevice, stream), "seeds");
-    MM_CUDA_TRY(cudaMemcpyAsync(s->ctl, &ctl, sizeof ctl, cudaMemcpyHostToDevice, stream), "control block");
     int executed = 0;
-    st = weighted ? stepped_rounds<true>(g, s, &executed, ms_a, ms_b, cap_rounds, stream)
-                  : stepped_rounds<false>(g, s, &executed, ms_a, ms_b, cap_rounds, stream);
+    st = is_weighted(type) ? stepped_rounds<true>(g, s, &executed, ms_kernels, cap_rounds, stream)
+                           : stepped_rounds<false>(g, s, &executed, ms_kernels, cap_rounds, stream);
     if (st != MM_OK) return st;
-    Ctl out;
-    MM_CUDA_TRY(cudaMemcpyAsync(&out, s->ctl, sizeof out, cudaMemcpyDeviceToHost, stream), "control read");
-    MM_CUDA_TRY(cudaStreamSynchronize(stream), "profile");
-    if (out.status == 1 || out.rounds > nseeds) {
-        set_error("mm_match: fewer seeds than rounds");
-        return MM_ERR_SEEDS;
-    }
-    *rounds_out = out.rounds;
-    if (launched) *launched = 2 + 2 * executed;
-    return MM_OK;
+    st = end_call(g, s, nseeds, rounds_out, nullptr, 0, stream);
+    if (st == MM_OK && launched) *launched = 3 + 3 * executed;  // init, rounds, tail, finish
+    return st;
 }
 
 void push_release(mm_graph *g)
 {
     PushState *s = (PushState *)g->push_exec;
     if (s) {
-        for (int i = 0; i < s->nplans; ++i) {
-            if (s->plans[i].exec) cudaGraphExecDestroy(s->plans[i].exec);
-            if (s->plans[i].graph) cudaGraphDestroy(s->plans[i].graph);
-        }
-        cudaFree(s->col);
-        cudaFree(s->req);
-        cudaFree(s->best);
-        cudaFree(s->lists);
-        cudaFree(s->seeds);
-        cudaFree(s->ctl);
-        cudaFree(s->stats);
-        delete s;
+        free_state(s);
         g->push_exec = nullptr;
     }
     for (int i = 0; i < 2; ++i) {

@@ -131,6 +131,42 @@ def test_long_lists_and_hubs_match_oracle(mm, orc, torch_cuda):
                     assert got_rounds == rounds and np.array_equal(got, want), (t, seed, path)
 
 
+def test_degree_class_boundaries_non_contiguous(mm, orc, torch_cuda):
+    """Lists of exactly 32/33/2048/2049/4096/4097 entries (the scan's class and
+    chunk edges), stored out of vertex order with gaps between lists."""
+    rng = np.random.default_rng(17)
+    n = 9000
+    lists = [[] for _ in range(n)]
+    hubs = {0: 32, 1: 33, 2: 2048, 3: 2049, 4: 4096, 5: 4097, 6: 6144}
+    for h, d in hubs.items():
+        for v in rng.choice(np.arange(10, n), size=d, replace=False):
+            lists[h].append(int(v))
+            lists[int(v)].append(h)
+    for _ in range(20000):
+        u, v = int(rng.integers(10, n)), int(rng.integers(10, n))
+        if u != v:
+            lists[u].append(v)
+            lists[v].append(u)
+    order = rng.permutation(n)
+    ranges = np.zeros((n, 2), np.int64)
+    nbrs = []
+    for v in order:
+        nbrs += [int(x) for x in rng.integers(0, n, int(rng.integers(0, 3)))]  # gap
+        b = len(nbrs)
+        nbrs += lists[v]
+        ranges[v] = (b, len(nbrs))
+    nbrs = np.array(nbrs, np.int32)
+    wts = (rng.integers(1, 5, len(nbrs)) / 4).astype(np.float32)
+    g = SmallGraph(n, ranges, nbrs, wts)
+    with mm.DeviceGraph(g, device=0) as dg:
+        for seed in (1, 2, 3):
+            seeds = orc.rand_seeds(seed, 256)
+            for t in mm.TYPES:
+                want, rounds, _ = orc.match(g, t, seeds, BARRIER)
+                got, got_rounds = gpu_match(mm, torch_cuda, g, t, seeds, BARRIER, 2, dg=dg)
+                assert got_rounds == rounds and np.array_equal(got, want), (t, seed)
+
+
 @pytest.mark.parametrize("path", [2, 1])
 def test_round_counters_match_oracle(mm, orc, torch_cuda, path):
     cols = [(0, 0), (1, 1), (2, 2), (3, 3), (4, 4), (5, 5), (6, 6), (7, 7)]  # (mm, oracle) column pairs
