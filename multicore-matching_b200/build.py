@@ -74,7 +74,10 @@ def build_mtc(verbose: bool = False) -> Path:
         return out
     libmm = PKG / "libmmatch.so"
     if _newer(out, srcs + _headers() + [libmm]):
-        _run([CXX, *CXX_FLAGS, "-fvisibility=default", "-shared", "-o", out, *srcs,
+        # C++14: Graph::random_shuffle draws its permutation with std::random_shuffle
+        # (removed in C++17), exactly as the reference does
+        flags = [f for f in CXX_FLAGS if not f.startswith("-std=")] + ["-std=c++14"]
+        _run([CXX, *flags, "-fvisibility=default", "-shared", "-o", out, *srcs,
               f"-L{PKG}", "-lmmatch", f"-Wl,-rpath,$ORIGIN",
               "-L/usr/local/cuda/lib64", "-lcudart"], verbose)
     return out

@@ -62,6 +62,10 @@ _REF_SIGS = {
     "mmref_run": (_I, [_I, _I, _P, _LL, _P, _P, _U, _U, _I, _P, ctypes.POINTER(ctypes.c_double),
                        ctypes.POINTER(_U)]),
     "mmref_check": (_I, [_I, _P, _LL, _P, _P, _P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_LL)]),
+    "mmref_read": (_I, [ctypes.c_char_p, _I, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_LL), _P, _P,
+                        _P]),
+    "mmref_cli": (_I, [ctypes.c_char_p, _I, _I, _U, _U, _I, _I, _P, ctypes.POINTER(_U)]),
+    "mmref_shuffle": (_I, [ctypes.c_char_p, _I, _U, _I, _P, _P, ctypes.POINTER(_U)]),
 }
 
 
@@ -154,3 +158,57 @@ def ref_check(g, m: np.ndarray):
     ok = ref_lib().mmref_check(g.n, _p(ranges), g.nnz, _p(nbrs), _p(w), _p(m), ctypes.byref(wt),
                                ctypes.byref(sz))
     return bool(ok), wt.value, sz.value
+
+
+def _is_mtx(path) -> int:
+    return 1 if str(path).endswith(".mtx") else 0
+
+
+def ref_read(path):
+    """The reference's Graph::readMETIS / readMatrixMarket (src/graph.cu:86-511) on `path`
+    (MatrixMarket when it ends in .mtx).  Returns (n, nrEdges, ranges[n,2], nbrs, weights)
+    or None when the reader threw."""
+    n, e, nnz = _I(0), _I(0), _LL(0)
+    p = str(path).encode()
+    rc = ref_lib().mmref_read(p, _is_mtx(path), ctypes.byref(n), ctypes.byref(e), ctypes.byref(nnz), None, None, None)
+    if rc == 2:
+        return None
+    if rc != 0:
+        raise OSError(f"cannot open {path}")
+    ranges = np.zeros((n.value, 2), dtype=np.int32)
+    nbrs = np.zeros(nnz.value, dtype=np.int32)
+    w = np.zeros(nnz.value, dtype=np.float32)
+    ref_lib().mmref_read(p, _is_mtx(path), ctypes.byref(n), ctypes.byref(e), ctypes.byref(nnz), _p(ranges), _p(nbrs),
+                         _p(w))
+    return n.value, e.value, ranges, nbrs, w
+
+
+def ref_shuffle(path, seed: int, reps: int, n: int, nnz: int):
+    """srand(seed) and `reps` reference Graph::random_shuffle calls (src/graph.cu:513-548).
+    Returns (ranges[n,2], nbrs, next rand() value)."""
+    ranges = np.zeros((max(n, 1), 2), dtype=np.int32)
+    nbrs = np.zeros(max(nnz, 1), dtype=np.int32)
+    nxt = _U(0)
+    rc = ref_lib().mmref_shuffle(str(path).encode(), _is_mtx(path), seed, reps, _p(ranges), _p(nbrs),
+                                 ctypes.byref(nxt))
+    if rc != 0:
+        raise ValueError(f"reference shuffle failed ({rc})")
+    return ranges[:n], nbrs[:nnz], nxt.value
+
+
+# GPU type -> (reference TBB matcher, fixed-round build): the TBB matchers run the
+# same colour/request/respond/match rounds (src/matchtbb.cu) as the GPU types.
+GPU_TO_TBB = {6: (10, True), 7: (10, False), 8: (11, True), 9: (11, False)}
+
+
+def ref_cli(path, gpu_type: int, barrier: int, seed: int, shuffle: bool, reps: int, n: int):
+    """The reference CLI loop (bin/match.cpp:380-420) with the TBB matcher that equals
+    GPU type `gpu_type`.  Returns (matches int32[reps, n], next rand() value)."""
+    tbb, fixed = GPU_TO_TBB[gpu_type]
+    out = np.zeros((reps, max(n, 1)), dtype=np.int32)
+    nxt = _U(0)
+    rc = ref_lib(fixed).mmref_cli(str(path).encode(), _is_mtx(path), tbb, barrier, seed, int(shuffle), reps,
+                                  _p(out), ctypes.byref(nxt))
+    if rc != 0:
+        raise ValueError(f"reference CLI loop failed ({rc})")
+    return out[:, :n], nxt.value

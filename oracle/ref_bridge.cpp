@@ -15,6 +15,8 @@
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
+#include <string>
 #include <vector>
 
 #include "graph.h"
@@ -111,4 +113,102 @@ MMREF_API int mmref_check(int n, const int *ranges, long long nnz, const int *nb
     *weight = wt;
     *size = sz;
     return mtc::GraphMatching::testMatching(m, g) ? 1 : 0;
+}
+
+/*
+ * Read a graph file with the reference's own readers (graph.cu:86-511) and
+ * copy its CSR out.  Call with null arrays first to get the sizes.
+ */
+MMREF_API int mmref_read(const char *path, int is_mtx, int *n, int *edges, long long *nnz, int *ranges, int *nbrs,
+                         float *w)
+{
+    mtc::Graph g;
+    std::ifstream f(path);
+    if (!f.good()) return 1;
+    try {
+        if (is_mtx) g.readMatrixMarket(f);
+        else g.readMETIS(f);
+    } catch (std::exception &) {
+        return 2;
+    }
+    *n = g.nrVertices;
+    *edges = g.nrEdges;
+    *nnz = (long long)g.neighbours.size();
+    if (ranges)
+        for (int v = 0; v < g.nrVertices; ++v) {
+            ranges[2 * v] = g.neighbourRanges[v].x;
+            ranges[2 * v + 1] = g.neighbourRanges[v].y;
+        }
+    if (nbrs && !g.neighbours.empty()) std::memcpy(nbrs, g.neighbours.data(), sizeof(int) * g.neighbours.size());
+    if (w && !g.neighbourWeights.empty())
+        std::memcpy(w, g.neighbourWeights.data(), sizeof(float) * g.neighbourWeights.size());
+    return 0;
+}
+
+/*
+ * The reference CLI's per-type loop (bin/match.cpp:380-420) with one of its
+ * CPU/TBB matchers: read `path`, srand(seed), then `reps` times: optional
+ * Graph::random_shuffle, match.  out receives reps x n match arrays; returns
+ * the next rand() value through next_rand.
+ */
+MMREF_API int mmref_cli(const char *path, int is_mtx, int type, unsigned barrier, unsigned seed, int shuffle, int reps,
+                        int *out, unsigned *next_rand)
+{
+    mtc::Graph g;
+    std::ifstream f(path);
+    if (!f.good()) return 1;
+    try {
+        if (is_mtx) g.readMatrixMarket(f);
+        else g.readMETIS(f);
+    } catch (std::exception &) {
+        return 2;
+    }
+    mtc::Graph g2 = g;
+    srand(seed);
+    for (int k = 0; k < reps; ++k) {
+        if (shuffle) g2.random_shuffle();
+        mtc::GraphMatching *m = nullptr;
+        switch (type) {
+        case 0: m = new mtc::GraphMatchingCPURandom(g2); break;
+        case 4: m = new mtc::GraphMatchingCPUWeighted(g2); break;
+        case 10: m = new mtc::GraphMatchingTBBRandom(g2, barrier); break;
+        case 11: m = new mtc::GraphMatchingTBBWeighted(g2, barrier); break;
+        default: return 3;
+        }
+        std::vector<int> match = m->initialMatching();
+        cudaEvent_t t1 = nullptr, t2 = nullptr;
+        m->performMatching(match, t1, t2);
+        std::memcpy(out + (size_t)k * g.nrVertices, match.data(), sizeof(int) * (size_t)g.nrVertices);
+        delete m;
+    }
+    *next_rand = (unsigned)rand();
+    return 0;
+}
+
+/*
+ * srand(seed), then `reps` calls of the reference's Graph::random_shuffle
+ * (graph.cu:513-548) on the graph read from `path`.  ranges_out[2n] and
+ * nbrs_out[nnz] receive the final CSR; next_rand the next rand() value.
+ */
+MMREF_API int mmref_shuffle(const char *path, int is_mtx, unsigned seed, int reps, int *ranges_out, int *nbrs_out,
+                            unsigned *next_rand)
+{
+    mtc::Graph g;
+    std::ifstream f(path);
+    if (!f.good()) return 1;
+    try {
+        if (is_mtx) g.readMatrixMarket(f);
+        else g.readMETIS(f);
+    } catch (std::exception &) {
+        return 2;
+    }
+    srand(seed);
+    for (int k = 0; k < reps; ++k) g.random_shuffle();
+    for (int v = 0; v < g.nrVertices; ++v) {
+        ranges_out[2 * v] = g.neighbourRanges[v].x;
+        ranges_out[2 * v + 1] = g.neighbourRanges[v].y;
+    }
+    if (!g.neighbours.empty()) std::memcpy(nbrs_out, g.neighbours.data(), sizeof(int) * g.neighbours.size());
+    *next_rand = (unsigned)rand();
+    return 0;
 }

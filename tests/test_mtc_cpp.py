@@ -1,0 +1,272 @@
+"""The reference-compatible C++ classes (include/mtc/*.h, libmtc.so).
+
+tests/cpp/mtc_harness.cpp is compiled against the drop-in headers and driven
+the way the reference's CLI drives its own classes (bin/match.cpp:363-470).
+
+CPU: Graph::readMETIS / readMatrixMarket produce the same CSR, edge counts
+and exceptions as the reference's readers (src/graph.cu:86-511), and
+Graph::random_shuffle the same permutation and rand() consumption
+(src/graph.cu:513-548), checked against the reference's own graph.cu built
+into oracle/_ref.
+
+GPU: the CLI loop (srand, optional shuffle, construct, performMatching,
+testMatching, getWeight) gives the reference's matchings bit for bit and
+leaves rand() where the reference leaves it.
+"""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import has_gpu
+
+ROOT = Path(__file__).resolve().parent.parent
+PKG = ROOT / "multicore-matching_b200"
+BARRIER = 0x88B81733
+
+
+@pytest.fixture(scope="module")
+def harness(mm, tmp_path_factory):
+    mm.lib()
+    assert (PKG / "libmtc.so").exists(), "libmtc.so is not built (__graft_entry__.build())"
+    exe = tmp_path_factory.mktemp("harness") / "mtc_harness"
+    cmd = ["g++", "-O2", "-std=c++14", "-o", str(exe), str(ROOT / "tests" / "cpp" / "mtc_harness.cpp"),
+           f"-I{ROOT / 'include' / 'mtc'}", f"-I{ROOT / 'include'}", "-I/usr/local/cuda/include",
+           f"-L{PKG}", "-lmtc", "-lmmatch", "-L/usr/local/cuda/lib64", "-lcudart", f"-Wl,-rpath,{PKG}"]
+    subprocess.run(cmd, check=True)
+    return exe
+
+
+def run(exe, *args, check=True):
+    p = subprocess.run([str(exe), *map(str, args)], capture_output=True, text=True, timeout=600)
+    if check and p.returncode != 0:
+        raise AssertionError(f"harness {args[0]} failed ({p.returncode}): {p.stdout} {p.stderr}")
+    return p
+
+
+def read_dump(path: Path):
+    b = path.read_bytes()
+    n, edges = np.frombuffer(b, np.int32, 2)
+    nnz = int(np.frombuffer(b, np.int64, 1, 8)[0])
+    off = 16
+    ranges = np.frombuffer(b, np.int32, 2 * n, off).reshape(n, 2)
+    off += 8 * n
+    nbrs = np.frombuffer(b, np.int32, nnz, off)
+    off += 4 * nnz
+    w = np.frombuffer(b, np.float32, nnz, off)
+    return int(n), int(edges), ranges, nbrs, w
+
+
+# --------------------------------------------------------------------------- files
+
+def write_metis(path: Path, g, weights: bool, header_edges=None, comment=True, vertex_weights=0):
+    lines = ["% generated graph"] if comment else []
+    edges = header_edges if header_edges is not None else g.nnz // 2
+    fmt = (10 if vertex_weights else 0) + (1 if weights else 0)
+    head = f"{g.n} {edges}"
+    if fmt:
+        head += f" {fmt:03d}"
+        if vertex_weights > 1:
+            head += f" {vertex_weights}"
+    lines.append(head)
+    for v in range(g.n):
+        b, e = g.ranges[v]
+        parts = [str(1 + (v % 7))] * vertex_weights
+        for j in range(b, e):
+            parts.append(str(int(g.nbrs[j]) + 1))
+            if weights:
+                parts.append(f"{float(g.weights[j]):.9g}")
+        lines.append(" ".join(parts))
+    path.write_text("\n".join(lines) + "\n")
+
+
+def write_mtx(path: Path, g, field="real"):
+    rows = []
+    for v in range(g.n):
+        b, e = g.ranges[v]
+        for j in range(b, e):
+            u = int(g.nbrs[j])
+            if u < v:
+                if field == "pattern":
+                    rows.append(f"{v + 1} {u + 1}")
+                elif field == "integer":
+                    rows.append(f"{v + 1} {u + 1} {int(round(float(g.weights[j]) * 1000))}")
+                elif field == "complex":
+                    rows.append(f"{v + 1} {u + 1} {float(g.weights[j]):.9g} {-0.5 * float(g.weights[j]):.9g}")
+                else:
+                    rows.append(f"{v + 1} {u + 1} {float(g.weights[j]):.9g}")
+    # diagonal and upper entries are read and dropped by the reader
+    rows.insert(len(rows) // 2, "1 1 5.0" if field != "pattern" else "1 1")
+    head = [f"%%MatrixMarket matrix coordinate {field} symmetric", "% comment line",
+            f"{g.n} {g.n} {len(rows)}"]
+    path.write_text("\n".join(head + rows) + "\n")
+
+
+def small_graphs(mm):
+    return [("rgg", mm.Graph.rgg(3000, 9.0, seed=11)), ("grid", mm.Graph.grid(37, 41)),
+            ("rmat", mm.Graph.rmat(11, 8, seed=5)), ("er", mm.Graph.er(1500, 6.0, seed=2))]
+
+
+# --------------------------------------------------------------------------- CPU: readers
+
+def ref_or_skip(orc):
+    if not orc.ref_available():
+        pytest.skip("reference build (oracle/_ref) not present")
+
+
+def assert_same_read(harness, orc, path: Path, tmp_path: Path):
+    ref = orc.ref_read(path)
+    out = tmp_path / "dump.bin"
+    p = run(harness, "dump", path, out, check=False)
+    if ref is None:
+        assert p.returncode == 4 and json.loads(p.stdout)["read_error"], p.stdout
+        return None
+    assert p.returncode == 0, p.stderr
+    n, edges, ranges, nbrs, w = read_dump(out)
+    rn, redges, rranges, rnbrs, rw = ref
+    assert (n, edges) == (rn, redges)
+    np.testing.assert_array_equal(ranges, rranges)
+    np.testing.assert_array_equal(nbrs, rnbrs)
+    np.testing.assert_array_equal(w.view(np.uint32), rw.view(np.uint32))
+    return n, edges, ranges, nbrs, w
+
+
+def test_metis_reader_matches_reference(mm, orc, harness, tmp_path):
+    ref_or_skip(orc)
+    for name, g in small_graphs(mm):
+        for weights in (False, True):
+            path = tmp_path / f"{name}_{int(weights)}.graph"
+            write_metis(path, g, weights)
+            got = assert_same_read(harness, orc, path, tmp_path)
+            assert got is not None and got[0] == g.n and got[1] == g.nnz // 2
+
+
+def test_metis_reader_edge_cases(mm, orc, harness, tmp_path):
+    ref_or_skip(orc)
+    cases = {
+        # self loops and repeated neighbours are dropped with a warning
+        "loops.graph": "4 4\n1 2 2 3\n1 3\n2 1 4\n3\n",
+        # wrong edge count in the header is corrected
+        "count.graph": "% c\n3 7\n2 3\n1\n1\n",
+        # vertex weights (fmt 10 and 11, ncon 2)
+        "vw.graph": "3 2 011 2\n5 6 2 0.5 3 0.25\n1 1 1 0.5\n2 2 1 0.25\n",
+        "vw1.graph": "3 2 10\n5 2 3\n1 1\n2 1\n",
+        # isolated vertices and trailing blank lines
+        "iso.graph": "5 1\n\n2\n1\n\n\n",
+        # invalid neighbour index -> exception
+        "bad.graph": "3 1\n2\n9\n\n",
+        # vertex weights given without the flag -> exception
+        "badvw.graph": "3 1 0 2\n2\n1\n\n",
+        # missing header -> exception
+        "nohead.graph": "% only a comment\n",
+        # empty graph
+        "empty.graph": "0 0\n",
+    }
+    for fname, text in cases.items():
+        path = tmp_path / fname
+        path.write_text(text)
+        assert_same_read(harness, orc, path, tmp_path)
+
+
+def test_matrix_market_reader_matches_reference(mm, orc, harness, tmp_path):
+    ref_or_skip(orc)
+    for name, g in small_graphs(mm)[:2]:
+        for field in ("real", "pattern", "integer", "complex"):
+            path = tmp_path / f"{name}_{field}.mtx"
+            write_mtx(path, g, field)
+            got = assert_same_read(harness, orc, path, tmp_path)
+            assert got is not None and got[1] == g.nnz // 2
+
+
+def test_matrix_market_edge_cases(orc, harness, tmp_path):
+    ref_or_skip(orc)
+    cases = {
+        "general.mtx": "%%MatrixMarket matrix coordinate real general\n3 3 2\n2 1 1.0\n3 2 1.0\n",
+        "nonsquare.mtx": "%%MatrixMarket matrix coordinate real symmetric\n3 4 1\n2 1 1.0\n",
+        "noheader.mtx": "3 3 1\n2 1 1.0\n",
+        "badindex.mtx": "%%MatrixMarket matrix coordinate real symmetric\n3 3 1\n4 1 1.0\n",
+        "skew.mtx": "%%MatrixMarket matrix coordinate real skew-symmetric\n3 3 2\n2 1 -2.5\n3 1 1.0\n",
+        "array.mtx": "%%MatrixMarket matrix array real symmetric\n3 3\n1\n2\n3\n4\n5\n6\n7\n8\n9\n",
+        "unknown_tag.mtx": "%%MatrixMarket matrix coordinate real symmetric fancy\n3 3 1\n2 1 1.0\n",
+        "zero.mtx": "%%MatrixMarket matrix coordinate real symmetric\n3 3 0\n",
+    }
+    for fname, text in cases.items():
+        path = tmp_path / fname
+        path.write_text(text)
+        assert_same_read(harness, orc, path, tmp_path)
+
+
+def test_random_shuffle_matches_reference(mm, orc, harness, tmp_path):
+    ref_or_skip(orc)
+    g = mm.Graph.rgg(2000, 8.0, seed=3)
+    path = tmp_path / "s.graph"
+    write_metis(path, g, True)
+    for seed, reps in ((12345, 1), (12345, 3), (7, 2)):
+        out = tmp_path / "sh.bin"
+        p = run(harness, "shuffle", path, seed, reps, out)
+        n, _, ranges, nbrs, _ = read_dump(out)
+        rranges, rnbrs, rnext = orc.ref_shuffle(path, seed, reps, g.n, g.nnz)
+        np.testing.assert_array_equal(ranges, rranges)
+        np.testing.assert_array_equal(nbrs, rnbrs)
+        assert json.loads(p.stdout)["next_rand"] == rnext
+
+
+# --------------------------------------------------------------------------- GPU: CLI loop
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not has_gpu(), reason="needs a GPU")
+@pytest.mark.parametrize("gtype", [6, 7, 8, 9])
+@pytest.mark.parametrize("shuffle", [False, True])
+def test_cli_loop_matches_reference(mm, orc, harness, tmp_path, gtype, shuffle):
+    g = mm.Graph.rgg(6000, 10.0, seed=21)
+    path = tmp_path / "g.graph"
+    write_metis(path, g, True)
+    reps = 3
+    out = tmp_path / "m.bin"
+    p = run(harness, "match", path, gtype, 12345, int(shuffle), reps, out)
+    res = json.loads(p.stdout)
+    got = np.fromfile(out, dtype=np.int32).reshape(reps, g.n)
+    assert all(r["valid"] for r in res["runs"])
+    if orc.ref_available():
+        want, nxt = orc.ref_cli(path, gtype, BARRIER, 12345, shuffle, reps, g.n)
+        np.testing.assert_array_equal(got, want)
+        assert res["next_rand"] == nxt
+    if not shuffle:
+        # every repetition sees the same graph and continues the same rand() stream
+        seeds = orc.rand_seeds(12345, 255 * reps + 1)
+        off = 0
+        for k in range(reps):
+            m, rounds, _ = orc.match(g, gtype, seeds[off:], BARRIER)
+            np.testing.assert_array_equal(got[k], m)
+            off += rounds
+        assert res["next_rand"] == int(seeds[off])
+        wt, sz = orc.weight(g, got[0])
+        assert res["runs"][0]["size"] == sz
+        assert abs(res["runs"][0]["weight"] - wt) <= 1e-9 * max(1.0, abs(wt))
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not has_gpu(), reason="needs a GPU")
+def test_cli_loop_matrix_market_and_empty(mm, orc, harness, tmp_path):
+    g = mm.Graph.grid(64, 50)
+    path = tmp_path / "g.mtx"
+    write_mtx(path, g, "real")
+    out = tmp_path / "m.bin"
+    p = run(harness, "match", path, 9, 777, 1, 2, out)
+    res = json.loads(p.stdout)
+    assert all(r["valid"] for r in res["runs"])
+    if orc.ref_available():
+        want, nxt = orc.ref_cli(path, 9, BARRIER, 777, True, 2, g.n)
+        np.testing.assert_array_equal(np.fromfile(out, dtype=np.int32).reshape(2, g.n), want)
+        assert res["next_rand"] == nxt
+    # a graph with vertices and no edges
+    path = tmp_path / "iso.graph"
+    path.write_text("5 0\n\n\n\n\n\n")
+    p = run(harness, "match", path, 7, 1, 0, 1, out)
+    res = json.loads(p.stdout)
+    assert res["runs"][0]["valid"] and res["runs"][0]["size"] == 0
