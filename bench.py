@@ -330,21 +330,40 @@ def main():
     lib = mm.lib()
     import ctypes
 
-    e2e_ms = []
+    e2e_ms, e2e_parts = [], []
     for i in range(args.e2e_steps + 1):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         h = ctypes.c_void_p()
         mm._check(lib.mm_graph_create(g.n, ranges_h.data_ptr(), g.nnz, nbrs_h.data_ptr(),
                                       None if w_h is None else w_h.data_ptr(), local, ctypes.byref(h)))
+        t1 = time.perf_counter()
         rr = ctypes.c_int()
         sd = np.ascontiguousarray(seeds)
         mm._check(lib.mm_match(h, t, BARRIER, sd.ctypes.data, len(sd), match_h.data_ptr(), ctypes.byref(rr), None))
+        t2 = time.perf_counter()
         lib.mm_graph_destroy(h)
-        dt = (time.perf_counter() - t0) * 1e3
+        t3 = time.perf_counter()
+        dt = (t3 - t0) * 1e3
         if i > 0:
             e2e_ms.append(dt)
+            e2e_parts.append(((t1 - t0) * 1e3, (t2 - t1) * 1e3, (t3 - t2) * 1e3))
     e2e = statistics.mean(e2e_ms)
+    e2e_split = [statistics.mean(x[k] for x in e2e_parts) for k in range(3)]
+    # where the first call's time goes: reverse-key build (mm_graph_prepare), first and second match
+    torch.cuda.synchronize()
+    h = ctypes.c_void_p()
+    mm._check(lib.mm_graph_create(g.n, ranges_h.data_ptr(), g.nnz, nbrs_h.data_ptr(),
+                                  None if w_h is None else w_h.data_ptr(), local, ctypes.byref(h)))
+    tp = [time.perf_counter()]
+    mm._check(lib.mm_graph_prepare(h, t))
+    tp.append(time.perf_counter())
+    for _ in range(2):
+        mm._check(lib.mm_match(h, t, BARRIER, sd.ctypes.data, len(sd), match_h.data_ptr(), ctypes.byref(rr), None))
+        tp.append(time.perf_counter())
+    lib.mm_graph_destroy(h)
+    e2e_detail = {"ms_prepare": (tp[1] - tp[0]) * 1e3, "ms_match_first": (tp[2] - tp[1]) * 1e3,
+                  "ms_match_again": (tp[3] - tp[2]) * 1e3}
     h2d = g.n * 8 + g.nnz * 4 + (g.nnz * 4 if weighted else 0) + 255 * 4
     d2h = g.n * 4
     e2e_value = edges * world / (e2e / 1e3)
@@ -367,13 +386,17 @@ def main():
                        "l2": "inputs > L2 (CSR > 1 GB) and a 512 MB L2 flush between steps"},
             "ms_to_maximal": ms, "edges_per_step": edges,
             "e2e": {"value": e2e_value, "unit": "edges/s", "ms_per_step": e2e, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+                    "d2h_bytes_per_step": d2h, "ms_create": e2e_split[0], "ms_first_match": e2e_split[1],
+                    "ms_destroy": e2e_split[2], **e2e_detail},
             "roofline": {"bound": "hbm", "kernel": dom,
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_kind": peak_kind,
                          "bytes_per_launch": float(dom_bytes.mean()), "launches": int(nr),
                          "ms_short_scan": float(ms_k[:, 0].sum()), "ms_staged_scan": float(ms_k[:, 1].sum()),
                          "ms_commit": float(ms_k[:, 2].sum()), "ms_tail": ms_tail,
+                         "per_round_ms": {"short": [round(float(x), 4) for x in ms_k[:, 0]],
+                                          "staged": [round(float(x), 4) for x in ms_k[:, 1]],
+                                          "commit": [round(float(x), 4) for x in ms_k[:, 2]]},
                          "reference_formula_gbs": work["reference_bytes"] / (ms / 1e3) / 1e9},
             "gpu_launches": gpu_launches,
             "clocks": clocks.summary(),

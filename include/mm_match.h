@@ -101,8 +101,19 @@ mm_status mm_graph_create_device(int n, const int *d_ranges, long long nnz, cons
  */
 mm_status mm_graph_prepare(mm_graph *g, int type);
 
-/* Free all device memory of g.  Replaces ~GraphMatchingGPU (src/matchgpu.cu:68-73, 117-121). */
+/*
+ * Free all device memory of g.  Replaces ~GraphMatchingGPU (src/matchgpu.cu:68-73, 117-121).
+ * Waits for the device to finish its work first.  The memory goes back to the
+ * library's per-device pool, where the next graph reuses it.
+ */
 void mm_graph_destroy(mm_graph *g);
+
+/*
+ * Hand the pool's unused device memory on `device` back to the driver (no
+ * counterpart in the reference, whose objects cudaMalloc and cudaFree
+ * directly).  Live graphs keep theirs.
+ */
+mm_status mm_release_cached_memory(int device);
 
 int mm_graph_n(const mm_graph *g);
 long long mm_graph_nnz(const mm_graph *g);

@@ -70,6 +70,7 @@ _MM_SIGS = {
     "mm_graph_create": (_I, [_I, _P, _LL, _P, _P, _I, ctypes.POINTER(_P)]),
     "mm_graph_create_device": (_I, [_I, _P, _LL, _P, _P, ctypes.POINTER(_P)]),
     "mm_graph_prepare": (_I, [_P, _I]),
+    "mm_release_cached_memory": (_I, [_I]),
     "mm_graph_destroy": (None, [_P]),
     "mm_graph_n": (_I, [_P]),
     "mm_graph_nnz": (_LL, [_P]),

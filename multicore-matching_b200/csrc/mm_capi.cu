@@ -7,8 +7,10 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <mutex>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "mm_common.cuh"
 
@@ -26,6 +28,107 @@ mm_status cuda_fail(cudaError_t e, const char *what)
     set_error(std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
     if (e == cudaErrorMemoryAllocation) return MM_ERR_NOMEM;
     return MM_ERR_CUDA;
+}
+
+// ---- memory ----------------------------------------------------------------
+// Device buffers come from one stream-ordered pool per device whose release
+// threshold is unlimited: memory a destroyed graph returns stays mapped in the
+// pool and the next graph of similar size reuses it without a new mapping
+// (cudaMalloc / cudaFree of gigabytes cost tens to hundreds of milliseconds).
+// mm_release_cached_memory hands the unused part back to the driver.
+
+namespace {
+std::mutex g_pool_mu;
+constexpr int kMaxDevices = 256;
+cudaMemPool_t g_pools[kMaxDevices] = {};
+
+struct PinnedBlock {
+    void *ptr;
+    size_t bytes;
+};
+std::mutex g_pinned_mu;
+std::vector<PinnedBlock> g_pinned_free;
+}  // namespace
+
+static cudaError_t device_pool(int device, cudaMemPool_t *out)
+{
+    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (!g_pools[device]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t pool = nullptr;
+        cudaError_t e = cudaMemPoolCreate(&pool, &props);
+        if (e != cudaSuccess) return e;
+        uint64_t keep = ~0ull;
+        e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) {
+            cudaMemPoolDestroy(pool);
+            return e;
+        }
+        g_pools[device] = pool;
+    }
+    *out = g_pools[device];
+    return cudaSuccess;
+}
+
+cudaError_t dev_alloc(void **p, size_t bytes, cudaStream_t stream)
+{
+    *p = nullptr;
+    int device = -1;
+    cudaError_t e = cudaGetDevice(&device);
+    cudaMemPool_t pool = nullptr;
+    if (e == cudaSuccess) e = device_pool(device, &pool);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync(p, bytes ? bytes : 1, pool, stream);
+    return e;
+}
+
+void dev_free(void *p, cudaStream_t stream)
+{
+    if (p) cudaFreeAsync(p, stream);
+}
+
+cudaError_t pinned_get(void **p, size_t bytes)
+{
+    {
+        std::lock_guard<std::mutex> lock(g_pinned_mu);
+        for (size_t i = 0; i < g_pinned_free.size(); ++i)
+            if (g_pinned_free[i].bytes >= bytes) {
+                *p = g_pinned_free[i].ptr;
+                g_pinned_free.erase(g_pinned_free.begin() + (long)i);
+                return cudaSuccess;
+            }
+    }
+    const size_t rounded = (bytes + 4095) / 4096 * 4096;
+    return cudaHostAlloc(p, rounded, cudaHostAllocPortable);
+}
+
+void pinned_put(void *p, size_t bytes)
+{
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(g_pinned_mu);
+    g_pinned_free.push_back(PinnedBlock{p, (bytes + 4095) / 4096 * 4096});
+}
+
+mm_status release_cached(int device)
+{
+    cudaMemPool_t pool = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mu);
+        if (device >= 0 && device < kMaxDevices) pool = g_pools[device];
+    }
+    if (!pool) return MM_OK;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    MM_CUDA_TRY(cudaSetDevice(device), "set device");
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemPoolTrimTo(pool, 0);
+    if (prev >= 0) cudaSetDevice(prev);
+    if (e != cudaSuccess) return cuda_fail(e, "release cached memory");
+    return MM_OK;
 }
 
 mm_status ensure_scratch(mm_graph *g, size_t bytes)
@@ -78,12 +181,14 @@ void free_graph(mm_graph *g)
     int prev = -1;
     cudaGetDevice(&prev);
     cudaSetDevice(g->device);
+    cudaDeviceSynchronize();  // pooled frees are stream-ordered: let every stream finish with the graph
     push_release(g);
-    cudaFree(g->d_ranges);
-    cudaFree(g->d_nbrs);
-    cudaFree(g->d_w);
+    dev_free(g->d_ranges, 0);
+    dev_free(g->d_nbrs, 0);
+    dev_free(g->d_w, 0);
     cudaFree(g->scratch);
-    cudaFree(g->d_out);
+    dev_free(g->d_out, 0);
+    cudaStreamSynchronize(0);
     if (prev >= 0) cudaSetDevice(prev);
     delete g;
 }
@@ -98,7 +203,7 @@ mm_status finish_create(mm_graph *g, bool have_weights)
     }
     g->has_weights = have_weights;
     int *d_bad = nullptr;
-    MM_CUDA_TRY(cudaMalloc(&d_bad, sizeof(int)), "validation flag");
+    MM_CUDA_TRY(dev_alloc((void **)&d_bad, sizeof(int), 0), "validation flag");
     cudaError_t e = cudaMemset(d_bad, 0, sizeof(int));
     if (e == cudaSuccess && g->n > 0) {
         k_validate<<<grid_for((long long)g->n * 32, 256, 148 * 16), 256>>>(g->d_ranges, g->d_nbrs, g->n, g->nnz, d_bad);
@@ -106,7 +211,7 @@ mm_status finish_create(mm_graph *g, bool have_weights)
     }
     int bad = 0;
     if (e == cudaSuccess) e = cudaMemcpy(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost);
-    cudaFree(d_bad);
+    dev_free(d_bad, 0);
     if (e != cudaSuccess) return cuda_fail(e, "graph validation");
     if (bad & 1) {
         set_error("mm_graph_create: a neighbour range lies outside [0, nnz)");
@@ -150,9 +255,9 @@ mm_status create_common(int n, const int *ranges, long long nnz, const int *nbrs
     // that 16-byte vector loads starting at any in-range, 4-aligned slot stay inside.
     const size_t nv = (size_t)(n > 0 ? n : 1), ne = ((size_t)nnz + 3) / 4 * 4 + 4;
     const cudaMemcpyKind kind = from_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    cudaError_t e = cudaMalloc(&g->d_ranges, nv * sizeof(int2));
-    if (e == cudaSuccess) e = cudaMalloc(&g->d_nbrs, ne * sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc(&g->d_w, ne * sizeof(float));
+    cudaError_t e = dev_alloc((void **)&g->d_ranges, nv * sizeof(int2), 0);
+    if (e == cudaSuccess) e = dev_alloc((void **)&g->d_nbrs, ne * sizeof(int), 0);
+    if (e == cudaSuccess) e = dev_alloc((void **)&g->d_w, ne * sizeof(float), 0);
     if (e == cudaSuccess) e = cudaMemset(g->d_nbrs + nnz, 0, (ne - (size_t)nnz) * sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(g->d_w + nnz, 0, (ne - (size_t)nnz) * sizeof(float));
     if (e == cudaSuccess && n > 0) e = cudaMemcpy(g->d_ranges, ranges, (size_t)n * sizeof(int2), kind);
@@ -233,6 +338,8 @@ MM_API mm_status mm_graph_prepare(mm_graph *g, int type)
 
 MM_API void mm_graph_destroy(mm_graph *g) { free_graph(g); }
 
+MM_API mm_status mm_release_cached_memory(int device) { return release_cached(device); }
+
 MM_API int mm_graph_n(const mm_graph *g) { return g ? g->n : 0; }
 MM_API long long mm_graph_nnz(const mm_graph *g) { return g ? g->nnz : 0; }
 MM_API int mm_graph_weighted(const mm_graph *g) { return g && g->has_weights ? 1 : 0; }
@@ -270,7 +377,10 @@ MM_API mm_status mm_match(mm_graph *g, int type, uint32_t barrier, const uint32_
     if (s != MM_OK) return s;
     DeviceGuard guard(g->device);
     cudaStream_t st = (cudaStream_t)stream;
-    if (!g->d_out) MM_CUDA_TRY(cudaMalloc(&g->d_out, (size_t)(g->n > 0 ? g->n : 1) * sizeof(int)), "match buffer");
+    if (!g->d_out) {
+        MM_CUDA_TRY(dev_alloc((void **)&g->d_out, (size_t)(g->n > 0 ? g->n : 1) * sizeof(int), 0), "match buffer");
+        MM_CUDA_TRY(cudaStreamSynchronize(0), "match buffer");
+    }
     s = push_match(g, type, barrier, seeds, nseeds, g->d_out, rounds_out, nullptr, 0, st);
     if (s == MM_OK && g->n > 0) {
         cudaError_t e = cudaMemcpyAsync(match_out, g->d_out, (size_t)g->n * sizeof(int), cudaMemcpyDeviceToHost, st);

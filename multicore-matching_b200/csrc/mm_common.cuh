@@ -111,6 +111,16 @@ mm_status cuda_fail(cudaError_t e, const char *what);
         if (mm_e_ != cudaSuccess) return mm::cuda_fail(mm_e_, what); \
     } while (0)
 
+// Pooled device memory (one stream-ordered pool per device, never trimmed
+// unless mm_release_cached_memory asks): allocation and free are ordered on
+// `stream`; a buffer used on other streams needs that stream synchronised first.
+cudaError_t dev_alloc(void **p, size_t bytes, cudaStream_t stream);
+void dev_free(void *p, cudaStream_t stream);
+// Small page-locked host blocks, recycled process-wide.
+cudaError_t pinned_get(void **p, size_t bytes);
+void pinned_put(void *p, size_t bytes);
+mm_status release_cached(int device);
+
 // Ensure g->scratch holds at least `bytes`; returns MM_OK or an error.
 mm_status ensure_scratch(mm_graph *g, size_t bytes);
 

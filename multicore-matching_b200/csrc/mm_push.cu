@@ -1239,6 +1239,127 @@ __global__ void k_pair_groups(const unsigned long long *keys, const int *vals, l
     }
 }
 
+// ---- reverse keys from sorted lists ----------------------------------------
+// When every neighbour list is sorted, the entries of u that point back at v
+// form one run in u's list, found by binary search.  Of the two entries of a
+// pair {v, u} only the one whose partner list is shorter searches (ties by
+// id): it finds the run of entries pointing back in the partner's list, stores
+// the best of their keys in its own slot (pull) and max-combines its own key
+// into the slots of that run (push), which nobody else writes.  Each pair thus
+// costs one search in its shorter list; hub lists are never searched by their
+// many neighbours.  Slots are cut into chunks of kRevChunk; k_chunk_owner
+// finds the vertex owning each chunk's first slot, k_revkey_sorted resolves
+// the owner of every slot in shared memory and checks sortedness on the way
+// (any descending neighbour pair sets *unsorted and the pair-sort build runs).
+// revkey must be zero on entry.
+constexpr int kRevChunk = 2048;
+constexpr int kRevThreads = 256;
+
+__device__ __forceinline__ long long slot_prefix(const int2 *ranges, int contiguous, const long long *slot_off,
+                                                 long long v)
+{
+    return contiguous ? (long long)ranges[v].x : slot_off[v];
+}
+
+// Owner of slot s: the largest v with prefix(v) <= s.
+__device__ __forceinline__ int owner_of(const int2 *ranges, int contiguous, const long long *slot_off, int lo, int hi,
+                                        long long s)
+{
+    while (lo < hi) {
+        const int mid = (int)(((long long)lo + hi + 1) >> 1);
+        if (slot_prefix(ranges, contiguous, slot_off, mid) <= s) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void k_chunk_owner(const int2 *ranges, int n, int contiguous, const long long *slot_off, long long S,
+                              int *chunk_v)
+{
+    const long long chunks = (S + kRevChunk - 1) / kRevChunk;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c <= chunks;
+         c += (long long)gridDim.x * blockDim.x) {
+        const long long s = c * kRevChunk < S ? c * kRevChunk : S - 1;
+        chunk_v[c] = owner_of(ranges, contiguous, slot_off, 0, n - 1, s);
+    }
+}
+
+// Key red `owner` gives its entry at absolute position q (0: never picked).
+template <bool kW>
+__device__ __forceinline__ unsigned long long entry_red_key(const float *w, int q)
+{
+    if (kW) {
+        const float x = __ldg(w + q);
+        return x > -1.0f ? (((unsigned long long)weight_order(x) << 32) | (uint32_t)~q) : 0ull;
+    }
+    return (unsigned long long)(uint32_t)~q;
+}
+
+template <bool kW>
+__global__ void __launch_bounds__(kRevThreads) k_revkey_sorted(const int2 *ranges, const int *nbrs, const float *w,
+                                                               int contiguous, const long long *slot_off, long long S,
+                                                               const int *chunk_v, unsigned long long *revkey,
+                                                               int *unsorted)
+{
+    constexpr int kCap = kRevChunk + 1;
+    __shared__ int pre[kCap];  // prefix(v0 + i) - chunk start
+    __shared__ int bad;
+    if (threadIdx.x == 0) bad = 0;
+    const long long chunks = (S + kRevChunk - 1) / kRevChunk;
+    for (long long c = blockIdx.x; c < chunks; c += gridDim.x) {
+        const long long s0 = c * kRevChunk;
+        const int v0 = chunk_v[c], v1 = chunk_v[c + 1];
+        const int cnt = v1 - v0 + 1;
+        const bool in_smem = cnt <= kCap;
+        __syncthreads();
+        if (in_smem)
+            for (int i = threadIdx.x; i < cnt; i += kRevThreads)
+                pre[i] = (int)(slot_prefix(ranges, contiguous, slot_off, v0 + i) - s0);
+        __syncthreads();
+        for (int k = threadIdx.x; k < kRevChunk; k += kRevThreads) {
+            const long long s = s0 + k;
+            if (s >= S) break;
+            int v;
+            if (in_smem) {
+                int lo = 0, hi = cnt - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (pre[mid] <= k) lo = mid;
+                    else hi = mid - 1;
+                }
+                v = v0 + lo;
+            } else {
+                v = owner_of(ranges, contiguous, slot_off, v0, v1, s);
+            }
+            const int2 rv = ranges[v];
+            const int pos = contiguous ? (int)s : (int)(rv.x + (s - slot_off[v]));
+            const int u = nbrs[pos];
+            if (pos + 1 < rv.y && nbrs[pos + 1] < u) bad = 1;
+            if (u == v) continue;  // self-loops never carry a proposal
+            const int2 ru = ranges[u];
+            const int dv = degree_of(rv), du = degree_of(ru);
+            if (du > dv || (du == dv && u > v)) continue;  // u's entries search my list and push here
+            int lo = ru.x, hi = ru.x + du;  // first entry >= v in u's list
+            while (lo < hi) {
+                const int mid = (int)(((long long)lo + hi) >> 1);
+                if (__ldg(nbrs + mid) < v) lo = mid + 1;
+                else hi = mid;
+            }
+            const unsigned long long mine = entry_red_key<kW>(w, pos);
+            const long long su0 = contiguous ? 0ll : slot_off[u] - ru.x;  // slot of entry q of u: su0 + q
+            unsigned long long key = 0ull;
+            for (int q = lo; q < ru.x + du && __ldg(nbrs + q) == v; ++q) {
+                const unsigned long long kq = entry_red_key<kW>(w, q);
+                key = kq > key ? kq : key;
+                if (mine) atomicMax(revkey + su0 + q, mine);
+            }
+            if (key) revkey[s] = key;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && bad) atomicOr(unsorted, 1);
+}
+
 // Control block rounded to 256 bytes so the seeds that follow it stay aligned.
 constexpr size_t kCtlBytes = (sizeof(Ctl) + 255) / 256 * 256;
 
@@ -1283,17 +1404,18 @@ void free_state(PushState *s)
         if (s->plans[i].exec) cudaGraphExecDestroy(s->plans[i].exec);
         if (s->plans[i].graph) cudaGraphDestroy(s->plans[i].graph);
     }
-    cudaFree(s->col);
-    cudaFree(s->req);
-    cudaFree(s->best);
-    cudaFree(s->part_key);
-    cudaFree(s->part_cnt);
-    cudaFree(s->list_mem);
-    cudaFree(s->seg_mem);
-    cudaFree(s->ctl);
-    cudaFreeHost(s->host_stage);
-    cudaFreeHost(s->host_back);
-    cudaFree(s->stats);
+    // callers have synchronised the device (graph destroy or a failed set-up)
+    dev_free(s->col, 0);
+    dev_free(s->req, 0);
+    dev_free(s->best, 0);
+    dev_free(s->part_key, 0);
+    dev_free(s->part_cnt, 0);
+    dev_free(s->list_mem, 0);
+    dev_free(s->seg_mem, 0);
+    dev_free(s->ctl, 0);
+    pinned_put(s->host_stage, kCtlBytes + 256 * sizeof(uint32_t));
+    pinned_put(s->host_back, kCtlBytes);
+    dev_free(s->stats, 0);
     delete s;
 }
 
@@ -1311,20 +1433,24 @@ mm_status alloc_state(mm_graph *g, PushState **out)
     size_t per_parity = 0;
     for (int l = 0; l < kLists; ++l) per_parity += cap[l];
     const size_t nseg_cap = (size_t)(g->long_entries / kSegEntries) + 2;
+    // pooled on the legacy stream, then synchronised so that any stream may use them
     cudaError_t e = cudaSuccess;
-    if (e == cudaSuccess) e = cudaMalloc(&s->col, n);
-    if (e == cudaSuccess) e = cudaMalloc(&s->req, n * sizeof(int2));
-    if (e == cudaSuccess) e = cudaMalloc(&s->best, n * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMalloc(&s->part_key, n * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMalloc(&s->part_cnt, n * sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc(&s->list_mem, (2 * per_parity + 1) * sizeof(int4));
-    if (e == cudaSuccess) e = cudaMalloc(&s->seg_mem, 2 * nseg_cap * sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc(&s->ctl, kCtlBytes + 256 * sizeof(uint32_t));
+    if (e == cudaSuccess) e = dev_alloc((void **)&s->col, n, 0);
+    if (e == cudaSuccess) e = dev_alloc((void **)&s->req, n * sizeof(int2), 0);
+    if (e == cudaSuccess) e = dev_alloc((void **)&s->best, n * sizeof(unsigned long long), 0);
+    if (e == cudaSuccess) e = dev_alloc((void **)&s->part_key, n * sizeof(unsigned long long), 0);
+    if (e == cudaSuccess) e = dev_alloc((void **)&s->part_cnt, n * sizeof(int), 0);
+    if (e == cudaSuccess) e = dev_alloc((void **)&s->list_mem, (2 * per_parity + 1) * sizeof(int4), 0);
+    if (e == cudaSuccess) e = dev_alloc((void **)&s->seg_mem, 2 * nseg_cap * sizeof(int), 0);
+    if (e == cudaSuccess) e = dev_alloc((void **)&s->ctl, kCtlBytes + 256 * sizeof(uint32_t), 0);
     if (e == cudaSuccess) s->seeds = reinterpret_cast<uint32_t *>(reinterpret_cast<unsigned char *>(s->ctl) + kCtlBytes);
-    if (e == cudaSuccess) e = cudaHostAlloc(&s->host_stage, kCtlBytes + 256 * sizeof(uint32_t), cudaHostAllocDefault);
-    if (e == cudaSuccess) e = cudaHostAlloc(&s->host_back, kCtlBytes, cudaHostAllocDefault);
-    if (e == cudaSuccess) e = cudaMalloc(&s->stats, sizeof(unsigned long long) * kMaxRounds * MM_STATS_COLS);
+    if (e == cudaSuccess) e = pinned_get((void **)&s->host_stage, kCtlBytes + 256 * sizeof(uint32_t));
+    if (e == cudaSuccess) e = pinned_get((void **)&s->host_back, kCtlBytes);
+    if (e == cudaSuccess)
+        e = dev_alloc((void **)&s->stats, sizeof(unsigned long long) * kMaxRounds * MM_STATS_COLS, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) {
+        cudaDeviceSynchronize();
         free_state(s);
         cudaGetLastError();
         set_error(std::string("push: device allocation failed: ") + cudaGetErrorString(e));
@@ -1603,20 +1729,20 @@ mm_status push_prepare(mm_graph *g, int weighted, cudaStream_t stream)
     if (!g->scanned) {
         PrepInfo *d_info = nullptr;
         long long *d_deg = nullptr;
-        MM_CUDA_TRY(cudaMalloc(&d_info, sizeof(PrepInfo)), "prep info");
+        MM_CUDA_TRY(dev_alloc((void **)&d_info, sizeof(PrepInfo), stream), "prep info");
         MM_CUDA_TRY(cudaMemsetAsync(d_info, 0, sizeof(PrepInfo), stream), "prep info clear");
-        cudaError_t e = cudaMalloc(&d_deg, sizeof(long long) * (size_t)n);
+        cudaError_t e = dev_alloc((void **)&d_deg, sizeof(long long) * (size_t)n, stream);
         if (e != cudaSuccess) {
-            cudaFree(d_info);
+            dev_free(d_info, stream);
             return cuda_fail(e, "prep degrees");
         }
         k_scan_ranges<<<grid_for(n, 256, 148 * 8), 256, 0, stream>>>(g->d_ranges, n, g->nnz, d_info, d_deg);
         PrepInfo info;
         e = cudaMemcpyAsync(&info, d_info, sizeof info, cudaMemcpyDeviceToHost, stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-        cudaFree(d_info);
+        dev_free(d_info, stream);
         if (e != cudaSuccess) {
-            cudaFree(d_deg);
+            dev_free(d_deg, stream);
             return cuda_fail(e, "prep scan");
         }
         g->sum_degree = (long long)info.sum_deg;
@@ -1626,45 +1752,82 @@ mm_status push_prepare(mm_graph *g, int weighted, cudaStream_t stream)
         g->long_entries = (long long)info.long_entries;
         g->contiguous = info.noncontig == 0;
         if (g->sum_degree >= (1ll << 31) - 1) {
-            cudaFree(d_deg);
+            dev_free(d_deg, stream);
             set_error("push: more than 2^31 - 2 adjacency slots are not supported");
             return MM_ERR_UNSUPPORTED;
         }
         if (!g->contiguous) {
-            e = cudaMalloc(&g->d_slot_off, sizeof(long long) * (size_t)n);
+            e = dev_alloc((void **)&g->d_slot_off, sizeof(long long) * (size_t)n, stream);
             void *tmp = nullptr;
             size_t tmp_bytes = 0;
             if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_deg, g->d_slot_off, n, stream);
-            if (e == cudaSuccess) e = cudaMalloc(&tmp, tmp_bytes);
+            if (e == cudaSuccess) e = dev_alloc((void **)&tmp, tmp_bytes, stream);
             if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, d_deg, g->d_slot_off, n, stream);
             if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-            cudaFree(tmp);
+            dev_free(tmp, stream);
             if (e != cudaSuccess) {
-                cudaFree(d_deg);
+                dev_free(d_deg, stream);
                 return cuda_fail(e, "slot offsets");
             }
         }
-        cudaFree(d_deg);
+        dev_free(d_deg, stream);
         g->scanned = true;
     }
     const long long S = g->sum_degree;
 
     unsigned long long *revkey = nullptr;
-    cudaError_t e = cudaMalloc(&revkey, sizeof(unsigned long long) * (size_t)(S > 0 ? S : 1));
+    cudaError_t e = dev_alloc((void **)&revkey, sizeof(unsigned long long) * (size_t)(S > 0 ? S : 1), stream);
     if (e != cudaSuccess) return cuda_fail(e, "reverse keys");
     if (S == 0) {
         g->d_revkey[wi] = revkey;
         return MM_OK;
     }
+    // Sorted lists: binary-search build.
+    {
+        const long long chunks = (S + kRevChunk - 1) / kRevChunk;
+        int *chunk_v = nullptr;
+        e = dev_alloc((void **)&chunk_v, sizeof(int) * (size_t)(chunks + 2), stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(chunk_v + chunks + 1, 0, sizeof(int), stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(revkey, 0, sizeof(unsigned long long) * (size_t)S, stream);
+        if (e == cudaSuccess) {
+            k_chunk_owner<<<grid_for(chunks + 1, 256, 148 * 8), 256, 0, stream>>>(
+                g->d_ranges, n, g->contiguous ? 1 : 0, g->d_slot_off, S, chunk_v);
+            const int grid = grid_for(chunks, 1, 148 * 8);
+            if (weighted)
+                k_revkey_sorted<true><<<grid, kRevThreads, 0, stream>>>(g->d_ranges, g->d_nbrs, g->d_w,
+                                                                        g->contiguous ? 1 : 0, g->d_slot_off, S,
+                                                                        chunk_v, revkey, chunk_v + chunks + 1);
+            else
+                k_revkey_sorted<false><<<grid, kRevThreads, 0, stream>>>(g->d_ranges, g->d_nbrs, g->d_w,
+                                                                         g->contiguous ? 1 : 0, g->d_slot_off, S,
+                                                                         chunk_v, revkey, chunk_v + chunks + 1);
+            e = cudaGetLastError();
+        }
+        int unsorted = 1;
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(&unsorted, chunk_v + chunks + 1, sizeof(int), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        dev_free(chunk_v, stream);
+        if (e != cudaSuccess) {
+            dev_free(revkey, stream);
+            return cuda_fail(e, "reverse key build (sorted lists)");
+        }
+        if (!unsorted) {
+            g->d_revkey[wi] = revkey;
+            return MM_OK;
+        }
+    }
+
+    // General lists: sort the (unordered pair, direction) items.
     const int bits = bits_for(n);
     unsigned long long *k0 = nullptr, *k1 = nullptr;
     int *v0 = nullptr, *v1 = nullptr;
     void *tmp = nullptr;
     size_t tmp_bytes = 0;
-    e = cudaMalloc(&k0, sizeof(unsigned long long) * S);
-    if (e == cudaSuccess) e = cudaMalloc(&k1, sizeof(unsigned long long) * S);
-    if (e == cudaSuccess) e = cudaMalloc(&v0, sizeof(int) * S);
-    if (e == cudaSuccess) e = cudaMalloc(&v1, sizeof(int) * S);
+    e = dev_alloc((void **)&k0, sizeof(unsigned long long) * S, stream);
+    if (e == cudaSuccess) e = dev_alloc((void **)&k1, sizeof(unsigned long long) * S, stream);
+    if (e == cudaSuccess) e = dev_alloc((void **)&v0, sizeof(int) * S, stream);
+    if (e == cudaSuccess) e = dev_alloc((void **)&v1, sizeof(int) * S, stream);
     if (e == cudaSuccess) {
         k_pair_items<<<grid_for(n * 32ll, 256, 148 * 16), 256, 0, stream>>>(
             g->d_ranges, g->d_nbrs, n, bits, g->contiguous ? 1 : 0, g->d_slot_off, k0, v0);
@@ -1674,7 +1837,7 @@ mm_status push_prepare(mm_graph *g, int weighted, cudaStream_t stream)
     cub::DoubleBuffer<int> vb(v0, v1);
     const int end_bit = 2 * bits + 1;
     if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, kb, vb, (int)S, 0, end_bit, stream);
-    if (e == cudaSuccess) e = cudaMalloc(&tmp, tmp_bytes);
+    if (e == cudaSuccess) e = dev_alloc((void **)&tmp, tmp_bytes, stream);
     if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, kb, vb, (int)S, 0, end_bit, stream);
     if (e == cudaSuccess) {
         const int grid = grid_for(S, 256, 148 * 16);
@@ -1687,13 +1850,13 @@ mm_status push_prepare(mm_graph *g, int weighted, cudaStream_t stream)
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-    cudaFree(tmp);
-    cudaFree(k0);
-    cudaFree(k1);
-    cudaFree(v0);
-    cudaFree(v1);
+    dev_free(tmp, stream);
+    dev_free(k0, stream);
+    dev_free(k1, stream);
+    dev_free(v0, stream);
+    dev_free(v1, stream);
     if (e != cudaSuccess) {
-        cudaFree(revkey);
+        dev_free(revkey, stream);
         return cuda_fail(e, "reverse key build");
     }
     g->d_revkey[wi] = revkey;
@@ -1767,10 +1930,10 @@ void push_release(mm_graph *g)
         g->push_exec = nullptr;
     }
     for (int i = 0; i < 2; ++i) {
-        cudaFree(g->d_revkey[i]);
+        dev_free(g->d_revkey[i], 0);
         g->d_revkey[i] = nullptr;
     }
-    cudaFree(g->d_slot_off);
+    dev_free(g->d_slot_off, 0);
     g->d_slot_off = nullptr;
 }
 

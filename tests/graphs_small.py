@@ -27,7 +27,7 @@ class SmallGraph:
 
 def random_graph(rng: np.random.Generator, n: int, avg_deg: float = 3.0, symmetric: bool = True,
                  dup: float = 0.05, loops: float = 0.03, gaps: bool = False, shuffle_ranges: bool = False,
-                 empty_reversed: float = 0.0, special_weights: bool = True) -> SmallGraph:
+                 empty_reversed: float = 0.0, special_weights: bool = True, sort_lists: bool = False) -> SmallGraph:
     m = int(n * avg_deg / 2)
     lists = [[] for _ in range(n)]
     for _ in range(m):
@@ -44,6 +44,8 @@ def random_graph(rng: np.random.Generator, n: int, avg_deg: float = 3.0, symmetr
             lists[u].append((v, np.float32(rng.integers(1, 8) / 4)))
     for l in lists:
         rng.shuffle(l)
+        if sort_lists:  # ascending neighbour ids, duplicates kept in their shuffled order
+            l.sort(key=lambda e: e[0])
     order = np.arange(n)
     if shuffle_ranges:
         rng.shuffle(order)

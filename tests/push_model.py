@@ -48,6 +48,89 @@ def reverse_keys(n, ranges, nbrs, w, weighted):
     return rk
 
 
+def reverse_keys_sorted(n, ranges, nbrs, w, weighted, chunk=2048):
+    """The binary-search build of k_chunk_owner + k_revkey_sorted, index for index:
+    slots numbered by the degree prefix, owners found per chunk (in a table of at most
+    chunk + 1 prefixes, else by search between the chunk's owner bounds); of the two
+    entries of a pair only the one whose partner list is shorter (ties by id)
+    searches it, stores the best key of the run it finds and max-combines its own
+    key into the run's entries.  Returns the keys by (owner, entry) or None when
+    some list has a descending pair."""
+    deg = np.maximum(ranges[:, 1] - ranges[:, 0], 0).astype(np.int64)
+    contiguous = bool(n > 0 and ranges[0, 0] == 0 and np.all(ranges[:, 1] >= ranges[:, 0])
+                      and np.all(ranges[1:, 0] == ranges[:-1, 1]) and ranges[-1, 1] == len(nbrs))
+    slot_off = np.concatenate([[0], np.cumsum(deg)[:-1]]) if n else np.zeros(0, np.int64)
+    S = int(deg.sum())
+
+    def prefix(v):
+        return int(ranges[v, 0]) if contiguous else int(slot_off[v])
+
+    def owner_of(lo, hi, s):
+        while lo < hi:
+            mid = (lo + hi + 1) >> 1
+            if prefix(mid) <= s:
+                lo = mid
+            else:
+                hi = mid - 1
+        return lo
+
+    chunks = (S + chunk - 1) // chunk
+    chunk_v = [owner_of(0, n - 1, min(c * chunk, S - 1)) for c in range(chunks + 1)]
+    rk, bad = {}, False
+    pulled, pushed = set(), set()  # the kernel stores pulls plainly: no slot may be in both
+    for c in range(chunks):
+        s0 = c * chunk
+        v0, v1 = chunk_v[c], chunk_v[c + 1]
+        cnt = v1 - v0 + 1
+        pre = [prefix(v0 + i) - s0 for i in range(cnt)] if cnt <= chunk + 1 else None
+        for k in range(chunk):
+            s = s0 + k
+            if s >= S:
+                break
+            if pre is not None:
+                lo, hi = 0, cnt - 1
+                while lo < hi:
+                    mid = (lo + hi + 1) >> 1
+                    if pre[mid] <= k:
+                        lo = mid
+                    else:
+                        hi = mid - 1
+                v = v0 + lo
+            else:
+                v = owner_of(v0, v1, s)
+            pos = s if contiguous else int(ranges[v, 0]) + (s - int(slot_off[v]))
+            assert ranges[v, 0] <= pos < ranges[v, 1]
+            u = int(nbrs[pos])
+            if pos + 1 < ranges[v, 1] and nbrs[pos + 1] < u:
+                bad = True
+            rk.setdefault((v, pos), 0)
+            if u == v:
+                continue
+            dv, du = int(deg[v]), int(deg[u])
+            if du > dv or (du == dv and u > v):
+                continue  # u's entries search v's list and push into this slot
+            lo, hi = int(ranges[u, 0]), int(ranges[u, 0]) + du
+            while lo < hi:
+                mid = (lo + hi) >> 1
+                if nbrs[mid] < v:
+                    lo = mid + 1
+                else:
+                    hi = mid
+            mine = cand_key(pos, float(w[pos]), weighted)
+            key, q = 0, lo
+            while q < int(ranges[u, 0]) + du and nbrs[q] == v:
+                key = max(key, cand_key(q, float(w[q]), weighted))
+                if mine:
+                    rk[(u, q)] = max(rk.get((u, q), 0), mine)
+                    pushed.add((u, q))
+                q += 1
+            pulled.add((v, pos))
+            if key:
+                rk[(v, pos)] = key
+    assert not (pulled & pushed)
+    return None if bad else rk
+
+
 def push_match(g, type_, seeds, barrier, colour_hash):
     n = g.n
     ranges = np.asarray(g.ranges)

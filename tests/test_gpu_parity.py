@@ -100,6 +100,55 @@ def test_adversarial_graphs_match_oracle(mm, orc, torch_cuda, path_name, path):
                     assert np.array_equal(got, want), (it, t, hex(barrier), int((got != want).sum()))
 
 
+def test_sorted_lists_match_oracle(mm, orc, torch_cuda):
+    """Sorted neighbour lists take the binary-search reverse-key build: duplicates,
+    self-loops, one-directional entries, gaps, lists out of vertex order, reversed
+    empty ranges, a run of isolated vertices longer than one slot chunk (2048),
+    hubs; and one descending pair anywhere sends the graph to the pair-sort build."""
+    rng = np.random.default_rng(4242)
+    graphs = []
+    for it in range(40):
+        n = int(rng.integers(1, 400))
+        graphs.append(random_graph(rng, n, avg_deg=float(rng.uniform(0.5, 9)), symmetric=bool(rng.random() < 0.6),
+                                   gaps=bool(rng.random() < 0.3), shuffle_ranges=bool(rng.random() < 0.3),
+                                   empty_reversed=0.2 if rng.random() < 0.3 else 0.0, dup=0.1, loops=0.1,
+                                   sort_lists=True))
+    # sorted symmetric graph with two hubs and 5000 isolated vertices (ids 2000..6999)
+    # inside one slot chunk
+    n = 9000
+    active = np.concatenate([np.arange(2, 2000), np.arange(7000, n)])
+    lists = [[] for _ in range(n)]
+    for h in (0, 1):
+        for v in active[h::1 + h]:
+            lists[h].append(int(v))
+            lists[int(v)].append(h)
+    for _ in range(8000):
+        u, v = int(rng.choice(active)), int(rng.choice(active))
+        if u != v:
+            lists[u].append(v)
+            lists[v].append(u)
+    ranges, nbrs = [], []
+    for v in range(n):
+        b = len(nbrs)
+        nbrs += sorted(lists[v])
+        ranges.append((b, len(nbrs)))
+    nbrs = np.array(nbrs, np.int32)
+    wts = (rng.integers(1, 6, len(nbrs)) / 4).astype(np.float32)
+    graphs.append(SmallGraph(n, np.array(ranges), nbrs, wts))
+    # the same graph with one list's last two entries swapped (unsorted -> pair sort)
+    nb2 = nbrs.copy()
+    b, e = ranges[1]
+    nb2[e - 2], nb2[e - 1] = nb2[e - 1], nb2[e - 2]
+    graphs.append(SmallGraph(n, np.array(ranges), nb2, wts))
+    for gi, g in enumerate(graphs):
+        seeds = orc.rand_seeds(gi + 1, 256)
+        with mm.DeviceGraph(g, device=0) as dg:
+            for t in mm.TYPES:
+                want, rounds, _ = orc.match(g, t, seeds, BARRIER)
+                got, got_rounds = gpu_match(mm, torch_cuda, g, t, seeds, BARRIER, 2, dg=dg)
+                assert got_rounds == rounds and np.array_equal(got, want), (gi, t)
+
+
 def test_long_lists_and_hubs_match_oracle(mm, orc, torch_cuda):
     """Stars and cliques push lists past the block-scan threshold (1024)."""
     n = 6000

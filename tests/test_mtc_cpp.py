@@ -233,9 +233,15 @@ def test_cli_loop_matches_reference(mm, orc, harness, tmp_path, gtype, shuffle):
     got = np.fromfile(out, dtype=np.int32).reshape(reps, g.n)
     assert all(r["valid"] for r in res["runs"])
     if orc.ref_available():
-        want, nxt = orc.ref_cli(path, gtype, BARRIER, 12345, shuffle, reps, g.n)
-        np.testing.assert_array_equal(got, want)
-        assert res["next_rand"] == nxt
+        # The TBB loop stops once nothing can change, so with the 20-round cap it may
+        # draw fewer rand() values than GPU types 6/8, which always run 20 rounds: for
+        # those only the first repetition is comparable (same matching); the oracle
+        # below checks their rand() consumption.
+        k = reps if gtype in (7, 9) else 1
+        want, nxt = orc.ref_cli(path, gtype, BARRIER, 12345, shuffle, k, g.n)
+        np.testing.assert_array_equal(got[:k], want)
+        if gtype in (7, 9):
+            assert res["next_rand"] == nxt
     if not shuffle:
         # every repetition sees the same graph and continues the same rand() stream
         seeds = orc.rand_seeds(12345, 255 * reps + 1)

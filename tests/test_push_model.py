@@ -5,7 +5,7 @@ from __future__ import annotations
 import numpy as np
 
 from graphs_small import random_graph
-from push_model import push_match
+from push_model import push_match, reverse_keys, reverse_keys_sorted
 
 
 def test_push_model_equals_oracle(orc):
@@ -25,3 +25,31 @@ def test_push_model_equals_oracle(orc):
                 assert np.array_equal(got, want), (it, t, hex(barrier))
                 total += 1
     assert total == 120 * 16
+
+
+def test_sorted_reverse_key_build_equals_pair_definition():
+    """k_revkey_sorted's indexing (chunked owners, shared prefix table or bounded
+    search, lower bound in the neighbour's list) gives the reverse keys of their
+    definition on sorted lists, and reports every unsorted graph."""
+    rng = np.random.default_rng(77)
+    seen_unsorted = 0
+    for it in range(150):
+        n = int(rng.integers(1, 60))
+        sort = rng.random() < 0.8
+        g = random_graph(rng, n, avg_deg=float(rng.uniform(0.3, 7)), symmetric=bool(rng.random() < 0.6),
+                         gaps=bool(rng.random() < 0.3), shuffle_ranges=bool(rng.random() < 0.3),
+                         empty_reversed=0.3 if rng.random() < 0.3 else 0.0, dup=0.1, loops=0.1, sort_lists=sort)
+        if rng.random() < 0.3:  # long runs of isolated vertices inside a chunk
+            g.ranges[rng.random(n) < 0.5] = [0, 0]
+        w = g.weights
+        chunk = int(rng.choice([1, 2, 3, 8, 2048]))
+        for weighted in (False, True):
+            want = reverse_keys(n, g.ranges, g.nbrs, w, weighted)
+            got = reverse_keys_sorted(n, g.ranges, g.nbrs, w, weighted, chunk)
+            lists_sorted = all(np.all(np.diff(g.nbrs[b:e].astype(np.int64)) >= 0) for b, e in g.ranges if e > b)
+            if lists_sorted:
+                assert got == want, (it, chunk, weighted)
+            else:
+                assert got is None
+                seen_unsorted += 1
+    assert seen_unsorted > 0
