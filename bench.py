@@ -311,7 +311,7 @@ def main():
     staged_bytes = ew * stn[:, mm.ST_STAGED_DEG] + 36 * stn[:, mm.ST_STAGED_ITEMS]
     short_bytes = (ew * (stn[:, mm.ST_BLUE_DEG] - stn[:, mm.ST_STAGED_DEG])
                    + 36 * np.maximum(stn[:, mm.ST_BLUE] - stn[:, mm.ST_STAGED_ITEMS], 0))
-    kernels = {"k_phase_a_stream (staged long-list scan)": (staged_bytes, ms_k[:, 1]),
+    kernels = {"k_phase_a_long (long-list scan)": (staged_bytes, ms_k[:, 1]),
                "k_phase_a_short (short-list scan)": (short_bytes, ms_k[:, 0])}
     dom = max(kernels, key=lambda k: kernels[k][1].sum())
     dom_bytes, dom_ms = kernels[dom]
@@ -394,6 +394,10 @@ def main():
                          "bytes_per_launch": float(dom_bytes.mean()), "launches": int(nr),
                          "ms_short_scan": float(ms_k[:, 0].sum()), "ms_staged_scan": float(ms_k[:, 1].sum()),
                          "ms_commit": float(ms_k[:, 2].sum()), "ms_tail": ms_tail,
+                         "per_round_work": {k: [int(x) for x in stn[:, c]] for k, c in
+                                            (("blue", mm.ST_BLUE), ("blue_entries", mm.ST_BLUE_DEG),
+                                             ("long_entries", mm.ST_STAGED_DEG),
+                                             ("long_pieces", mm.ST_STAGED_ITEMS))},
                          "per_round_ms": {"short": [round(float(x), 4) for x in ms_k[:, 0]],
                                           "staged": [round(float(x), 4) for x in ms_k[:, 1]],
                                           "commit": [round(float(x), 4) for x in ms_k[:, 2]]},

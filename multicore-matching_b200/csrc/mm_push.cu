@@ -28,17 +28,20 @@
 // Work layout.  Vertices that can still be matched sit in worklists; an item
 // carries the vertex and its neighbour range, so the scans never read
 // neighbourRanges again.
-//   short lists (deg <= 32)   a warp walks the concatenated lists of 32 blue
-//                             vertices, loading entries directly
-//                             (k_phase_a_short)
+//   short lists (deg <= 32)   a warp takes 32 blue vertices and walks their
+//                             concatenated entries row by row, 32 consecutive
+//                             entries per load (k_phase_a_short)
 //   long lists  (deg  > 32)   blue ones are appended with their offset in the
 //                             round's concatenated long-list entry space; that
-//                             space is cut into 960-entry segments, each staged
-//                             into shared memory by bulk copies (TMA) and
-//                             scanned from there (k_phase_a_stream).  A list
-//                             cut by segment edges is combined by atomics and
-//                             its last piece proposes.  Every warp claims equal
-//                             amounts of work whatever the degree skew.
+//                             space is cut into 512-entry segments and a warp
+//                             walks one segment row by row (k_phase_a_long).
+//                             A list cut by segment edges is combined by
+//                             atomics and its last piece proposes.  Every warp
+//                             claims equal amounts of work whatever the skew.
+// Every load of neighbour ids and weights is a coalesced row of 32 consecutive
+// entries; a list's best entry is kept as a 64-bit key (weight order << 32 |
+// ~position) max-combined in shared memory, which orders ties by position
+// exactly as the reference's strict ">" scan in list order does.
 // The two scans run concurrently.
 //
 // Round t is three kernels: the two phase-A scans (blue scan + proposal) and
@@ -63,8 +66,7 @@ constexpr int kBlockA = 256;
 constexpr int kBlockB = 256;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kSmallMax = 32;       // short lists: degree <= 32
-constexpr int kSegEntries = 416;    // entries per staged segment (at most 15 pieces of lists > 32)
-constexpr int kSegCap = 512;        // slot capacity: a segment plus 16-byte alignment slack per piece
+constexpr int kSegEntries = 512;    // entries per long-list segment (at most 16 pieces of lists > 32)
 
 // Worklists.  kStaged holds blue long lists with their entry offsets.
 enum : int { kBlueS = 0, kRedS, kRedLong, kStaged, kLists };
@@ -81,7 +83,7 @@ struct Ctl {
     int cont;              // 1 while another round follows (read by the stepped driver)
     unsigned ticket;       // phase-B block arrivals
     int task_short[2];     // phase-A cursors by round parity: short-list batches
-    int task_stream[2];    //   and staged segments
+    int task_long[2];      //   and long-list segments
     int cnt[2][kLists];    // worklist lengths by round parity (kStaged unused)
     unsigned long long staged_pack[2];  // kStaged: (items << 32) | entries, by parity
     int retired[2];        // vertices of the round that were unmatchable as soon as coloured
@@ -201,46 +203,8 @@ __device__ __forceinline__ unsigned long long strip_key(float bw, int bj, bool a
     return alive ? 1ull : 0ull;
 }
 
-constexpr int kShortStep = 8;  // entries a lane loads (and gathers) at once
-
-// Phase A for up to 32 short lists, one per lane: each lane walks its own list
-// (at most 32 entries) kShortStep entries at a time, keeping the reference's
-// choice with a running float compare.  Random mode ranks every red neighbour
-// with weight 0, so the first one wins and the walk stops there.
-template <bool kW, bool kStats>
-__device__ void scan_short_lanes(const Params &p, const int4 *list, int begin, int count, int t)
-{
-    const int idx = begin + (threadIdx.x & 31);
-    if (idx >= count) return;
-    const int4 it = list[idx];
-    float bw = -1.0f;
-    int bj = 0;
-    bool alive = false;
-    for (int b = it.y; b < it.z; b += kShortStep) {
-        int nb[kShortStep];
-        float wv[kShortStep];
-#pragma unroll
-        for (int k = 0; k < kShortStep; ++k) {
-            const bool in = b + k < it.z;
-            nb[k] = in ? __ldcs(p.nbrs + b + k) : 0;
-            wv[k] = kW && in ? __ldcs(p.w + b + k) : 0.0f;
-        }
-        uint8_t c[kShortStep];
-#pragma unroll
-        for (int k = 0; k < kShortStep; ++k) c[k] = p.col[nb[k]];
-#pragma unroll
-        for (int k = 0; k < kShortStep; ++k) {
-            if (b + k >= it.z) break;
-            alive |= c[k] != kMatched;
-            if (c[k] == kRed && wv[k] > bw) {
-                bw = wv[k];
-                bj = b + k;
-            }
-        }
-        if (!kW && bw > -1.0f) break;  // grRequest returns at the first red neighbour
-    }
-    propose_counted<kW, kStats>(p, it, strip_key<kW>(bw, bj, alive), t);
-}
+constexpr int kShortStep = 8;  // entries a tail thread loads (and gathers) at once
+constexpr int kRows = 4;       // rows of 32 entries a warp keeps in flight in the grid scans
 
 // ---- worklist compaction for the set-up and commit passes ----
 //
@@ -379,11 +343,20 @@ __global__ void __launch_bounds__(kBlockT) k_init(Params p)
     }
 }
 
-// Phase A, short lists: warps claim batches of 32 blue short-list vertices.
-// Block 0 also resets the next round's list counters and cursors.
+// Phase A, short lists: a warp claims 32 blue short-list vertices, lays their
+// entries end to end (at most 1024) and walks them in rows of 32: lane l of
+// row r takes entry 32r + l, so every load is one coalesced row.  The owner of
+// each entry comes from a byte table the lanes fill for their own lists; keys
+// are max-combined per list in shared memory.  Block 0 also resets the next
+// round's list counters and cursors.
+constexpr int kWarpsA = kBlockA / 32;
+
 template <bool kW, bool kStats>
 __global__ void __launch_bounds__(kBlockA) k_phase_a_short(Params p)
 {
+    __shared__ unsigned long long s_acc[kWarpsA][32];
+    __shared__ int s_delta[kWarpsA][32];
+    __shared__ uint8_t s_owner[kWarpsA][32 * kSmallMax];
     Ctl *ctl = p.ctl;
     const int t = ctl->t;
     const int par = t & 1;
@@ -391,354 +364,179 @@ __global__ void __launch_bounds__(kBlockA) k_phase_a_short(Params p)
     if (blockIdx.x == 0 && threadIdx.x < kLists) ctl->cnt[par ^ 1][threadIdx.x] = 0;
     if (blockIdx.x == 0 && threadIdx.x == 32) {
         ctl->task_short[par ^ 1] = 0;
-        ctl->task_stream[par ^ 1] = 0;
+        ctl->task_long[par ^ 1] = 0;
         ctl->staged_pack[par ^ 1] = 0ull;
         ctl->retired[par ^ 1] = 0;
     }
     const int units = (n_short + 31) / 32;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long *acc = s_acc[warp];
+    int *delta = s_delta[warp];
+    uint8_t *owner = s_owner[warp];
+    const int4 *list = p.lists[par][kBlueS];
     for (;;) {
         int u = 0;
         if (lane == 0) u = atomicAdd(&ctl->task_short[par], 1);
         u = __shfl_sync(kFull, u, 0);
         if (u >= units) break;
-        scan_short_lanes<kW, kStats>(p, p.lists[par][kBlueS], u * 32, n_short, t);
-    }
-}
-
-// ---- staged scans of long lists (Blackwell bulk copies into shared memory) ----
-
-constexpr int kWarpsStream = 4;    // warps per staged-scan block, each an independent pipeline
-constexpr int kStages = 2;         // slots per warp: one being scanned, one in flight
-constexpr int kStep = 17;          // entries per lane per pass: a whole strip of a full slot
-
-// Bulk-copy destinations must be 16-byte aligned: every slot row is a multiple
-// of 16 bytes and the per-warp struct (laid out back to back) is 16-aligned.
-struct __align__(16) StreamWarpSmem {
-    int nb[kStages][kSegCap];           // neighbour ids
-    float w[kStages][kSegCap];          // weights
-    unsigned long long acc[32];         // per-piece running max of the segment being scanned
-    unsigned long long bar[kStages];    // one mbarrier per slot
-    int span_end[32];                   // one past each piece's copied span in the slot
-    int first[32];                      // slot index of each piece's first real entry
-    int last[32];                       // one past its last real entry
-    int delta[32];                      // global position of a slot entry = slot index + delta
-};
-static_assert(sizeof(StreamWarpSmem) % 16 == 0, "per-warp staging area must keep 16-byte alignment");
-static_assert((kSegCap * sizeof(int)) % 16 == 0, "slot rows must be multiples of 16 bytes");
-static_assert(offsetof(StreamWarpSmem, w) % 16 == 0, "weight slots must be 16-byte aligned");
-static_assert(offsetof(StreamWarpSmem, bar) % 8 == 0, "mbarriers must be 8-byte aligned");
-
-__device__ __forceinline__ uint32_t smem_addr(const void *ptr) { return (uint32_t)__cvta_generic_to_shared(ptr); }
-
-__device__ __forceinline__ void mbar_init(unsigned long long *bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect(unsigned long long *bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
-                 : "memory");
-}
-
-// try_wait that lets the hardware suspend the warp for up to ~1 us while the
-// phase is incomplete, instead of spinning on issue slots.
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_addr(bar)), "r"(parity), "r"(1000u)
-        : "memory");
-    return ok != 0;
-}
-
-__device__ __forceinline__ unsigned long long global_ns()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-    return t;
-}
-
-// Wait for a slot's copies; false if the wait gave up.  Each try suspends the
-// warp for up to ~1 us, and the clock is read only every 1024 tries, so the
-// bound (~2 s) costs nothing while copies land normally.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, uint32_t parity)
-{
-    if (mbar_try_wait(bar, parity)) return true;
-    const unsigned long long t0 = global_ns();
-    for (unsigned tries = 1;; ++tries) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if ((tries & 1023u) == 0 && global_ns() - t0 > 2000000000ull) return false;
-    }
-}
-
-// Bulk copy global -> shared, completing on `bar`; the source is streamed
-// (L2 evict-first) so it does not displace the colour and proposal arrays.
-__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, unsigned long long *bar,
-                                          unsigned long long policy)
-{
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;"
-        ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(policy)
-        : "memory");
-}
-
-__device__ __forceinline__ unsigned long long evict_first_policy()
-{
-    unsigned long long pol;
-    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
-    return pol;
-}
-
-// One staged segment as held by a warp: lane i holds the i-th list piece.
-struct StageSeg {
-    int4 it;      // the list's item {v, begin, end, offset}; it.x < 0 if none
-    int lo, hi;   // piece = list entries [lo, hi) (list-relative)
-    int off;      // slot offset (entries) of the piece's 16-byte-aligned copy
-    int plen;     // copied entries (aligned span)
-    int pieces;   // segments the whole list spans
-    int valid;    // warp-uniform: a segment was claimed
-};
-
-// Claim the next segment and start its bulk copies into `slot`.  The slot's
-// previous contents were only read by this warp and those reads completed
-// before the __syncwarp that ended its scan, so the copies may overwrite it.
-template <bool kW>
-__device__ __forceinline__ void claim_and_issue(const Params &p, StreamWarpSmem &sm, int par, int nseg, int nitems,
-                                                int slot, unsigned long long policy, StageSeg &g)
-{
-    const int lane = threadIdx.x & 31;
-    int s = 0;
-    if (lane == 0) s = atomicAdd(&p.ctl->task_stream[par], 1);
-    s = __shfl_sync(kFull, s, 0);
-    g.valid = s < nseg;
-    g.it = make_int4(-1, 0, 0, 0);
-    g.plen = 0;
-    g.lo = g.hi = 0;
-    g.pieces = 1;
-    if (!g.valid) return;
-    const int s_lo = s * kSegEntries, s_hi = s_lo + kSegEntries;
-    const int idx = p.seg_first[par][s] + lane;
-    if (idx < nitems) {
-        const int4 it = p.lists[par][kStaged][idx];
-        const int deg = degree_of(it);
-        if (it.w < s_hi && it.w + deg > s_lo) {
-            g.it = it;
-            g.lo = max(it.w, s_lo) - it.w;
-            g.hi = min(it.w + deg, s_hi) - it.w;
-            g.plen = ((it.y + g.hi + 3) & ~3) - ((it.y + g.lo) & ~3);
-            g.pieces = (it.w + deg - 1) / kSegEntries - it.w / kSegEntries + 1;
-        }
-    }
-    g.off = warp_incl_scan(g.plen) - g.plen;
-    uint32_t bytes = (uint32_t)g.plen * 4u * (kW ? 2u : 1u);
+        const int idx = u * 32 + lane;
+        const bool valid = idx < n_short;
+        const int4 it = valid ? list[idx] : make_int4(-1, 0, 0, 0);
+        const int deg = valid ? degree_of(it) : 0;
+        const int incl = warp_incl_scan(deg);
+        const int start = incl - deg;
+        const int total = __shfl_sync(kFull, incl, 31);
+        delta[lane] = it.y - start;  // global position of concatenated entry e: e + delta[owner]
+        acc[lane] = 0ull;
+        for (int k = 0; k < deg; ++k) owner[start + k] = (uint8_t)lane;
+        __syncwarp();
+        for (int base = 0; base < total; base += 32 * kRows) {
+            int own[kRows], pos[kRows], nb[kRows];
+            float wv[kRows];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(kFull, bytes, o);
-    if (lane == 0) mbar_expect(&sm.bar[slot], bytes);
-    if (g.plen > 0) {
-        const int a = (g.it.y + g.lo) & ~3;
-        bulk_load(&sm.nb[slot][g.off], p.nbrs + a, (uint32_t)g.plen * 4u, &sm.bar[slot], policy);
-        if (kW) bulk_load(&sm.w[slot][g.off], p.w + a, (uint32_t)g.plen * 4u, &sm.bar[slot], policy);
-    }
-}
-
-// Scan a staged segment from its slot.  Lane l walks the contiguous strip
-// [l*S, (l+1)*S) of the slot, S odd so the 32 lanes hit 32 banks.  Within a
-// strip entries come in increasing list position, so a running float compare
-// (strict >) keeps exactly the entry the reference's loop would; the piece an
-// entry belongs to is tracked in registers (alignment junk around a piece is
-// skipped), and the lane folds its key into sm.acc with a shared atomic max
-// where its strip leaves a piece.  Random mode ranks every red neighbour with
-// weight 0, so the first one seen wins.
-template <bool kW>
-__device__ __forceinline__ bool scan_segment(const Params &p, StreamWarpSmem &sm, const StageSeg &g, int slot,
-                                             uint32_t parity)
-{
-    const int lane = threadIdx.x & 31;
-    if (!mbar_wait_bounded(&sm.bar[slot], parity)) return false;
-    const int *snb = sm.nb[slot];
-    const float *sw = sm.w[slot];
-    const int first = g.off + ((g.it.y + g.lo) & 3);  // slot index of the piece's first entry
-    sm.span_end[lane] = g.off + g.plen;
-    sm.first[lane] = first;
-    sm.last[lane] = first + (g.hi - g.lo);
-    sm.delta[lane] = (g.it.y + g.lo) - first;
-    const int used = __shfl_sync(kFull, g.off + g.plen, 31);
-    __syncwarp();
-    const int stride = ((used + 31) / 32) | 1;
-    const int p0 = lane * stride, p1 = min(p0 + stride, used);
-    if (p0 < p1) {
-        // piece holding p0: first lane whose span ends after it
-        int lo = 0, hi = 31;
-        while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (sm.span_end[mid] <= p0) lo = mid + 1;
-            else hi = mid;
-        }
-        int own = lo, own_end = sm.span_end[lo], own_first = sm.first[lo], own_last = sm.last[lo];
-        int own_delta = sm.delta[lo];
-        float bw = -1.0f;
-        int bj = 0;
-        bool alive = false;
-        for (int base = p0; base < p1; base += kStep) {
-            int nbv[kStep];
-            float wv[kStep];
-#pragma unroll
-            for (int k = 0; k < kStep; ++k) {
-                const bool in = base + k < p1;
-                nbv[k] = in ? snb[base + k] : 0;
-                wv[k] = kW && in ? sw[base + k] : 0.0f;
+            for (int r = 0; r < kRows; ++r) {
+                const int e = base + r * 32 + lane;
+                const bool in = e < total;
+                own[r] = in ? owner[e] : -1;
+                pos[r] = in ? e + delta[own[r]] : 0;
+                nb[r] = in ? __ldcs(p.nbrs + pos[r]) : 0;
+                wv[r] = kW && in ? __ldcs(p.w + pos[r]) : 0.0f;
             }
-            // alignment junk can hold anything (gaps of a non-contiguous CSR are
-            // never validated): clamp the index; those entries are ignored below
-            uint8_t c[kStep];
+            uint8_t c[kRows];
 #pragma unroll
-            for (int k = 0; k < kStep; ++k) c[k] = p.col[min((unsigned)nbv[k], (unsigned)(p.n - 1))];
+            for (int r = 0; r < kRows; ++r) c[r] = own[r] >= 0 ? p.col[nb[r]] : (uint8_t)kMatched;
 #pragma unroll
-            for (int k = 0; k < kStep; ++k) {
-                const int q = base + k;
-                if (q >= p1) break;
-                if (q >= own_end) {  // strip leaves the piece: fold it and move on
-                    const unsigned long long key = strip_key<kW>(bw, bj, alive);
-                    if (key) atomicMax(&sm.acc[own], key);
-                    bw = -1.0f;
-                    alive = false;
-                    do {
-                        ++own;
-                        own_end = sm.span_end[own];
-                    } while (q >= own_end);
-                    own_first = sm.first[own];
-                    own_last = sm.last[own];
-                    own_delta = sm.delta[own];
-                }
-                const bool real = q >= own_first && q < own_last;
-                alive |= real && c[k] != kMatched;
-                if (real && c[k] == kRed && wv[k] > bw) {
-                    bw = wv[k];
-                    bj = q + own_delta;
-                }
+            for (int r = 0; r < kRows; ++r) {
+                const unsigned long long key = entry_key<kW>(c[r], pos[r], wv[r]);
+                if (key) atomicMax(&acc[own[r]], key);
             }
         }
-        const unsigned long long key = strip_key<kW>(bw, bj, alive);
-        if (key) atomicMax(&sm.acc[own], key);
+        __syncwarp();
+        if (valid) propose_counted<kW, kStats>(p, it, acc[lane], t);
+        __syncwarp();  // the tables are refilled by the next batch
     }
-    __syncwarp();
-    return true;
 }
 
-// Proposal of a whole list whose two loads (target id and reverse key) are in
-// flight; it is completed after the warp has scanned its next segment.
-struct PendingProposal {
-    int v;                  // -1: nothing pending
-    int target;
-    unsigned long long rk;
-};
+// ---- long lists: entry-balanced segments ----
+//
+// The blue long lists of a round are concatenated (each item's .w is its
+// offset) and cut into kSegEntries-entry segments; seg_first[s] is the first
+// item overlapping segment s.  A warp takes a segment: lane l describes the
+// l-th list piece in it (at most 16), then the warp walks the segment in rows
+// of 32 consecutive entries.  Each lane keeps a cursor on the piece its entry
+// falls in (it moves forward only) and a running key for it, folded into the
+// piece's shared slot when the cursor moves on.  A list inside one segment
+// proposes at once; a cut list max-combines its piece into part_key and the
+// piece that arrives last proposes.
 
-__device__ __forceinline__ void finish_proposal(const Params &p, const PendingProposal &q)
-{
-    if (q.v < 0) return;
-    if (q.rk) atomicMax(&p.best[q.target], q.rk);
-    p.req[q.v] = make_int2(q.target, (int)(uint32_t)q.rk);
-}
+constexpr int kWarpsL = 8;
 
-// Fold a scanned segment.  A whole list that proposes only issues its loads
-// here (finish_proposal completes it later); dead / non-proposing lists are
-// finished at once; a list cut by segment edges folds its piece into part_key
-// and its last piece to arrive proposes.
 template <bool kW, bool kStats>
-__device__ __forceinline__ PendingProposal finish_segment(const Params &p, StreamWarpSmem &sm, const StageSeg &g,
-                                                          int t)
+__device__ __forceinline__ void finish_piece(const Params &p, int4 it, int pieces, unsigned long long key, int t)
 {
-    const int lane = threadIdx.x & 31;
-    const unsigned long long key = sm.acc[lane];
-    sm.acc[lane] = 0ull;
-    __syncwarp();
-    PendingProposal q;
-    q.v = -1;
-    if (g.it.x < 0) return q;
-    if (kStats) {
-        atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_STAGED_DEG], (unsigned long long)(g.hi - g.lo));
-        atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_STAGED_ITEMS], 1ull);
+    if (pieces == 1) {
+        propose_counted<kW, kStats>(p, it, key, t);
+        return;
     }
-    if (g.pieces == 1) {
-        if (key < 2) {
-            propose_counted<kW, kStats>(p, g.it, key, t);
-            return q;
-        }
-        if (kStats) {
-            atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_REQ_ENTRIES],
-                      request_seen<kW>(g.it.y, degree_of(g.it), key));
-            atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_BLUE_DEG], (unsigned long long)degree_of(g.it));
-        }
-        const int j = (int)~(uint32_t)key;
-        const long long slot = p.contiguous ? (long long)j : p.slot_off[g.it.x] + (j - g.it.y);
-        q.v = g.it.x;
-        q.target = p.nbrs[j];
-        q.rk = p.revkey[slot];
-        return q;
-    }
-    const int v = g.it.x;
+    const int v = it.x;
     if (key) atomicMax(&p.part_key[v], key);
     // acq_rel: this piece's max is visible before its arrival counts, and the
     // last arrival sees every other piece's max
     int done;
     asm volatile("atom.add.acq_rel.gpu.s32 %0, [%1], 1;" : "=r"(done) : "l"(p.part_cnt + v) : "memory");
-    if (done == g.pieces - 1) {
+    if (done == pieces - 1) {
         const unsigned long long all = atomicExch(&p.part_key[v], 0ull);
         p.part_cnt[v] = 0;
-        propose_counted<kW, kStats>(p, g.it, all, t);
+        propose_counted<kW, kStats>(p, it, all, t);
     }
-    return q;
 }
 
-// Phase A, long lists: each warp runs a two-slot pipeline -- while it scans
-// one segment from shared memory, the bulk copies of the next are in flight.
 template <bool kW, bool kStats>
-__global__ void __launch_bounds__(kWarpsStream * 32) k_phase_a_stream(Params p)
+__global__ void __launch_bounds__(kWarpsL * 32) k_phase_a_long(Params p)
 {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    StreamWarpSmem &sm = reinterpret_cast<StreamWarpSmem *>(smem_raw)[threadIdx.x >> 5];
+    __shared__ unsigned long long s_acc[kWarpsL][32];
+    __shared__ int s_end[kWarpsL][33];    // segment-relative end of each piece; INT_MAX past the last
+    __shared__ int s_delta[kWarpsL][32];  // global position of segment entry e: e + delta[piece]
     Ctl *ctl = p.ctl;
     const int t = ctl->t;
     const int par = t & 1;
     const unsigned long long pack = ctl->staged_pack[par];
     const int nitems = (int)(pack >> 32);
-    const int nseg = (int)(((pack & 0xffffffffull) + kSegEntries - 1) / kSegEntries);
+    const int nentries = (int)(pack & 0xffffffffull);
+    const int nseg = (nentries + kSegEntries - 1) / kSegEntries;
     if (nseg == 0) return;
-    const int lane = threadIdx.x & 31;
-    if (lane == 0) {
-        for (int q = 0; q < kStages; ++q) mbar_init(&sm.bar[q], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    sm.acc[lane] = 0ull;
-    __syncwarp();
-    const unsigned long long policy = evict_first_policy();
-    uint32_t parity = 0u;  // bit q: phase parity of slot q's barrier
-    StageSeg cur, nxt;
-    PendingProposal pending;
-    pending.v = -1;
-    int s_cur = 0;
-    claim_and_issue<kW>(p, sm, par, nseg, nitems, s_cur, policy, cur);
-    while (cur.valid) {
-        claim_and_issue<kW>(p, sm, par, nseg, nitems, s_cur ^ 1, policy, nxt);
-        const bool ok = scan_segment<kW>(p, sm, cur, s_cur, (parity >> s_cur) & 1u);
-        parity ^= 1u << s_cur;
-        if (!ok) {
-            if (lane == 0) atomicExch(&ctl->status, 2);
-            return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long *acc = s_acc[warp];
+    int *pend = s_end[warp];
+    int *delta = s_delta[warp];
+    const int4 *list = p.lists[par][kStaged];
+    for (;;) {
+        int s = 0;
+        if (lane == 0) s = atomicAdd(&ctl->task_long[par], 1);
+        s = __shfl_sync(kFull, s, 0);
+        if (s >= nseg) break;
+        const int s_lo = s * kSegEntries;
+        const int seg_len = min(kSegEntries, nentries - s_lo);
+        const int idx = p.seg_first[par][s] + lane;
+        int4 it = make_int4(-1, 0, 0, 0);
+        int pieces = 1, lo = 0, hi = 0;
+        if (idx < nitems) {
+            const int4 x = list[idx];
+            const int deg = degree_of(x);
+            if (x.w < s_lo + seg_len && x.w + deg > s_lo) {
+                it = x;
+                lo = max(x.w, s_lo) - x.w;
+                hi = min(x.w + deg, s_lo + seg_len) - x.w;
+                pieces = (x.w + deg - 1) / kSegEntries - x.w / kSegEntries + 1;
+            }
         }
-        finish_proposal(p, pending);  // the previous segment's loads had this scan to land
-        pending = finish_segment<kW, kStats>(p, sm, cur, t);
-        cur = nxt;
-        s_cur ^= 1;
+        pend[lane] = it.x >= 0 ? it.w + hi - s_lo : 0x7fffffff;
+        if (lane == 0) pend[32] = 0x7fffffff;
+        delta[lane] = it.y - it.w + s_lo;
+        acc[lane] = 0ull;
+        __syncwarp();
+        int cur = 0;
+        unsigned long long best = 0ull;
+        int fold = 0;  // piece the running key belongs to
+        for (int base = 0; base < seg_len; base += 32 * kRows) {
+            int own[kRows], pos[kRows], nb[kRows];
+            float wv[kRows];
+#pragma unroll
+            for (int r = 0; r < kRows; ++r) {
+                const int e = base + r * 32 + lane;
+                const bool in = e < seg_len;
+                while (in && e >= pend[cur]) ++cur;
+                own[r] = in ? cur : -1;
+                pos[r] = e + delta[cur];
+                nb[r] = in ? __ldcs(p.nbrs + pos[r]) : 0;
+                wv[r] = kW && in ? __ldcs(p.w + pos[r]) : 0.0f;
+            }
+            uint8_t c[kRows];
+#pragma unroll
+            for (int r = 0; r < kRows; ++r) c[r] = own[r] >= 0 ? p.col[nb[r]] : (uint8_t)kMatched;
+#pragma unroll
+            for (int r = 0; r < kRows; ++r) {
+                if (own[r] < 0) continue;
+                if (own[r] != fold) {
+                    if (best) atomicMax(&acc[fold], best);
+                    best = 0ull;
+                    fold = own[r];
+                }
+                const unsigned long long key = entry_key<kW>(c[r], pos[r], wv[r]);
+                best = key > best ? key : best;
+            }
+        }
+        if (best) atomicMax(&acc[fold], best);
+        __syncwarp();
+        if (it.x >= 0) {
+            if (kStats) {
+                atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_STAGED_DEG], (unsigned long long)(hi - lo));
+                atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_STAGED_ITEMS], 1ull);
+            }
+            finish_piece<kW, kStats>(p, it, pieces, acc[lane], t);
+        }
+        __syncwarp();  // the tables are refilled by the next segment
     }
-    finish_proposal(p, pending);
-    // claims beyond the last segment armed nothing: no copy is in flight
 }
 
 // Rounds small enough for one block run in the tail kernel.
@@ -1388,7 +1186,7 @@ struct PushState {
     unsigned long long *stats = nullptr;
     Plan plans[8];
     int nplans = 0;
-    int blocks_a = 0, blocks_b = 0, blocks_stream = 0, stream_smem = 0;
+    int blocks_a = 0, blocks_b = 0, blocks_long = 0;
 };
 
 int bits_for(long long n)
@@ -1467,19 +1265,12 @@ mm_status alloc_state(mm_graph *g, PushState **out)
     int sms = 148, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    // the staged scan keeps two slots per warp in dynamic shared memory
-    const int stream_smem = (int)(sizeof(StreamWarpSmem) * kWarpsStream);
-    cudaFuncSetAttribute(k_phase_a_stream<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, stream_smem);
-    cudaFuncSetAttribute(k_phase_a_stream<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, stream_smem);
-    cudaFuncSetAttribute(k_phase_a_stream<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, stream_smem);
-    cudaFuncSetAttribute(k_phase_a_stream<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, stream_smem);
-    int occ_a = 0, occ_s = 0, occ_b = 0;
+    int occ_a = 0, occ_l = 0, occ_b = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_phase_a_short<true, false>, kBlockA, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, k_phase_a_stream<true, false>, kWarpsStream * 32, stream_smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_l, k_phase_a_long<true, false>, kWarpsL * 32, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_phase_b<true, false>, kBlockT, 0);
     s->blocks_a = sms * (occ_a > 0 ? occ_a : 4);
-    s->blocks_stream = sms * (occ_s > 0 ? occ_s : 1);
-    s->stream_smem = stream_smem;
+    s->blocks_long = sms * (occ_l > 0 ? occ_l : 4);
     s->blocks_b = sms * (occ_b > 0 ? occ_b : 4);
     cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) {
@@ -1556,10 +1347,9 @@ mm_status build_plan(mm_graph *g, PushState *s, Plan *plan)
         e = cudaGraphAddKernelNode(&n_a, body, nullptr, 0, &ka);
         if (e == cudaSuccess) {
             cudaKernelNodeParams kl = {};
-            kl.func = (void *)k_phase_a_stream<kW, kStats>;
-            kl.gridDim = dim3(s->blocks_stream);
-            kl.blockDim = dim3(kWarpsStream * 32);
-            kl.sharedMemBytes = (unsigned)s->stream_smem;
+            kl.func = (void *)k_phase_a_long<kW, kStats>;
+            kl.gridDim = dim3(s->blocks_long);
+            kl.blockDim = dim3(kWarpsL * 32);
             kl.kernelParams = args;
             e = cudaGraphAddKernelNode(&n_l, body, nullptr, 0, &kl);
         }
@@ -1670,7 +1460,7 @@ mm_status stepped_rounds(mm_graph *g, PushState *s, int *rounds_done, float *ms_
         cudaEventRecord(ev[0], stream);
         k_phase_a_short<kW, false><<<s->blocks_a, kBlockA, 0, stream>>>(p);
         cudaEventRecord(ev[1], stream);
-        k_phase_a_stream<kW, false><<<s->blocks_stream, kWarpsStream * 32, s->stream_smem, stream>>>(p);
+        k_phase_a_long<kW, false><<<s->blocks_long, kWarpsL * 32, 0, stream>>>(p);
         cudaEventRecord(ev[2], stream);
         k_phase_b<kW, false><<<s->blocks_b, kBlockT, 0, stream>>>(p);
         cudaEventRecord(ev[3], stream);
