@@ -17,10 +17,12 @@ One step = one matching of the whole graph to maximality.
   e2e       the same metric end to end through the C ABI with host buffers:
             upload + validation + preparation + matching + download + free per
             step (the reference's t0 -> t3 "total time").
-  roofline  the dominant kernel (phase A: blue scan + proposal) timed per
-            launch with CUDA events in a host-stepped run of the same kernels;
-            achieved = its algorithmic bytes / its duration, against the
-            measured HBM copy bandwidth.
+  roofline  the round kernel k_rounds, the only kernel of a matching (one
+            cooperative launch per step): achieved = its algorithmic bytes
+            (set-up, window, fallback and commit phases, from the instrumented run's
+            per-round counters) / the step's CUDA-event time, against the
+            measured HBM copy bandwidth.  The three round phases are also
+            reported separately, timed by the kernel's own barrier timestamps.
   cpu_baseline  the reference's own GraphMatchingTBBWeighted (same algorithm,
             src/matchtbb.cu:567-623) compiled from its sources into
             oracle/_ref, on all host cores, on the same graph and seeds; its
@@ -258,10 +260,10 @@ def main():
         r, ms_k, launches = dg.profile(t, seeds, out.data_ptr(), stream=sptr)
         torch.cuda.synchronize()
         print(json.dumps({"ncu_case": args.workload, "rounds": r, "launches": launches,
-                          "ms_short_scan": [round(float(x), 4) for x in ms_k[:-1, 0]],
-                          "ms_staged_scan": [round(float(x), 4) for x in ms_k[:-1, 1]],
-                          "ms_commit": [round(float(x), 4) for x in ms_k[:-1, 2]],
-                          "ms_tail": round(float(ms_k[-1, 3]), 4)}))
+                          "ms_window": [round(float(x), 4) for x in ms_k[:, 0]],
+                          "ms_fallback": [round(float(x), 4) for x in ms_k[:, 1]],
+                          "ms_commit": [round(float(x), 4) for x in ms_k[:, 2]],
+                          "ms_rounds_total": round(float(ms_k[:, 3].sum()), 4)}))
         dg.close()
         return 0
     # instrumented run: rounds and the work each round does
@@ -295,32 +297,25 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
     value = edges * world / (ms / 1e3)
-    # the scan kernels, timed per launch (host-stepped run of the same kernels)
+    # per-round phase times of the round kernel (barrier timestamps of the same launch shape)
     prof = []
     for _ in range(3):
         flush.fill_(1)
         _, ms_k, _ = dg.profile(t, seeds, out.data_ptr(), stream=sptr)
         prof.append(ms_k)
-    ms_k = np.mean(np.stack(prof), axis=0)  # [grid rounds + 1, (short scan, staged scan, commit, tail)]
-    ms_tail = float(ms_k[-1, 3])
-    ms_k = ms_k[:-1]
-    nr = ms_k.shape[0]
-    gpu_launches = args.steps * (3 + 3 * nr)
-    ew = 8 if weighted else 4
-    stn = st[:nr].astype(np.float64)
-    staged_bytes = ew * stn[:, mm.ST_STAGED_DEG] + 36 * stn[:, mm.ST_STAGED_ITEMS]
-    short_bytes = (ew * (stn[:, mm.ST_BLUE_DEG] - stn[:, mm.ST_STAGED_DEG])
-                   + 36 * np.maximum(stn[:, mm.ST_BLUE] - stn[:, mm.ST_STAGED_ITEMS], 0))
-    kernels = {"k_phase_a_long (long-list scan)": (staged_bytes, ms_k[:, 1]),
-               "k_phase_a_short (short-list scan)": (short_bytes, ms_k[:, 0])}
-    dom = max(kernels, key=lambda k: kernels[k][1].sum())
-    dom_bytes, dom_ms = kernels[dom]
-    achieved = dom_bytes.sum() / (dom_ms.sum() / 1e3) / 1e9
+    nr = min(x.shape[0] for x in prof)
+    ms_k = np.mean(np.stack([x[:nr] for x in prof]), axis=0)  # [executed rounds, (window, fallback, commit, sum)]
+    gpu_launches = args.steps * 1
+    phase_bytes = {"window": work["window_bytes"][:nr], "fallback": work["fallback_bytes"][:nr],
+                   "commit": work["commit_bytes"][:nr]}
+    kernel_bytes = work["kernel_bytes"]
+    # the round kernel is the only kernel of a matching: its bytes over the whole step's device time
+    achieved = kernel_bytes / (ms / 1e3) / 1e9
     peak, peak_kind = load_peaks()
     traffic = None
     tfile = ROOT / "profiles" / f"traffic_{args.workload}.json"
     if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get("dominant_bytes_per_launch")
+        traffic = json.loads(tfile.read_text()).get("dram_bytes_per_launch")
 
     # end to end through the C ABI with host buffers (pinned)
     ranges_h = torch.from_numpy(np.ascontiguousarray(g.ranges, dtype=np.int32)).pin_memory()
@@ -388,18 +383,20 @@ def main():
             "e2e": {"value": e2e_value, "unit": "edges/s", "ms_per_step": e2e, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_create": e2e_split[0], "ms_first_match": e2e_split[1],
                     "ms_destroy": e2e_split[2], **e2e_detail},
-            "roofline": {"bound": "hbm", "kernel": dom,
+            "roofline": {"bound": "hbm", "kernel": "k_rounds (whole matching: set-up, scan and commit phases)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_kind": peak_kind,
-                         "bytes_per_launch": float(dom_bytes.mean()), "launches": int(nr),
-                         "ms_short_scan": float(ms_k[:, 0].sum()), "ms_staged_scan": float(ms_k[:, 1].sum()),
-                         "ms_commit": float(ms_k[:, 2].sum()), "ms_tail": ms_tail,
-                         "per_round_work": {k: [int(x) for x in stn[:, c]] for k, c in
-                                            (("blue", mm.ST_BLUE), ("blue_entries", mm.ST_BLUE_DEG),
-                                             ("long_entries", mm.ST_STAGED_DEG),
-                                             ("long_pieces", mm.ST_STAGED_ITEMS))},
-                         "per_round_ms": {"short": [round(float(x), 4) for x in ms_k[:, 0]],
-                                          "staged": [round(float(x), 4) for x in ms_k[:, 1]],
+                         "bytes_per_launch": kernel_bytes, "launches_per_step": 1,
+                         "phases": {k: {"ms": float(ms_k[:, c].sum()), "bytes": float(phase_bytes[k].sum()),
+                                        "gbs": float(phase_bytes[k].sum() / max(ms_k[:, c].sum(), 1e-9) / 1e6),
+                                        "frac": float(phase_bytes[k].sum() / max(ms_k[:, c].sum(), 1e-9) / 1e6 / peak)}
+                                    for c, k in enumerate(("window", "fallback", "commit"))},
+                         "per_round_work": {k: [int(x) for x in st[:nr, c]] for k, c in
+                                            (("active", mm.ST_ACTIVE), ("blue", mm.ST_BLUE),
+                                             ("blue_entries", mm.ST_BLUE_DEG), ("window_entries", mm.ST_WINDOW_ENTRIES),
+                                             ("fallback_entries", mm.ST_STAGED_DEG), ("matched", mm.ST_MATCHED))},
+                         "per_round_ms": {"window": [round(float(x), 4) for x in ms_k[:, 0]],
+                                          "fallback": [round(float(x), 4) for x in ms_k[:, 1]],
                                           "commit": [round(float(x), 4) for x in ms_k[:, 2]]},
                          "reference_formula_gbs": work["reference_bytes"] / (ms / 1e3) / 1e9},
             "gpu_launches": gpu_launches,

@@ -65,7 +65,7 @@ enum {
 };
 
 /* Number of int64 counters per round written by mm_match_stats. */
-#define MM_STATS_COLS 10
+#define MM_STATS_COLS 11
 enum {
     MM_ST_ACTIVE = 0,     /* vertices that could still be matched at the round's colouring */
     MM_ST_BLUE = 1,       /* of those, coloured blue */
@@ -75,8 +75,9 @@ enum {
     MM_ST_BLUE_DEG = 5,   /* sum of degrees of blue vertices */
     MM_ST_RED_DEG = 6,    /* sum of degrees of red vertices */
     MM_ST_MATCHED = 7,    /* vertices matched in the round */
-    MM_ST_STAGED_DEG = 8,   /* push path: entries its staged long-list scan read */
-    MM_ST_STAGED_ITEMS = 9  /* push path: lists and chunks that scan handled */
+    MM_ST_STAGED_DEG = 8,   /* push path: entries its fallback (full-list) scan read */
+    MM_ST_STAGED_ITEMS = 9, /* push path: list pieces that scan handled */
+    MM_ST_WINDOW_ENTRIES = 10 /* push path: preference-window entries the blue scans read */
 };
 
 typedef struct mm_graph mm_graph;
@@ -155,15 +156,16 @@ mm_status mm_match_stats(mm_graph *g, int type, uint32_t barrier, const uint32_t
                          int stats_rounds, int path, void *stream);
 
 /*
- * Measurement entry: the push path's kernels launched one by one from the host
- * with CUDA events on `stream` around each launch (it synchronises once per
- * round, so it is slower than mm_match_device and only meant for timing the
- * individual kernels).  ms_per_kernel[r * MM_PROFILE_KERNELS + k] receives the
- * duration of round r's kernel k for r < cap_rounds: k = 0 short-list scan,
- * 1 staged long-list scan, 2 commit/recolour; the row after the last such
- * round holds in k = 3 the single-block tail kernel that runs the remaining
- * small rounds.  *launches receives the number of kernels launched (init,
- * 3 per grid round, tail, finish).  Same matching result.
+ * Measurement entry: the same single launch of the round kernel as
+ * mm_match_device, with timestamps taken by the kernel as its grid barriers
+ * complete (the device's global timer, nanoseconds).
+ * ms_per_kernel[r * MM_PROFILE_KERNELS + k] receives, for each round r <
+ * cap_rounds that the kernel executed, k = 0 the window scan (blue vertices'
+ * preference windows and proposals), k = 1 the fallback scan of lists longer
+ * than their window (0 in rounds without one), k = 2 the commit phase
+ * (commit, recolour, worklist compaction), k = 3 their sum; rows of rounds
+ * not executed are zero.  *launches receives the number of kernels launched
+ * (1).  Same matching result.
  */
 #define MM_PROFILE_KERNELS 4
 mm_status mm_match_profile(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds,

@@ -36,10 +36,10 @@ PATH_AUTO, PATH_PULL, PATH_PUSH = 0, 1, 2
 # Default select barrier of the reference CLI (bin/match.cpp:183): p(blue) ~ 0.534.
 DEFAULT_BARRIER = 0x88B81733
 
-STATS_COLS = 10
-PROFILE_KERNELS = 4  # short-list scan, staged long-list scan, commit/recolour, tail
+STATS_COLS = 11
+PROFILE_KERNELS = 4  # window scan, fallback scan, commit/recolour, their sum
 (ST_ACTIVE, ST_BLUE, ST_RED, ST_REQ_ENTRIES, ST_RESP_ENTRIES, ST_BLUE_DEG, ST_RED_DEG, ST_MATCHED,
- ST_STAGED_DEG, ST_STAGED_ITEMS) = range(10)
+ ST_STAGED_DEG, ST_STAGED_ITEMS, ST_WINDOW_ENTRIES) = range(11)
 
 STATUS = {0: "MM_OK", 1: "MM_ERR_ARG", 2: "MM_ERR_GRAPH", 3: "MM_ERR_CUDA", 4: "MM_ERR_NOMEM",
           5: "MM_ERR_UNSUPPORTED", 6: "MM_ERR_SEEDS", 7: "MM_ERR_DEVICE"}
@@ -287,11 +287,12 @@ class DeviceGraph:
 
 
     def profile(self, type_: int, seeds: np.ndarray, d_out: int, barrier: int = DEFAULT_BARRIER, stream: int = 0):
-        """Host-stepped run with CUDA events per launch.
+        """Timed run of the round kernel with barrier timestamps.
 
-        Returns (rounds, ms[r, k], launches) with k = 0 short-list scan,
-        1 staged long-list scan, 2 commit/recolour (one row per grid round),
-        then a last row with the single-block tail kernel's time in k = 3."""
+        Returns (rounds, ms[r, k], launches): one row per round the kernel
+        executed, k = 0 window scan (blue preference windows + proposals),
+        1 fallback scan of longer lists, 2 commit (commit + recolour +
+        compaction), 3 their sum; launches is 1."""
         seeds = np.ascontiguousarray(seeds, dtype=np.uint32)
         rounds = ctypes.c_int(0)
         launches = ctypes.c_int(0)
@@ -299,8 +300,8 @@ class DeviceGraph:
         _check(self._lib.mm_match_profile(self.handle, type_, barrier, _ptr(seeds), len(seeds), d_out,
                                           ctypes.byref(rounds), _ptr(ms), 255, ctypes.byref(launches),
                                           stream or None))
-        grid_rounds = (launches.value - 3) // 3
-        return rounds.value, ms[: grid_rounds + 1], launches.value
+        executed = int(np.count_nonzero(ms[:, 3] > 0))
+        return rounds.value, ms[:executed], launches.value
 
 
 def roofline_bytes(stats: np.ndarray, weighted: bool) -> dict:
@@ -309,20 +310,38 @@ def roofline_bytes(stats: np.ndarray, weighted: bool) -> dict:
     reference_bytes: the bytes the reference's round loop must move,
         sum_r [24 |A_r| + (4 + 4 w) E_r] with E_r the entries its request and
         respond loops inspect (gathers of match/requests assumed L2-resident).
-    push_bytes: the bytes the push path must move: blue lists only,
-        sum_r [(4 + 4 w) blue_deg_r + 40 |blue_r| + 24 |red_r|].
+    window_bytes[r]: the window scan: 32 per blue vertex (worklist item 16,
+        reverse key 8, request 8) and per window entry read 8 (weighted:
+        neighbour + position) or 4 (random: neighbour).
+    fallback_bytes[r]: the fallback scan: (4 + 4 w) per entry and 36 per list
+        piece (item 16, proposal 20).
+    commit_bytes[r]: the commit phase: 41 per active vertex (item 16,
+        request or best key 8, colour 1, next worklist item 16) minus 12 per
+        matched vertex (match value 4 written, no next item).
+    init_bytes: the set-up pass, 33 per vertex (range 8, colour 1, best key 8,
+        worklist item 16), 41 with the weighted types' window offset.
     edges: sum_r E_r (edges traversed, for TEPS).
     """
     ew = 8 if weighted else 4
     act = stats[:, ST_ACTIVE].astype(np.float64)
     e = stats[:, ST_REQ_ENTRIES].astype(np.float64) + stats[:, ST_RESP_ENTRIES]
     blue = stats[:, ST_BLUE].astype(np.float64)
-    red = stats[:, ST_RED].astype(np.float64)
-    bdeg = stats[:, ST_BLUE_DEG].astype(np.float64)
+    matched = stats[:, ST_MATCHED].astype(np.float64)
+    win = stats[:, ST_WINDOW_ENTRIES].astype(np.float64)
+    fb = stats[:, ST_STAGED_DEG].astype(np.float64)
+    pieces = stats[:, ST_STAGED_ITEMS].astype(np.float64)
+    window = 32 * blue + (8 if weighted else 4) * win
+    fallback = ew * fb + 36 * pieces
+    commit = 41 * act - 12 * matched
+    init = (41 if weighted else 33) * float(act[0]) if len(act) else 0.0
     return {
         "edges": float(e.sum()),
         "reference_bytes": float((24 * act + ew * e).sum()),
-        "push_bytes": float((ew * bdeg + 40 * blue + 24 * red).sum()),
+        "window_bytes": window,
+        "fallback_bytes": fallback,
+        "commit_bytes": commit,
+        "init_bytes": init,
+        "kernel_bytes": float(window.sum() + fallback.sum() + commit.sum() + init),
     }
 
 

@@ -60,10 +60,13 @@ def build_mmatch(verbose: bool = False) -> Path:
         if _newer(o, [s] + _headers() + [Path(__file__)]):
             _run([NVCC, *NVCC_FLAGS, "-c", s, "-o", o], verbose)
         objs.append(o)
+    script = OBJ / "mmatch.map"
+    script.write_text("{ global: mm_*; local: *; };\n")
     if _newer(out, objs):
-        # static cudart, all foreign symbols hidden: only the mm_* API is exported
+        # static cudart, and a version script: only the mm_* C ABI is exported
+        # (template instantiations from C++ headers would otherwise leak as weak symbols)
         _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", out, *objs,
-              "-Xlinker", "--exclude-libs,ALL"], verbose)
+              "-Xlinker", "--exclude-libs,ALL", "-Xlinker", f"--version-script={script}"], verbose)
     return out
 
 

@@ -96,6 +96,8 @@ struct mm_graph {
     // push path: reverse proposal keys, one per adjacency slot, per weighting
     unsigned long long *d_revkey[2] = {nullptr, nullptr};  // [0] random, [1] weighted
     long long *d_slot_off = nullptr;  // non-contiguous CSR: slot index of vertex v's first entry
+    int2 *d_pwin = nullptr;           // weighted types: preference windows {neighbour, position | flag}
+    long long *d_pwin_off = nullptr;  // weighted types: first window slot of each vertex; [n] = total
 
     // push path: captured CUDA graph of the round loop
     void *push_exec = nullptr;  // internal (mm::PushPlan *)

@@ -2,7 +2,7 @@
 //
 // Same matching as the reference's GPU round (src/matchgpu.cu:184-451), with
 // the work re-cut so that each round streams only the adjacency lists of BLUE
-// vertices and the loop never returns to the host.
+// vertices, and the whole loop runs in one cooperative kernel launch.
 //
 // Reformulation (exact, for any CSR the reference accepts):
 //   * Respond (grRespond / gwRespond, matchgpu.cu:329-357, 411-451) lets red r
@@ -30,25 +30,25 @@
 // neighbourRanges again.
 //   short lists (deg <= 32)   a warp takes 32 blue vertices and walks their
 //                             concatenated entries row by row, 32 consecutive
-//                             entries per load (k_phase_a_short)
+//                             entries per load (scan_short)
 //   long lists  (deg  > 32)   blue ones are appended with their offset in the
 //                             round's concatenated long-list entry space; that
 //                             space is cut into 512-entry segments and a warp
-//                             walks one segment row by row (k_phase_a_long).
+//                             walks one segment row by row (scan_long).
 //                             A list cut by segment edges is combined by
 //                             atomics and its last piece proposes.  Every warp
-//                             claims equal amounts of work whatever the skew.
+//                             gets equal amounts of work whatever the skew.
 // Every load of neighbour ids and weights is a coalesced row of 32 consecutive
-// entries; a list's best entry is kept as a 64-bit key (weight order << 32 |
+// entries.  A list's best entry is kept as a 64-bit key (weight order << 32 |
 // ~position) max-combined in shared memory, which orders ties by position
 // exactly as the reference's strict ">" scan in list order does.
-// The two scans run concurrently.
 //
-// Round t is three kernels: the two phase-A scans (blue scan + proposal) and
-// phase B (commit + recolour + worklist compaction).  They form the body of a
-// CUDA graph WHILE node; the last block of phase B decides whether another
-// round runs (cudaGraphSetConditional), so there is no host synchronisation
-// inside the loop.
+// Loop.  k_rounds is launched cooperatively (all blocks resident) and runs
+// set-up, then per round the scan phase (A: blue scans + proposals) and the
+// commit phase (B: commit + recolour + worklist compaction), with bounded grid
+// barriers in between.  Nothing returns to the host until the matching is
+// maximal (the reference copies a flag back every round, matchgpu.cu:607-614),
+// and no round pays for kernel launches.
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
@@ -62,14 +62,17 @@
 namespace mm {
 namespace {
 
-constexpr int kBlockA = 256;
-constexpr int kBlockB = 256;
+constexpr int kThreads = 512;            // threads per block of the round kernel
+constexpr int kWarps = kThreads / 32;
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kSmallMax = 32;       // short lists: degree <= 32
-constexpr int kSegEntries = 512;    // entries per long-list segment (at most 16 pieces of lists > 32)
+constexpr int kWin = 32;                 // preference window: the first min(deg, 32) choices
+constexpr int kSegEntries = 992;         // entries per fallback segment: 31 rows of 32; at most 32
+                                         // pieces of lists > 32 entries overlap one segment
 
-// Worklists.  kStaged holds blue long lists with their entry offsets.
-enum : int { kBlueS = 0, kRedS, kRedLong, kStaged, kLists };
+// Worklists: blue and red vertices by round parity; the staged list holds the round's
+// fallback lists (blue lists longer than the window with no red choice in
+// it) with their offsets in the concatenated fallback entry space.
+enum : int { kBlue = 0, kRed = 1, kParityLists = 2 };
 
 struct Ctl {
     int *match;            // output array of this call
@@ -77,17 +80,11 @@ struct Ctl {
     int cap;               // 20 or 255
     int maximal;
     int nseeds;
-    int t;                 // 0-based index of the round being executed
     int rounds;            // rounds the reference executes (set at loop exit)
-    int status;            // 0 ok, 1 seeds exhausted, 2 a bounded device wait gave up
-    int cont;              // 1 while another round follows (read by the stepped driver)
-    unsigned ticket;       // phase-B block arrivals
-    int task_short[2];     // phase-A cursors by round parity: short-list batches
-    int task_long[2];      //   and long-list segments
-    int cnt[2][kLists];    // worklist lengths by round parity (kStaged unused)
-    unsigned long long staged_pack[2];  // kStaged: (items << 32) | entries, by parity
+    int status;            // 0 ok, 1 seeds exhausted, 2 a bounded grid-barrier wait gave up
+    int cnt[2][kParityLists];      // worklist lengths by round parity
+    unsigned long long staged_pack;  // fallback list of the round: (items << 32) | entries
     int retired[2];        // vertices of the round that were unmatchable as soon as coloured
-    int tail;              // 1: the remaining rounds run in the single-block tail kernel
 };
 
 struct Params {
@@ -98,21 +95,26 @@ struct Params {
     const float *w;
     const unsigned long long *revkey;
     const long long *slot_off;
+    const int2 *pwin;               // weighted: preference windows {neighbour, position | flag}
+    const long long *pwin_off;      // weighted: first window slot of each vertex (< 2^31)
     uint8_t *col;
     int2 *req;
     unsigned long long *best;       // per red vertex: max proposal key this round
-    unsigned long long *part_key;   // per cut long list: max over finished pieces
-    int *part_cnt;                  // per cut long list: finished pieces
-    int4 *lists[2][kLists];         // items {v, begin, end, offset} by parity and list id
-    int *seg_first[2];              // per staged segment: item holding its first entry
+    unsigned long long *part_key;   // per cut fallback list: max over finished pieces
+    int *part_cnt;                  // per cut fallback list: finished pieces
+    int4 *lists[2][kParityLists];   // items {v, begin, end, window offset} by parity and colour
+    int4 *staged;                   // fallback items {v, begin, end, entry offset}
+    int *seg_first;                 // per fallback segment: item holding its first entry
     const uint32_t *seeds;
     Ctl *ctl;
     unsigned long long *stats;      // [kMaxRounds][MM_STATS_COLS] or null
-    cudaGraphConditionalHandle loop;
+    unsigned long long *tstamp;     // [3 * kMaxRounds + 1] barrier times (ns) or null
+    unsigned *bar;                  // [kBarWords] grid barrier words, zero at launch
 };
 
 __device__ __forceinline__ int degree_of(int2 r) { return r.y > r.x ? r.y - r.x : 0; }
 __device__ __forceinline__ int degree_of(int4 it) { return it.z > it.y ? it.z - it.y : 0; }
+__device__ __forceinline__ int win_len(int deg) { return deg < kWin ? deg : kWin; }
 
 __device__ __forceinline__ int warp_incl_scan(int v)
 {
@@ -130,6 +132,78 @@ __device__ __forceinline__ void stat_add(const Params &p, int round, int col, un
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFull, v, o);
     if ((threadIdx.x & 31) == 0 && v) atomicAdd(&p.stats[(size_t)round * MM_STATS_COLS + col], v);
+}
+
+// ---- grid barrier ----
+//
+// The round kernel is launched cooperatively, so all its blocks are resident
+// at once and a barrier over them cannot deadlock on scheduling.  Blocks
+// arrive in groups of kBarGroup on their group's word, and the last of each
+// group arrives on the top word, which every block polls; each word sits in
+// its own 128-byte line, so no word sees more than kBarGroup (or group-count)
+// atomics per barrier.  Every word uses the same counting: the first member
+// adds 2^31 - (members - 1), every other member adds 1, so the top bit flips
+// exactly when the last member arrives and the low bits return to where they
+// were.  Each wait is still bounded: after kSpinLimit polls the block records
+// status 2 and the kernel returns; the other blocks then give up at their next
+// barrier.  Thread 0's fences (release before arriving, acquire after the
+// wait), with the block barriers around them, make every block's writes of
+// the phase visible to every thread of every block afterwards.
+constexpr long long kSpinLimit = 1ll << 22;
+constexpr int kBarGroup = 16;
+constexpr int kBarStride = 32;   // words per barrier line (128 bytes)
+constexpr int kBarMaxGroups = 64;
+constexpr int kBarWords = (kBarMaxGroups + 1) * kBarStride;  // group words, then the top word
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __noinline__ bool grid_sync(unsigned *bar, Ctl *ctl, unsigned long long *tstamp, int mark)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned nb = gridDim.x, b = blockIdx.x;
+        const unsigned g = b / kBarGroup, ngroups = (nb + kBarGroup - 1) / kBarGroup;
+        const unsigned gsize = min((unsigned)kBarGroup, nb - g * kBarGroup);
+        unsigned *gword = bar + g * kBarStride;
+        unsigned *top = bar + kBarMaxGroups * kBarStride;
+        const unsigned top_before = ld_acquire(top);  // cannot flip before this block arrives
+        fence_acq_rel();
+        const unsigned ginc = b % kBarGroup == 0 ? 0x80000000u - (gsize - 1u) : 1u;
+        const unsigned gold = atomicAdd(gword, ginc);
+        if (((gold + ginc) ^ gold) & 0x80000000u) {  // last of the group
+            const unsigned tinc = g == 0 ? 0x80000000u - (ngroups - 1u) : 1u;
+            atomicAdd(top, tinc);
+        }
+        int ok = 1;
+        long long it = 0;
+        while (((top_before ^ ld_acquire(top)) & 0x80000000u) == 0u) {
+            if (++it > kSpinLimit) {
+                ok = 0;
+                break;
+            }
+            if (it > 64) __nanosleep(32);
+        }
+        fence_acq_rel();
+        if (!ok) atomicExch(&ctl->status, 2);
+        s_ok = ok;
+        if (tstamp && b == 0 && mark >= 0) tstamp[mark] = global_ns();
+    }
+    __syncthreads();
+    return s_ok != 0;
 }
 
 // Key under which a blue vertex ranks a red neighbour at position j
@@ -152,46 +226,6 @@ __device__ __forceinline__ unsigned long long entry_key(uint8_t c, int j, float 
     return c == kMatched ? 0ull : 1ull;
 }
 
-// Finish blue vertex v after its scan: dead, no proposal, or propose.
-__device__ __forceinline__ void propose(const Params &p, int v, int begin, unsigned long long key)
-{
-    if (key == 0) {  // no unmatched neighbour: unmatchable (requests == n + 1)
-        p.col[v] = kDead;
-        p.ctl->match[v] = 2;
-        p.req[v] = make_int2(-1, 0);
-        return;
-    }
-    if (key == 1) {  // unmatched neighbours but no red one to propose to
-        p.req[v] = make_int2(-2, 0);
-        return;
-    }
-    const int j = (int)~(uint32_t)key;
-    const int target = p.nbrs[j];
-    const long long slot = p.contiguous ? (long long)j : p.slot_off[v] + (j - begin);
-    const unsigned long long rk = p.revkey[slot];
-    if (rk) atomicMax(&p.best[target], rk);
-    p.req[v] = make_int2(target, (int)(uint32_t)rk);
-}
-
-// Adjacency entries the reference's request loop inspects for this vertex
-// (random mode stops at the first red neighbour).
-template <bool kW>
-__device__ __forceinline__ unsigned long long request_seen(int begin, int deg, unsigned long long key)
-{
-    if (kW || key < 2) return (unsigned long long)deg;
-    return (unsigned long long)((int)~(uint32_t)key - begin + 1);
-}
-
-template <bool kW, bool kStats>
-__device__ __forceinline__ void propose_counted(const Params &p, int4 it, unsigned long long key, int t)
-{
-    if (kStats) {
-        atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_REQ_ENTRIES], request_seen<kW>(it.y, degree_of(it), key));
-        atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_BLUE_DEG], (unsigned long long)degree_of(it));
-    }
-    propose(p, it.x, it.y, key);
-}
-
 // Key of a scan's best entry: weight order and position of its best red
 // neighbour (the reference's rule: strict > from -1 in list order), else 1 if
 // an unmatched neighbour was seen, else 0.
@@ -203,101 +237,151 @@ __device__ __forceinline__ unsigned long long strip_key(float bw, int bj, bool a
     return alive ? 1ull : 0ull;
 }
 
-constexpr int kShortStep = 8;  // entries a tail thread loads (and gathers) at once
-constexpr int kRows = 4;       // rows of 32 entries a warp keeps in flight in the grid scans
+// Fold one scanned entry (neighbour colour c, weight w, position j) into a
+// lane's running best: strict > from -1 over increasing positions, so ties
+// keep the earliest entry; in random mode the first red entry.
+template <bool kW>
+__device__ __forceinline__ void fold_entry(uint8_t c, float w, int j, float &bw, int &bj, bool &alive)
+{
+    alive |= c != kMatched;
+    if (c == kRed) {
+        const float x = kW ? w : 0.0f;
+        if (x > bw) {
+            bw = x;
+            bj = j;
+        }
+    }
+}
+
+// Blue vertex v proposes to `target`, the neighbour at position j of its list
+// (begin = first position): the reverse key of that slot goes to best[target].
+__device__ __forceinline__ void propose_to(const Params &p, int v, int begin, int j, int target)
+{
+    const long long slot = p.contiguous ? (long long)j : __ldg(p.slot_off + v) + (j - begin);
+    const unsigned long long rk = __ldg(p.revkey + slot);
+    if (rk) atomicMax(&p.best[target], rk);
+    p.req[v] = make_int2(target, (int)(uint32_t)rk);
+}
+
+// Blue vertex v without a red choice: unmatchable if no neighbour is
+// unmatched (requests == n + 1), else no proposal this round.
+__device__ __forceinline__ void no_proposal(const Params &p, int v, bool alive)
+{
+    if (!alive) {
+        p.col[v] = kDead;
+        p.ctl->match[v] = 2;
+        p.req[v] = make_int2(-1, 0);
+    } else {
+        p.req[v] = make_int2(-2, 0);
+    }
+}
+
+// Finish blue vertex v after a full scan whose result is `key`.
+__device__ __forceinline__ void propose(const Params &p, int v, int begin, unsigned long long key)
+{
+    if (key < 2) {
+        no_proposal(p, v, key == 1);
+        return;
+    }
+    const int j = (int)~(uint32_t)key;
+    propose_to(p, v, begin, j, __ldg(p.nbrs + j));
+}
+
+// Adjacency entries the reference's request loop inspects for this vertex
+// (random mode stops at the first red neighbour, at position j).
+template <bool kW>
+__device__ __forceinline__ unsigned long long request_seen(int begin, int deg, int j)
+{
+    if (kW || j < 0) return (unsigned long long)deg;
+    return (unsigned long long)(j - begin + 1);
+}
+
+template <bool kW, bool kStats>
+__device__ __forceinline__ void propose_counted(const Params &p, int4 it, unsigned long long key, int t)
+{
+    if (kStats) {
+        const int j = key >= 2 ? (int)~(uint32_t)key : -1;
+        atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_REQ_ENTRIES], request_seen<kW>(it.y, degree_of(it), j));
+        atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_BLUE_DEG], (unsigned long long)degree_of(it));
+    }
+    propose(p, it.x, it.y, key);
+}
+
+constexpr int kRows = 4;    // fallback scan: rows of 32 entries per iteration
+constexpr int kStages = 3;  // fallback scan: iterations staged in shared memory (2 loading, 1 in use)
+
+// Fallback-scan staging of one warp: neighbour ids and weights of kStages
+// iterations, written by cp.async.
+struct LongStage {
+    int nb[kStages][kRows * 32];
+    float w[kStages][kRows * 32];
+};
+
+// Shared memory of the round kernel (dynamic).
+struct Smem {
+    int delta[kWarps][33];                // fallback scan: global position of segment entry e = e + delta[k]
+    int pend[kWarps][33];                 // fallback scan: segment-relative end of each piece
+    LongStage stage[kWarps];
+    int tile_warp[kWarps][2];             // compaction: per-warp counts, then offsets
+    int tile_base[2];                     // compaction: tile bases
+};
 
 // ---- worklist compaction for the set-up and commit passes ----
 //
 // A block handles tiles of kTileItems vertices, kPer per thread.  Each thread
 // decides the next list of its vertices; the block counts them per list with
-// warp scans, takes one atomic per list and tile (the staged list's item and
-// entry counts in one 64-bit atomic), and writes its items.
+// warp scans, takes one atomic per list and tile, and writes its items.
 
-constexpr int kBlockT = 512;
 constexpr int kPer = 4;
-constexpr int kTileItems = kBlockT * kPer;
-constexpr int kWarpsT = kBlockT / 32;
+constexpr int kTileItems = kThreads * kPer;
 
-// dest[k]: -1 (drop) or the list id kBlueS, kRedS, kRedLong, kStaged.
-__device__ __forceinline__ void compact_tile(const Params &p, int parity, const int (&dest)[kPer],
+// dest[k]: -1 (drop), kBlue or kRed.
+__device__ __forceinline__ void compact_tile(const Params &p, Smem &sm, int parity, const int (&dest)[kPer],
                                              const int4 (&item)[kPer])
 {
-    __shared__ int s_warp[kWarpsT][5];  // per-warp counts, then per-warp offsets within the tile
-    __shared__ int s_base[5];           // tile bases: 4 list indices, then the staged entry offset
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int c[4] = {0, 0, 0, 0}, ent = 0;
+    int c[2] = {0, 0};
 #pragma unroll
     for (int k = 0; k < kPer; ++k) {
-#pragma unroll
-        for (int l = 0; l < 4; ++l) c[l] += dest[k] == l;
-        if (dest[k] == kStaged) ent += degree_of(item[k]);
+        c[0] += dest[k] == kBlue;
+        c[1] += dest[k] == kRed;
     }
-    int ex[5];
+    int ex[2];
 #pragma unroll
-    for (int l = 0; l < 5; ++l) {
-        const int v = l < 4 ? c[l] : ent;
-        const int incl = warp_incl_scan(v);
-        ex[l] = incl - v;
-        if (lane == 31) s_warp[warp][l] = incl;
+    for (int l = 0; l < 2; ++l) {
+        const int incl = warp_incl_scan(c[l]);
+        ex[l] = incl - c[l];
+        if (lane == 31) sm.tile_warp[warp][l] = incl;
     }
     __syncthreads();
-    if (threadIdx.x < 4) {
+    if (threadIdx.x < 2) {
         const int l = threadIdx.x;
         int run = 0;
-        for (int w = 0; w < kWarpsT; ++w) {
-            const int x = s_warp[w][l];
-            s_warp[w][l] = run;
+        for (int w = 0; w < kWarps; ++w) {
+            const int x = sm.tile_warp[w][l];
+            sm.tile_warp[w][l] = run;
             run += x;
         }
-        if (l < kStaged) {
-            s_base[l] = run ? atomicAdd(&p.ctl->cnt[parity][l], run) : 0;
-        } else {
-            int run_e = 0;
-            for (int w = 0; w < kWarpsT; ++w) {
-                const int x = s_warp[w][4];
-                s_warp[w][4] = run_e;
-                run_e += x;
-            }
-            unsigned long long old = 0;
-            if (run) old = atomicAdd(&p.ctl->staged_pack[parity], ((unsigned long long)run << 32) | (unsigned)run_e);
-            s_base[3] = (int)(old >> 32);
-            s_base[4] = (int)(old & 0xffffffffull);
-        }
+        sm.tile_base[l] = run ? atomicAdd(&p.ctl->cnt[parity][l], run) : 0;
     }
     __syncthreads();
-    int rc[4] = {0, 0, 0, 0}, re = 0;
+    int rc[2] = {0, 0};
 #pragma unroll
     for (int k = 0; k < kPer; ++k) {
         const int l = dest[k];
         if (l < 0) continue;
-        int idx = 0;
-#pragma unroll
-        for (int m = 0; m < 4; ++m)
-            if (l == m) idx = s_base[m] + s_warp[warp][m] + ex[m] + rc[m]++;
-        if (l != kStaged) {
-            p.lists[parity][l][idx] = item[k];
-        } else {
-            const int deg = degree_of(item[k]);
-            const int off = s_base[4] + s_warp[warp][4] + ex[4] + re;
-            re += deg;
-            p.lists[parity][kStaged][idx] = make_int4(item[k].x, item[k].y, item[k].z, off);
-            for (int s = (off + kSegEntries - 1) / kSegEntries; s * kSegEntries < off + deg; ++s)
-                p.seg_first[parity][s] = idx;
-        }
+        const int idx = l == kBlue ? sm.tile_base[0] + sm.tile_warp[warp][0] + ex[0] + rc[0]++
+                                   : sm.tile_base[1] + sm.tile_warp[warp][1] + ex[1] + rc[1]++;
+        p.lists[parity][l][idx] = item[k];
     }
-    __syncthreads();  // s_warp / s_base are reused by the next tile
+    __syncthreads();  // tile_warp / tile_base are reused by the next tile
 }
 
-__device__ __forceinline__ int next_list(bool blue, int deg)
-{
-    if (deg > kSmallMax) return blue ? kStaged : kRedLong;
-    return blue ? kBlueS : kRedS;
-}
-
-// Round set-up: colour every vertex with seeds[0], clear proposal slots, and
-// fill the first worklists.
-template <bool kStats>
-__global__ void __launch_bounds__(kBlockT) k_init(Params p)
+// Set-up: colour every vertex with seeds[0] and fill the first worklists.
+// best[] starts at 0 and stays 0 for every vertex that is not matched: a red
+// vertex that receives a proposal is matched in the same round.
+template <bool kW, bool kStats>
+__device__ void init_phase(const Params &p, Smem &sm)
 {
     const Ctl *ctl = p.ctl;
     const uint32_t seed = p.seeds[0], barrier = ctl->barrier;
@@ -309,17 +393,18 @@ __global__ void __launch_bounds__(kBlockT) k_init(Params p)
         unsigned long long act = 0, blue_n = 0;
 #pragma unroll
         for (int k = 0; k < kPer; ++k) {
-            const int v = tile * kTileItems + k * kBlockT + threadIdx.x;
+            const int v = tile * kTileItems + k * kThreads + threadIdx.x;
             dest[k] = -1;
             item[k] = make_int4(v, 0, 0, 0);
             if (v < n) {
-                const int2 r = p.ranges[v];
+                const int2 r = __ldg(p.ranges + v);
                 item[k].y = r.x;
                 item[k].z = r.y;
+                if (kW) item[k].w = (int)__ldg(p.pwin_off + v);
                 const int deg = degree_of(r);
                 const bool blue = colour_of((uint32_t)v, seed, barrier) == kBlue;
                 p.best[v] = 0ull;
-                if (deg > kSmallMax) {
+                if (deg > kWin) {
                     p.part_key[v] = 0ull;
                     p.part_cnt[v] = 0;
                 }
@@ -330,7 +415,7 @@ __global__ void __launch_bounds__(kBlockT) k_init(Params p)
                     p.ctl->match[v] = 2;
                 } else {
                     p.col[v] = blue ? kBlue : kRed;
-                    dest[k] = next_list(blue, deg);
+                    dest[k] = blue ? kBlue : kRed;
                 }
             }
         }
@@ -339,98 +424,155 @@ __global__ void __launch_bounds__(kBlockT) k_init(Params p)
             stat_add(p, 0, MM_ST_BLUE, blue_n);
             stat_add(p, 0, MM_ST_RED, act - blue_n);
         }
-        compact_tile(p, 0, dest, item);
+        compact_tile(p, sm, 0, dest, item);
     }
 }
 
-// Phase A, short lists: a warp claims 32 blue short-list vertices, lays their
-// entries end to end (at most 1024) and walks them in rows of 32: lane l of
-// row r takes entry 32r + l, so every load is one coalesced row.  The owner of
-// each entry comes from a byte table the lanes fill for their own lists; keys
-// are max-combined per list in shared memory.  Block 0 also resets the next
-// round's list counters and cursors.
-constexpr int kWarpsA = kBlockA / 32;
+// ---- phase A1: preference windows ----
+//
+// A blue vertex picks the entry the reference's request loop would pick
+// (gwRequest: the heaviest red neighbour, strict > from -1, earliest position
+// on ties; grRequest: the first red neighbour in list order).  Its candidates
+// in that order of preference are its window: for weighted types the
+// preparation step sorts each list's best min(deg, 32) entries by (weight,
+// earlier position) into pwin, with entries whose weight can never be picked
+// (<= -1 or NaN) flagged and last; for random types the window is simply the
+// first min(deg, 32) entries of the list.  So the first red candidate in the
+// window is the reference's choice, and the scan stops there.  A list that
+// fits in its window and has no red candidate is decided too (unmatchable iff
+// no entry is unmatched).  A longer list with no red candidate in its window
+// falls back to a full scan in phase A2: it is appended to the round's
+// fallback list.  Each thread walks kPerW vertices at once, two window entries
+// per vertex and step.
+constexpr int kPerW = 2;
 
 template <bool kW, bool kStats>
-__global__ void __launch_bounds__(kBlockA) k_phase_a_short(Params p)
+__device__ void scan_window(const Params &p, int t, int par)
 {
-    __shared__ unsigned long long s_acc[kWarpsA][32];
-    __shared__ int s_delta[kWarpsA][32];
-    __shared__ uint8_t s_owner[kWarpsA][32 * kSmallMax];
     Ctl *ctl = p.ctl;
-    const int t = ctl->t;
-    const int par = t & 1;
-    const int n_short = ctl->cnt[par][kBlueS];
-    if (blockIdx.x == 0 && threadIdx.x < kLists) ctl->cnt[par ^ 1][threadIdx.x] = 0;
-    if (blockIdx.x == 0 && threadIdx.x == 32) {
-        ctl->task_short[par ^ 1] = 0;
-        ctl->task_long[par ^ 1] = 0;
-        ctl->staged_pack[par ^ 1] = 0ull;
-        ctl->retired[par ^ 1] = 0;
-    }
-    const int units = (n_short + 31) / 32;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    unsigned long long *acc = s_acc[warp];
-    int *delta = s_delta[warp];
-    uint8_t *owner = s_owner[warp];
-    const int4 *list = p.lists[par][kBlueS];
-    for (;;) {
-        int u = 0;
-        if (lane == 0) u = atomicAdd(&ctl->task_short[par], 1);
-        u = __shfl_sync(kFull, u, 0);
-        if (u >= units) break;
-        const int idx = u * 32 + lane;
-        const bool valid = idx < n_short;
-        const int4 it = valid ? list[idx] : make_int4(-1, 0, 0, 0);
-        const int deg = valid ? degree_of(it) : 0;
-        const int incl = warp_incl_scan(deg);
-        const int start = incl - deg;
-        const int total = __shfl_sync(kFull, incl, 31);
-        delta[lane] = it.y - start;  // global position of concatenated entry e: e + delta[owner]
-        acc[lane] = 0ull;
-        for (int k = 0; k < deg; ++k) owner[start + k] = (uint8_t)lane;
-        __syncwarp();
-        for (int base = 0; base < total; base += 32 * kRows) {
-            int own[kRows], pos[kRows], nb[kRows];
-            float wv[kRows];
+    const int n_blue = __ldcg(&ctl->cnt[par][kBlue]);
+    const int4 *list = p.lists[par][kBlue];
+    const long long stride = (long long)gridDim.x * kThreads;
+    for (long long i0 = (long long)blockIdx.x * kThreads + threadIdx.x; i0 < n_blue; i0 += stride * kPerW) {
+        int4 it[kPerW];
+        int wl[kPerW], cj[kPerW], ct[kPerW], seen[kPerW];
+        bool open[kPerW], alive[kPerW];
 #pragma unroll
-            for (int r = 0; r < kRows; ++r) {
-                const int e = base + r * 32 + lane;
-                const bool in = e < total;
-                own[r] = in ? owner[e] : -1;
-                pos[r] = in ? e + delta[own[r]] : 0;
-                nb[r] = in ? __ldcs(p.nbrs + pos[r]) : 0;
-                wv[r] = kW && in ? __ldcs(p.w + pos[r]) : 0.0f;
+        for (int k = 0; k < kPerW; ++k) {
+            const long long i = i0 + k * stride;
+            it[k] = i < n_blue ? __ldcg(list + i) : make_int4(-1, 0, 0, 0);
+            wl[k] = it[k].x >= 0 ? win_len(degree_of(it[k])) : 0;
+            open[k] = wl[k] > 0;
+            alive[k] = false;
+            cj[k] = -1;
+            ct[k] = 0;
+            seen[k] = 0;
+        }
+        for (int q = 0; q < kWin; q += 2) {
+            bool any = false;
+#pragma unroll
+            for (int k = 0; k < kPerW; ++k) any |= open[k];
+            if (!any) break;
+            int nb0[kPerW], nb1[kPerW], j0[kPerW], j1[kPerW];
+#pragma unroll
+            for (int k = 0; k < kPerW; ++k) {
+                nb0[k] = nb1[k] = 0;
+                j0[k] = j1[k] = 0;
+                if (!open[k]) continue;
+                if (kW) {
+                    const int4 e = __ldg(reinterpret_cast<const int4 *>(p.pwin + it[k].w + q));
+                    nb0[k] = e.x;
+                    j0[k] = e.y;
+                    nb1[k] = e.z;
+                    j1[k] = e.w;
+                } else {
+                    j0[k] = it[k].y + q;
+                    j1[k] = j0[k] + 1;
+                    nb0[k] = __ldg(p.nbrs + j0[k]);
+                    if (q + 1 < wl[k]) nb1[k] = __ldg(p.nbrs + j1[k]);
+                }
             }
-            uint8_t c[kRows];
+            uint8_t c0[kPerW], c1[kPerW];
 #pragma unroll
-            for (int r = 0; r < kRows; ++r) c[r] = own[r] >= 0 ? p.col[nb[r]] : (uint8_t)kMatched;
+            for (int k = 0; k < kPerW; ++k) {
+                c0[k] = c1[k] = kMatched;
+                if (!open[k]) continue;
+                c0[k] = p.col[nb0[k]];
+                if (q + 1 < wl[k]) c1[k] = p.col[nb1[k]];
+            }
 #pragma unroll
-            for (int r = 0; r < kRows; ++r) {
-                const unsigned long long key = entry_key<kW>(c[r], pos[r], wv[r]);
-                if (key) atomicMax(&acc[own[r]], key);
+            for (int k = 0; k < kPerW; ++k) {
+                if (!open[k]) continue;
+                // entry q, then q + 1 (flag bit 31: a weight that can never be picked)
+                if (c0[k] == kRed && j0[k] >= 0) {
+                    cj[k] = j0[k];
+                    ct[k] = nb0[k];
+                    seen[k] += 1;
+                    open[k] = false;
+                    continue;
+                }
+                alive[k] |= c0[k] != kMatched;
+                seen[k] += 1;
+                if (q + 1 < wl[k]) {
+                    if (c1[k] == kRed && j1[k] >= 0) {
+                        cj[k] = j1[k];
+                        ct[k] = nb1[k];
+                        seen[k] += 1;
+                        open[k] = false;
+                        continue;
+                    }
+                    alive[k] |= c1[k] != kMatched;
+                    seen[k] += 1;
+                }
+                if (q + 2 >= wl[k]) open[k] = false;
             }
         }
-        __syncwarp();
-        if (valid) propose_counted<kW, kStats>(p, it, acc[lane], t);
-        __syncwarp();  // the tables are refilled by the next batch
+#pragma unroll
+        for (int k = 0; k < kPerW; ++k) {
+            if (it[k].x < 0) continue;
+            const int v = it[k].x, deg = degree_of(it[k]);
+            if (kStats) atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_WINDOW_ENTRIES], (unsigned long long)seen[k]);
+            if (cj[k] >= 0 || deg <= kWin) {
+                if (kStats) {
+                    atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_REQ_ENTRIES],
+                              request_seen<kW>(it[k].y, deg, cj[k]));
+                    atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_BLUE_DEG], (unsigned long long)deg);
+                }
+                if (cj[k] >= 0) propose_to(p, v, it[k].y, cj[k] & 0x7fffffff, ct[k]);
+                else no_proposal(p, v, alive[k]);
+            } else {
+                // fallback: the whole list is scanned in phase A2
+                const unsigned long long old =
+                    atomicAdd(&ctl->staged_pack, (1ull << 32) | (unsigned long long)(unsigned)deg);
+                const int idx = (int)(old >> 32), off = (int)(old & 0xffffffffull);
+                p.staged[idx] = make_int4(v, it[k].y, it[k].z, off);
+                for (int s = (off + kSegEntries - 1) / kSegEntries; s * kSegEntries < off + deg; ++s)
+                    p.seg_first[s] = idx;
+            }
+        }
     }
 }
 
-// ---- long lists: entry-balanced segments ----
+// ---- phase A2: fallback lists, entry-balanced segments ----
 //
-// The blue long lists of a round are concatenated (each item's .w is its
-// offset) and cut into kSegEntries-entry segments; seg_first[s] is the first
-// item overlapping segment s.  A warp takes a segment: lane l describes the
-// l-th list piece in it (at most 16), then the warp walks the segment in rows
-// of 32 consecutive entries.  Each lane keeps a cursor on the piece its entry
-// falls in (it moves forward only) and a running key for it, folded into the
-// piece's shared slot when the cursor moves on.  A list inside one segment
-// proposes at once; a cut list max-combines its piece into part_key and the
-// piece that arrives last proposes.
-
-constexpr int kWarpsL = 8;
-
+// The round's fallback lists are concatenated (each item's .w is its offset)
+// and cut into kSegEntries-entry segments; seg_first[s] is the first item
+// overlapping segment s.  Items are numbered in offset order: one 64-bit
+// atomic hands out both.  A warp takes a segment: lane l describes the l-th
+// list piece in it (at most 32), then the warp walks the segment in rows of
+// 32 consecutive entries.  Every piece but the segment's first and last is a
+// whole list of more than 32 entries, so a row holds at most one piece
+// boundary and the piece being scanned is the same for the whole warp: each
+// lane keeps a running best (weight, position, alive) for it, and at the
+// boundary the warp max-reduces the lanes' keys with shuffles and the lane
+// describing the piece finishes it.  A list inside one segment proposes at
+// once; a cut list max-combines its piece into part_key and the piece that
+// arrives last proposes.
+//
+// Loads are pipelined over iterations of kRows rows: the neighbour ids and
+// weights of iteration i+2 stream into shared memory (cp.async, kStages
+// buffers) and the colour gathers of iteration i+1 are in flight while
+// iteration i is folded.
 template <bool kW, bool kStats>
 __device__ __forceinline__ void finish_piece(const Params &p, int4 it, int pieces, unsigned long long key, int t)
 {
@@ -446,42 +588,75 @@ __device__ __forceinline__ void finish_piece(const Params &p, int4 it, int piece
     asm volatile("atom.add.acq_rel.gpu.s32 %0, [%1], 1;" : "=r"(done) : "l"(p.part_cnt + v) : "memory");
     if (done == pieces - 1) {
         const unsigned long long all = atomicExch(&p.part_key[v], 0ull);
-        p.part_cnt[v] = 0;
+        atomicExch(&p.part_cnt[v], 0);
         propose_counted<kW, kStats>(p, it, all, t);
     }
 }
 
-template <bool kW, bool kStats>
-__global__ void __launch_bounds__(kWarpsL * 32) k_phase_a_long(Params p)
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async4_s(unsigned saddr, const void *gmem)
 {
-    __shared__ unsigned long long s_acc[kWarpsL][32];
-    __shared__ int s_end[kWarpsL][33];    // segment-relative end of each piece; INT_MAX past the last
-    __shared__ int s_delta[kWarpsL][32];  // global position of segment entry e: e + delta[piece]
-    Ctl *ctl = p.ctl;
-    const int t = ctl->t;
-    const int par = t & 1;
-    const unsigned long long pack = ctl->staged_pack[par];
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(saddr), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long k)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long y = __shfl_xor_sync(kFull, k, o);
+        k = y > k ? y : k;
+    }
+    return k;
+}
+
+// Finish piece k of the segment table: lane k holds its item.
+template <bool kW, bool kStats>
+__device__ __forceinline__ void finish_table_piece(const Params &p, int k, int lane, int4 it, int pieces, int lo, int hi,
+                                                   unsigned long long key, int t)
+{
+    if (lane == k) {
+        if (kStats) {
+            atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_STAGED_DEG], (unsigned long long)(hi - lo));
+            atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_STAGED_ITEMS], 1ull);
+        }
+        finish_piece<kW, kStats>(p, it, pieces, key, t);
+    }
+}
+
+template <bool kW, bool kStats>
+__device__ void scan_long(const Params &p, Smem &sm, int t, int gwarp, int nwarps)
+{
+    const unsigned long long pack = __ldcg(&p.ctl->staged_pack);
     const int nitems = (int)(pack >> 32);
     const int nentries = (int)(pack & 0xffffffffull);
     const int nseg = (nentries + kSegEntries - 1) / kSegEntries;
-    if (nseg == 0) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    unsigned long long *acc = s_acc[warp];
-    int *pend = s_end[warp];
-    int *delta = s_delta[warp];
-    const int4 *list = p.lists[par][kStaged];
-    for (;;) {
-        int s = 0;
-        if (lane == 0) s = atomicAdd(&ctl->task_long[par], 1);
-        s = __shfl_sync(kFull, s, 0);
-        if (s >= nseg) break;
+    int *pend = sm.pend[warp];
+    int *delta = sm.delta[warp];
+    LongStage &stg = sm.stage[warp];
+    // shared addresses of this lane's slots in stage 0 (stage k: + k * kStageBytes)
+    constexpr unsigned kStageBytes = kRows * 32 * 4;
+    const unsigned nb_slot = (unsigned)__cvta_generic_to_shared(&stg.nb[0][lane]);
+    const unsigned w_slot = (unsigned)__cvta_generic_to_shared(&stg.w[0][lane]);
+    const int4 *list = p.staged;
+    const int *seg_first = p.seg_first;
+    // the piece table of segment s + nwarps is loaded while segment s is
+    // scanned: seg_first two segments ahead, the items one segment ahead
+    int sf_a = gwarp < nseg ? __ldcg(seg_first + gwarp) + lane : nitems;
+    int sf_b = gwarp + nwarps < nseg ? __ldcg(seg_first + gwarp + nwarps) + lane : nitems;
+    int4 x_a = sf_a < nitems ? __ldcg(list + sf_a) : make_int4(-1, 0, 0, -1);
+    for (int s = gwarp; s < nseg; s += nwarps) {
         const int s_lo = s * kSegEntries;
         const int seg_len = min(kSegEntries, nentries - s_lo);
-        const int idx = p.seg_first[par][s] + lane;
+        const int idx = sf_a;
+        const int4 x = x_a;
+        x_a = sf_b < nitems ? __ldcg(list + sf_b) : make_int4(-1, 0, 0, -1);
+        sf_a = sf_b;
+        sf_b = s + 2 * nwarps < nseg ? __ldcg(seg_first + s + 2 * nwarps) + lane : nitems;
         int4 it = make_int4(-1, 0, 0, 0);
         int pieces = 1, lo = 0, hi = 0;
         if (idx < nitems) {
-            const int4 x = list[idx];
             const int deg = degree_of(x);
             if (x.w < s_lo + seg_len && x.w + deg > s_lo) {
                 it = x;
@@ -493,121 +668,128 @@ __global__ void __launch_bounds__(kWarpsL * 32) k_phase_a_long(Params p)
         pend[lane] = it.x >= 0 ? it.w + hi - s_lo : 0x7fffffff;
         if (lane == 0) pend[32] = 0x7fffffff;
         delta[lane] = it.y - it.w + s_lo;
-        acc[lane] = 0ull;
+        if (lane == 0) delta[32] = 0;
         __syncwarp();
-        int cur = 0;
-        unsigned long long best = 0ull;
-        int fold = 0;  // piece the running key belongs to
-        for (int base = 0; base < seg_len; base += 32 * kRows) {
-            int own[kRows], pos[kRows], nb[kRows];
-            float wv[kRows];
+        const int nit = (seg_len + 32 * kRows - 1) / (32 * kRows);
+        // Load side: piece kl holds the first entry of the row being staged;
+        // its end and the position offsets of kl and kl + 1 stay in registers.
+        int kl = 0, endl = pend[0], dl0 = delta[0], dl1 = delta[1];
+        int stage_in = 0;  // stage that iteration i + 2 is staged into
+        auto issue = [&](int i) {
+            if (i < nit) {
+                const unsigned so = (unsigned)stage_in * kStageBytes;
 #pragma unroll
-            for (int r = 0; r < kRows; ++r) {
-                const int e = base + r * 32 + lane;
-                const bool in = e < seg_len;
-                while (in && e >= pend[cur]) ++cur;
-                own[r] = in ? cur : -1;
-                pos[r] = e + delta[cur];
-                nb[r] = in ? __ldcs(p.nbrs + pos[r]) : 0;
-                wv[r] = kW && in ? __ldcs(p.w + pos[r]) : 0.0f;
-            }
-            uint8_t c[kRows];
-#pragma unroll
-            for (int r = 0; r < kRows; ++r) c[r] = own[r] >= 0 ? p.col[nb[r]] : (uint8_t)kMatched;
-#pragma unroll
-            for (int r = 0; r < kRows; ++r) {
-                if (own[r] < 0) continue;
-                if (own[r] != fold) {
-                    if (best) atomicMax(&acc[fold], best);
-                    best = 0ull;
-                    fold = own[r];
+                for (int r = 0; r < kRows; ++r) {
+                    const int rb = i * 32 * kRows + r * 32;
+                    if (rb < seg_len) {
+                        while (endl <= rb) {
+                            ++kl;
+                            endl = pend[kl];
+                            dl0 = dl1;
+                            dl1 = delta[kl + 1];
+                        }
+                        const int e = rb + lane;
+                        if (e < seg_len) {
+                            const int pos = e + (e >= endl ? dl1 : dl0);
+                            cp_async4_s(nb_slot + so + r * 128, p.nbrs + pos);
+                            if (kW) cp_async4_s(w_slot + so + r * 128, p.w + pos);
+                        }
+                    }
                 }
-                const unsigned long long key = entry_key<kW>(c[r], pos[r], wv[r]);
-                best = key > best ? key : best;
             }
-        }
-        if (best) atomicMax(&acc[fold], best);
-        __syncwarp();
-        if (it.x >= 0) {
-            if (kStats) {
-                atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_STAGED_DEG], (unsigned long long)(hi - lo));
-                atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_STAGED_ITEMS], 1ull);
+            cp_async_commit();
+            stage_in = stage_in == kStages - 1 ? 0 : stage_in + 1;
+        };
+        // colours of iteration i (staged in stage st), one byte per row
+        auto gather = [&](int i, int st) -> unsigned {
+            unsigned c = 0x03030303u;  // kMatched in every row
+            if (i < nit) {
+#pragma unroll
+                for (int r = 0; r < kRows; ++r) {
+                    const int e = i * 32 * kRows + r * 32 + lane;
+                    if (e < seg_len) {
+                        const unsigned x = p.col[stg.nb[st][r * 32 + lane]];
+                        c = (c & ~(0xffu << (8 * r))) | (x << (8 * r));
+                    }
+                }
             }
-            finish_piece<kW, kStats>(p, it, pieces, acc[lane], t);
+            return c;
+        };
+        issue(0);
+        issue(1);
+        cp_async_wait1();
+        unsigned cc = gather(0, 0);
+        // Fold side: piece kp, its end and the offsets of kp and kp + 1.
+        int kp = 0, endp = pend[0], dp0 = delta[0], dp1 = delta[1];
+        int st = 0;  // stage of iteration i
+        float bw = -1.0f;
+        int bj = 0;
+        bool alive = false;
+        for (int i = 0; i < nit; ++i) {
+            issue(i + 2);
+            cp_async_wait1();
+            const int st1 = st == kStages - 1 ? 0 : st + 1;
+            const unsigned cn = gather(i + 1, st1);
+#pragma unroll
+            for (int r = 0; r < kRows; ++r) {
+                const int rb = i * 32 * kRows + r * 32;
+                if (rb >= seg_len) break;
+                const int e = rb + lane;
+                const bool in = e < seg_len;
+                const uint8_t c = (uint8_t)(cc >> (8 * r));
+                const float wv = kW ? stg.w[st][r * 32 + lane] : 0.0f;
+                if (endp < min(rb + 32, seg_len)) {
+                    // piece kp ends inside this row: finish it, then start kp + 1
+                    const bool second = e >= endp;
+                    if (in && !second) fold_entry<kW>(c, wv, e + dp0, bw, bj, alive);
+                    const unsigned long long key = warp_max_u64(strip_key<kW>(bw, bj, alive));
+                    finish_table_piece<kW, kStats>(p, kp, lane, it, pieces, lo, hi, key, t);
+                    bw = -1.0f;
+                    alive = false;
+                    ++kp;
+                    endp = pend[kp];
+                    dp0 = dp1;
+                    dp1 = delta[kp + 1];
+                    if (in && second) fold_entry<kW>(c, wv, e + dp0, bw, bj, alive);
+                } else if (in) {
+                    fold_entry<kW>(c, wv, e + dp0, bw, bj, alive);
+                }
+            }
+            cc = cn;
+            st = st1;
         }
-        __syncwarp();  // the tables are refilled by the next segment
+        {
+            const unsigned long long key = warp_max_u64(strip_key<kW>(bw, bj, alive));
+            finish_table_piece<kW, kStats>(p, kp, lane, it, pieces, lo, hi, key, t);
+        }
+        __syncwarp();  // the tables and stages are refilled by the next segment
     }
-}
-
-// Rounds small enough for one block run in the tail kernel.
-constexpr int kTailThreads = 1024;
-constexpr long long kTailItems = 4096;        // vertices that can still be matched
-constexpr unsigned kTailEntries = 32768;      // entries of blue long lists
-
-// Close round t (one thread): record the outcome and decide what runs next.
-// Returns true if another round runs in the caller's loop.
-__device__ __forceinline__ bool close_round(Ctl *ctl, int t, int cap, bool has_next, bool seeds_short, long long next,
-                                            unsigned staged_entries, int retired, bool in_tail)
-{
-    const bool more = has_next && next > 0;
-    if (!more) {
-        if (seeds_short) ctl->status = 1;
-        // Vertices retired while being coloured for round t+1 are still active
-        // in that round for the reference, so it runs round t+1 and only finds
-        // nothing left at round t+2.
-        if (!ctl->maximal || next > 0) ctl->rounds = cap;
-        else ctl->rounds = min(retired > 0 ? t + 3 : t + 2, cap);
-    }
-    ctl->t = t + 1;
-    const bool to_tail = more && !in_tail && next <= kTailItems && staged_entries <= kTailEntries;
-    if (to_tail) ctl->tail = 1;
-    const bool loop = more && !to_tail;
-    ctl->cont = loop ? 1 : 0;
-    return loop;
 }
 
 // Phase B: commit proposals, recolour survivors with the next seed, compact
-// the worklists; the last block closes the round.
+// the worklists of round t+1.
 template <bool kW, bool kStats>
-__global__ void __launch_bounds__(kBlockT) k_phase_b(Params p)
+__device__ void commit_phase(const Params &p, Smem &sm, int t, bool has_next)
 {
     Ctl *ctl = p.ctl;
-    const int t = ctl->t;
     const int par = t & 1;
-    const int cap = ctl->cap;
-    bool has_next = t + 1 < cap;
-    const bool seeds_short = has_next && t + 1 >= ctl->nseeds;
-    if (seeds_short) has_next = false;
     const uint32_t next_seed = has_next ? p.seeds[t + 1] : 0u;
     const uint32_t barrier = ctl->barrier;
-    // lists in the order: blue short, blue long (staged), red short, red long
-    const int c0 = ctl->cnt[par][kBlueS], c1 = (int)(ctl->staged_pack[par] >> 32), c2 = ctl->cnt[par][kRedS],
-              c3 = ctl->cnt[par][kRedLong];
-    const long long total = (long long)c0 + c1 + c2 + c3;
+    const int c0 = __ldcg(&ctl->cnt[par][kBlue]), c1 = __ldcg(&ctl->cnt[par][kRed]);
+    const long long total = (long long)c0 + c1;
     const long long ntiles = (total + kTileItems - 1) / kTileItems;
     int *match = ctl->match;
+    int retired = 0;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         int4 it[kPer];
         bool in[kPer], blue[kPer];
 #pragma unroll
         for (int k = 0; k < kPer; ++k) {
-            long long i = tile * kTileItems + k * kBlockT + threadIdx.x;
+            const long long i = tile * kTileItems + k * kThreads + threadIdx.x;
             in[k] = i < total;
-            blue[k] = true;
+            blue[k] = i < c0;
             it[k] = make_int4(0, 0, 0, 0);
-            if (in[k]) {
-                if (i < c0) {
-                    it[k] = p.lists[par][kBlueS][i];
-                } else if ((i -= c0) < c1) {
-                    it[k] = p.lists[par][kStaged][i];
-                } else if ((i -= c1) < c2) {
-                    it[k] = p.lists[par][kRedS][i];
-                    blue[k] = false;
-                } else {
-                    it[k] = p.lists[par][kRedLong][i - c2];
-                    blue[k] = false;
-                }
-            }
+            if (in[k]) it[k] = blue[k] ? __ldcg(p.lists[par][kBlue] + i) : __ldcg(p.lists[par][kRed] + (i - c0));
         }
         // proposal state: blue -> its request, red -> the best proposal it received
         int2 q[kPer];
@@ -617,13 +799,13 @@ __global__ void __launch_bounds__(kBlockT) k_phase_b(Params p)
             q[k] = make_int2(-1, 0);
             key[k] = 0ull;
             if (in[k]) {
-                if (blue[k]) q[k] = p.req[it[k].x];
-                else key[k] = p.best[it[k].x];
+                if (blue[k]) q[k] = __ldcg(p.req + it[k].x);
+                else key[k] = __ldcg(p.best + it[k].x);
             }
         }
 #pragma unroll
         for (int k = 0; k < kPer; ++k)
-            if (in[k] && blue[k] && q[k].y != 0) key[k] = p.best[q[k].x];
+            if (in[k] && blue[k] && q[k].y != 0) key[k] = __ldcg(p.best + q[k].x);
         int partner[kPer];
 #pragma unroll
         for (int k = 0; k < kPer; ++k) {
@@ -632,12 +814,11 @@ __global__ void __launch_bounds__(kBlockT) k_phase_b(Params p)
             if (blue[k]) {
                 if (q[k].y != 0 && (uint32_t)key[k] == (uint32_t)q[k].y) partner[k] = q[k].x;
             } else if (key[k]) {
-                partner[k] = p.nbrs[(int)~(uint32_t)key[k]];
+                partner[k] = __ldg(p.nbrs + (int)~(uint32_t)key[k]);
             }
         }
         int dest[kPer];
         unsigned long long matched = 0, seen = 0, rdeg = 0, act = 0, nblue = 0;
-        int retired = 0;
 #pragma unroll
         for (int k = 0; k < kPer; ++k) {
             dest[k] = -1;
@@ -657,7 +838,7 @@ __global__ void __launch_bounds__(kBlockT) k_phase_b(Params p)
             if (blue[k] && q[k].x == -1) continue;  // unmatchable (marked in phase A)
             // survivor
             if (!has_next) {
-                dest[k] = next_list(blue[k], deg);
+                dest[k] = blue[k] ? kBlue : kRed;
                 continue;
             }
             const bool nb = colour_of((uint32_t)v, next_seed, barrier) == kBlue;
@@ -669,7 +850,7 @@ __global__ void __launch_bounds__(kBlockT) k_phase_b(Params p)
                 ++retired;
             } else {
                 p.col[v] = nb ? kBlue : kRed;
-                dest[k] = next_list(nb, deg);
+                dest[k] = nb ? kBlue : kRed;
             }
         }
         if (kStats) {
@@ -682,241 +863,81 @@ __global__ void __launch_bounds__(kBlockT) k_phase_b(Params p)
                 stat_add(p, t + 1, MM_ST_RED, act - nblue);
             }
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) retired += __shfl_xor_sync(kFull, retired, o);
-        if ((threadIdx.x & 31) == 0 && retired) atomicAdd(&ctl->retired[par ^ 1], retired);
-        compact_tile(p, par ^ 1, dest, it);
+        compact_tile(p, sm, par ^ 1, dest, it);
     }
-    // Round bookkeeping by the last block to arrive.
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned ticket = atomicAdd(&ctl->ticket, 1u);
-        if (ticket == gridDim.x - 1) {
-            __threadfence();
-            long long next = (long long)(atomicAdd(&ctl->staged_pack[par ^ 1], 0ull) >> 32);
 #pragma unroll
-            for (int l = 0; l < kStaged; ++l) next += atomicAdd(&ctl->cnt[par ^ 1][l], 0);
-            const int retired_all = atomicAdd(&ctl->retired[par ^ 1], 0);
-            const unsigned staged_entries =
-                (unsigned)(atomicAdd(&ctl->staged_pack[par ^ 1], 0ull) & 0xffffffffull);
-            ctl->ticket = 0u;
-            const bool cont = close_round(ctl, t, cap, has_next, seeds_short, next, staged_entries, retired_all, false);
-            // Outside a graph (the stepped profiling driver) the host reads ctl->cont instead.
-            if (p.loop) cudaGraphSetConditional(p.loop, cont ? 1u : 0u);
-        }
-    }
+    for (int o = 16; o > 0; o >>= 1) retired += __shfl_xor_sync(kFull, retired, o);
+    if ((threadIdx.x & 31) == 0 && retired) atomicAdd(&ctl->retired[par ^ 1], retired);
 }
 
-// ---- tail: the last, small rounds in one block ----
-//
-// Same round as the grid kernels (scan + propose, commit + recolour), with
-// block barriers between the phases instead of kernel launches.  Values that
-// other threads of the block changed by atomics (best, counters) are read
-// from L2 (__ldcg), never from this SM's L1.
-
-// One short list scanned by one thread, kShortStep loads and gathers at a time.
+// The whole matching in one cooperative launch: set-up, then per round the
+// window scan (A1), the fallback scan (A2, only in rounds that have fallback
+// lists) and the commit phase (B), separated by grid barriers.  Every block
+// reads the same counters after a barrier, so all blocks take the same
+// branches and leave the loop at the same round.  Afterwards, vertices that
+// could still be matched keep their last colour as their match value (the
+// reference leaves match[v] = 0 / 1 for them).
 template <bool kW, bool kStats>
-__device__ void tail_scan_thread(const Params &p, int4 it, int t)
+__global__ void __launch_bounds__(kThreads, 2) k_rounds(Params p)
 {
-    float bw = -1.0f;
-    int bj = 0;
-    bool alive = false;
-    for (int b = it.y; b < it.z; b += kShortStep) {
-        int nb[kShortStep];
-        float wv[kShortStep];
-#pragma unroll
-        for (int k = 0; k < kShortStep; ++k) {
-            const bool in = b + k < it.z;
-            nb[k] = in ? p.nbrs[b + k] : 0;
-            wv[k] = kW && in ? p.w[b + k] : 0.0f;
-        }
-        uint8_t c[kShortStep];
-#pragma unroll
-        for (int k = 0; k < kShortStep; ++k) c[k] = __ldcg(p.col + nb[k]);
-#pragma unroll
-        for (int k = 0; k < kShortStep; ++k) {
-            if (b + k >= it.z) break;
-            alive |= c[k] != kMatched;
-            if (c[k] == kRed && wv[k] > bw) {
-                bw = wv[k];
-                bj = b + k;
-            }
-        }
-        if (!kW && bw > -1.0f) break;  // grRequest returns at the first red neighbour
-    }
-    propose_counted<kW, kStats>(p, it, strip_key<kW>(bw, bj, alive), t);
-}
-
-// One long list scanned by one warp: 4 entries per lane per step, 32 apart.
-template <bool kW, bool kStats>
-__device__ void tail_scan_warp(const Params &p, int4 it, int t)
-{
-    const int lane = threadIdx.x & 31;
-    float bw = -1.0f;
-    int bj = 0;
-    bool alive = false;
-    for (int base = it.y; base < it.z; base += 128) {
-        int nb[4];
-        float wv[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int j = base + k * 32 + lane;
-            nb[k] = j < it.z ? p.nbrs[j] : 0;
-            wv[k] = kW && j < it.z ? p.w[j] : 0.0f;
-        }
-        uint8_t c[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) c[k] = __ldcg(p.col + nb[k]);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int j = base + k * 32 + lane;
-            if (j >= it.z) break;
-            alive |= c[k] != kMatched;
-            if (c[k] == kRed && wv[k] > bw) {
-                bw = wv[k];
-                bj = j;
-            }
-        }
-        if (!kW && __any_sync(kFull, bw > -1.0f)) break;
-    }
-    unsigned long long key = strip_key<kW>(bw, bj, alive);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const unsigned long long k2 = __shfl_xor_sync(kFull, key, o);
-        key = k2 > key ? k2 : key;
-    }
-    if (lane == 0) propose_counted<kW, kStats>(p, it, key, t);
-}
-
-template <bool kW, bool kStats>
-__global__ void __launch_bounds__(kTailThreads) k_tail(Params p)
-{
+    extern __shared__ __align__(16) unsigned char dsmem[];
+    Smem &sm = *reinterpret_cast<Smem *>(dsmem);
     Ctl *ctl = p.ctl;
-    if (!__ldcg(&ctl->tail)) return;
-    __shared__ int s_t, s_more;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (;;) {
-        if (tid == 0) {
-            const int t = ctl->t;
-            s_t = t;
-            const int nx = (t & 1) ^ 1;
-            for (int l = 0; l < kLists; ++l) ctl->cnt[nx][l] = 0;
-            ctl->staged_pack[nx] = 0ull;
-            ctl->retired[nx] = 0;
-        }
-        __syncthreads();
-        const int t = s_t, par = t & 1, nx = par ^ 1;
-        const int cap = ctl->cap;
-        const int c_bs = __ldcg(&ctl->cnt[par][kBlueS]);
-        const int c_st = (int)(__ldcg(&ctl->staged_pack[par]) >> 32);
-        const int c_rs = __ldcg(&ctl->cnt[par][kRedS]);
-        const int c_rl = __ldcg(&ctl->cnt[par][kRedLong]);
-        // scan + propose
-        for (int i = tid; i < c_bs; i += kTailThreads) tail_scan_thread<kW, kStats>(p, p.lists[par][kBlueS][i], t);
-        for (int i = warp; i < c_st; i += kTailThreads / 32) tail_scan_warp<kW, kStats>(p, p.lists[par][kStaged][i], t);
-        __syncthreads();
-        // commit + recolour + compact
-        bool has_next = t + 1 < cap;
-        const bool seeds_short = has_next && t + 1 >= ctl->nseeds;
-        if (seeds_short) has_next = false;
-        const uint32_t next_seed = has_next ? p.seeds[t + 1] : 0u;
-        const uint32_t barrier = ctl->barrier;
-        int *match = ctl->match;
-        const int total = c_bs + c_st + c_rs + c_rl;
-        for (int i = tid; i < total; i += kTailThreads) {
-            int4 it;
-            bool blue = true;
-            if (i < c_bs) it = p.lists[par][kBlueS][i];
-            else if (i < c_bs + c_st) it = p.lists[par][kStaged][i - c_bs];
-            else if (i < c_bs + c_st + c_rs) { it = p.lists[par][kRedS][i - c_bs - c_st]; blue = false; }
-            else { it = p.lists[par][kRedLong][i - c_bs - c_st - c_rs]; blue = false; }
-            const int v = it.x;
-            const int deg = degree_of(it);
-            int partner = -1;
-            bool dead = false;
-            if (blue) {
-                const int2 q = __ldcg(&p.req[v]);
-                dead = q.x == -1;
-                if (q.y != 0 && (uint32_t)__ldcg(&p.best[q.x]) == (uint32_t)q.y) partner = q.x;
-            } else {
-                const unsigned long long key = __ldcg(&p.best[v]);
-                if (key) partner = p.nbrs[(int)~(uint32_t)key];
-                if (kStats) {
-                    atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_RED_DEG], (unsigned long long)deg);
-                    atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_RESP_ENTRIES],
-                              kW ? (unsigned long long)deg
-                                 : (key ? (unsigned long long)((int)~(uint32_t)key - it.y + 1) : (unsigned long long)deg));
-                }
-            }
-            if (partner >= 0) {
-                match[v] = 4 + min(v, partner);
-                p.col[v] = kMatched;
-                if (kStats) atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_MATCHED], 1ull);
-                continue;
-            }
-            if (dead) continue;
-            int dest;
-            if (!has_next) {
-                dest = next_list(blue, deg);
-            } else {
-                const bool nb = colour_of((uint32_t)v, next_seed, barrier) == kBlue;
-                if (kStats) {
-                    atomicAdd(&p.stats[(size_t)(t + 1) * MM_STATS_COLS + MM_ST_ACTIVE], 1ull);
-                    atomicAdd(&p.stats[(size_t)(t + 1) * MM_STATS_COLS + (nb ? MM_ST_BLUE : MM_ST_RED)], 1ull);
-                }
-                if (nb && deg == 0) {  // no neighbours: unmatchable as soon as it is blue
-                    p.col[v] = kDead;
-                    match[v] = 2;
-                    atomicAdd(&ctl->retired[nx], 1);
-                    continue;
-                }
-                p.col[v] = nb ? kBlue : kRed;
-                dest = next_list(nb, deg);
-            }
-            if (dest == kStaged) {
-                const unsigned long long old =
-                    atomicAdd(&ctl->staged_pack[nx], (1ull << 32) | (unsigned long long)(unsigned)deg);
-                p.lists[nx][kStaged][(int)(old >> 32)] = make_int4(it.x, it.y, it.z, (int)(old & 0xffffffffull));
-            } else {
-                p.lists[nx][dest][atomicAdd(&ctl->cnt[nx][dest], 1)] = it;
-            }
-        }
-        __syncthreads();
-        if (tid == 0) {
-            long long next = (long long)(__ldcg(&ctl->staged_pack[nx]) >> 32);
-            for (int l = 0; l < kStaged; ++l) next += __ldcg(&ctl->cnt[nx][l]);
-            s_more = close_round(ctl, t, cap, has_next, seeds_short, next, 0u, __ldcg(&ctl->retired[nx]), true);
-        }
-        __syncthreads();
-        if (!s_more) break;
-    }
-    (void)lane;
-}
+    const int cap = ctl->cap;
+    const int maximal = ctl->maximal;
+    const int nseeds = ctl->nseeds;
+    const int gwarp = blockIdx.x * kWarps + (threadIdx.x >> 5);
+    const int nwarps = gridDim.x * kWarps;
 
-// After the loop: vertices still able to match keep their last colour as
-// their match value (the reference leaves match[v] = 0 / 1 for them).
-__global__ void __launch_bounds__(kBlockB) k_finish(Params p)
-{
-    const Ctl *ctl = p.ctl;
-    const int par = ctl->t & 1;
-    int cnt[kLists];
-    long long total = 0;
-#pragma unroll
-    for (int l = 0; l < kLists; ++l) {
-        cnt[l] = l == kStaged ? (int)(ctl->staged_pack[par] >> 32) : ctl->cnt[par][l];
-        total += cnt[l];
-    }
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        int which = 0;
-        long long k = i;
-        while (which < kLists - 1 && k >= cnt[which]) {
-            k -= cnt[which];
-            ++which;
+    init_phase<kW, kStats>(p, sm);
+    if (!grid_sync(p.bar, p.ctl, p.tstamp, 0)) return;
+    int t = 0;
+    for (;; ++t) {
+        const int par = t & 1;
+        // phase A1; the next round's counters were last read in round t - 1
+        if (blockIdx.x == 0 && threadIdx.x < kParityLists) {
+            ctl->cnt[par ^ 1][threadIdx.x] = 0;
+            if (threadIdx.x == 0) ctl->retired[par ^ 1] = 0;
         }
-        const int v = p.lists[par][which][k].x;
-        ctl->match[v] = p.col[v];
+        scan_window<kW, kStats>(p, t, par);
+        if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 1)) return;
+        // phase A2 (all blocks see the same fallback count)
+        if (__ldcg(&ctl->staged_pack) != 0ull) {
+            scan_long<kW, kStats>(p, sm, t, gwarp, nwarps);
+            if (!grid_sync(p.bar, p.ctl, p.tstamp, -1)) return;
+        }
+        if (p.tstamp && blockIdx.x == 0 && threadIdx.x == 0) p.tstamp[3 * t + 2] = global_ns();
+        // phase B; the fallback list is empty again for the next round
+        bool has_next = t + 1 < cap;
+        const bool seeds_short = has_next && t + 1 >= nseeds;
+        if (seeds_short) has_next = false;
+        commit_phase<kW, kStats>(p, sm, t, has_next);
+        if (blockIdx.x == 0 && threadIdx.x == 0) ctl->staged_pack = 0ull;
+        if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 3)) return;
+        // close the round (every block decides alike)
+        const long long next = (long long)__ldcg(&ctl->cnt[par ^ 1][kBlue]) + __ldcg(&ctl->cnt[par ^ 1][kRed]);
+        const bool more = has_next && next > 0;
+        if (!more) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                if (seeds_short) ctl->status = 1;
+                // Vertices retired while being coloured for round t+1 are still
+                // active in that round for the reference, so it runs round t+1
+                // and only finds nothing left at round t+2.
+                const int retired_all = __ldcg(&ctl->retired[par ^ 1]);
+                if (!maximal || next > 0) ctl->rounds = cap;
+                else ctl->rounds = min(retired_all > 0 ? t + 3 : t + 2, cap);
+            }
+            break;
+        }
+    }
+    // finish: survivors of the last round (lists of parity (t + 1) & 1)
+    const int par = (t + 1) & 1;
+    const int cb = __ldcg(&ctl->cnt[par][kBlue]), cr = __ldcg(&ctl->cnt[par][kRed]);
+    const long long total = (long long)cb + cr;
+    int *match = ctl->match;
+    for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < total; i += (long long)gridDim.x * kThreads) {
+        const int v = i < cb ? __ldcg(p.lists[par][kBlue] + i).x : __ldcg(p.lists[par][kRed] + (i - cb)).x;
+        match[v] = __ldcg(p.col + v);
     }
 }
 
@@ -926,7 +947,7 @@ __global__ void __launch_bounds__(kBlockB) k_finish(Params p)
 struct PrepInfo {
     unsigned long long sum_deg;
     unsigned long long max_deg;
-    unsigned long long short_count;   // lists of at most kSmallMax entries
+    unsigned long long short_count;   // lists of at most kWin entries
     unsigned long long long_count;    // longer lists
     unsigned long long long_entries;  // entries in longer lists
     int noncontig;
@@ -942,7 +963,7 @@ __global__ void k_scan_ranges(const int2 *ranges, int n, long long nnz, PrepInfo
         const int d = degree_of(r);
         sum += d;
         mx = d > (long long)mx ? d : mx;
-        if (d > kSmallMax) {
+        if (d > kWin) {
             nlong += 1;
             elong += d;
         } else {
@@ -1034,6 +1055,102 @@ __global__ void k_pair_groups(const unsigned long long *keys, const int *vals, l
             best_dir[dir] = k > best_dir[dir] ? k : best_dir[dir];
         }
         for (long long x = q; x < end; ++x) revkey[vals[x]] = best_dir[(keys[x] & 1ull) ^ 1ull];
+    }
+}
+
+// ---- preference windows (weighted types) ----
+//
+// pwin holds, for every vertex, its best min(deg, 32) entries in the order in
+// which the reference's gwRequest would prefer them: candidates (weight > -1)
+// by weight, then earlier position; entries whose weight can never be picked
+// after them, flagged by bit 31 of the position.  A vertex's window starts at
+// pwin_off[v], an even slot (pairs are read as one 16-byte load).
+__device__ __forceinline__ unsigned long long pref_key(float w, int j)
+{
+    return w > -1.0f ? (((unsigned long long)weight_order(w) << 32) | (uint32_t)~j) : (unsigned long long)(uint32_t)~j;
+}
+
+// One compare-exchange step of a bitonic network across the warp: the lower
+// lane of each pair keeps the larger key in a descending block.
+__device__ __forceinline__ void cas_step(unsigned long long &k, int &nb, int &j, int lane, int stride, bool desc)
+{
+    const unsigned long long ok = __shfl_xor_sync(kFull, k, stride);
+    const int onb = __shfl_xor_sync(kFull, nb, stride);
+    const int oj = __shfl_xor_sync(kFull, j, stride);
+    const bool lower = (lane & stride) == 0;
+    if (lower == desc ? ok > k : ok < k) {
+        k = ok;
+        nb = onb;
+        j = oj;
+    }
+}
+
+__device__ __forceinline__ void warp_sort_desc(unsigned long long &k, int &nb, int &j, int lane)
+{
+#pragma unroll
+    for (int size = 2; size <= 32; size <<= 1)
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) cas_step(k, nb, j, lane, stride, (lane & size) == 0);
+}
+
+__global__ void k_win_sizes(const int2 *ranges, int n, long long *slots)
+{
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        slots[v] = (win_len(degree_of(ranges[v])) + 1) & ~1;
+}
+
+constexpr int kWinRows = 8;  // rows of 32 entries tested against the window threshold per step
+
+// A warp per vertex keeps the best 32 entries seen so far sorted across its
+// lanes; a row can change them only if one of its keys beats the 32nd.
+__global__ void __launch_bounds__(256) k_win_build(const int2 *ranges, const int *nbrs, const float *w, int n,
+                                                   const long long *pwin_off, int2 *pwin)
+{
+    const int lane = threadIdx.x & 31;
+    const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long v = gwarp; v < n; v += nwarps) {
+        const int2 r = ranges[v];
+        const int deg = degree_of(r);
+        if (deg == 0) continue;
+        unsigned long long k = 0ull;
+        int nb = 0, j = 0;
+        if (lane < deg) {
+            j = r.x + lane;
+            nb = __ldg(nbrs + j);
+            k = pref_key(__ldg(w + j), j);
+        }
+        warp_sort_desc(k, nb, j, lane);
+        for (int base = r.x + 32; base < r.y; base += 32 * kWinRows) {
+            float wr[kWinRows];
+#pragma unroll
+            for (int q = 0; q < kWinRows; ++q) {
+                const int jj = base + q * 32 + lane;
+                wr[q] = jj < r.y ? __ldg(w + jj) : 0.0f;
+            }
+#pragma unroll
+            for (int q = 0; q < kWinRows; ++q) {
+                const int jj = base + q * 32 + lane;
+                if (base + q * 32 >= r.y) break;
+                const unsigned long long thr = __shfl_sync(kFull, k, 31);
+                unsigned long long k2 = jj < r.y ? pref_key(wr[q], jj) : 0ull;
+                if (!__any_sync(kFull, k2 > thr)) continue;
+                int nb2 = jj < r.y ? __ldg(nbrs + jj) : 0, j2 = jj;
+                warp_sort_desc(k2, nb2, j2, lane);
+                // merge: the larger of T[l] and R[31 - l] is a bitonic sequence
+                // holding the best 32 of both; sort it descending
+                const unsigned long long rk = __shfl_sync(kFull, k2, 31 - lane);
+                const int rnb = __shfl_sync(kFull, nb2, 31 - lane), rj = __shfl_sync(kFull, j2, 31 - lane);
+                if (rk > k) {
+                    k = rk;
+                    nb = rnb;
+                    j = rj;
+                }
+#pragma unroll
+                for (int stride = 16; stride > 0; stride >>= 1) cas_step(k, nb, j, lane, stride, true);
+            }
+        }
+        if (lane < win_len(deg)) pwin[pwin_off[v] + lane] = make_int2(nb, k >= (1ull << 32) ? j : (int)((unsigned)j | 0x80000000u));
     }
 }
 
@@ -1158,36 +1275,6 @@ __global__ void __launch_bounds__(kRevThreads) k_revkey_sorted(const int2 *range
     if (threadIdx.x == 0 && bad) atomicOr(unsorted, 1);
 }
 
-// Control block rounded to 256 bytes so the seeds that follow it stay aligned.
-constexpr size_t kCtlBytes = (sizeof(Ctl) + 255) / 256 * 256;
-
-// Captured round loop of one (graph, type, stats) combination.
-struct Plan {
-    int type = 0;
-    bool stats = false;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-};
-
-struct PushState {
-    uint8_t *col = nullptr;
-    int2 *req = nullptr;
-    unsigned long long *best = nullptr;
-    unsigned long long *part_key = nullptr;
-    int *part_cnt = nullptr;
-    int4 *list_mem = nullptr;
-    int4 *lists[2][kLists] = {};
-    int *seg_mem = nullptr;
-    int *seg_first[2] = {};
-    uint32_t *seeds = nullptr;        // device: right after ctl in one allocation
-    Ctl *ctl = nullptr;
-    unsigned char *host_stage = nullptr;  // pinned: control block + seeds, uploaded in one copy
-    unsigned char *host_back = nullptr;   // pinned: control block read back
-    unsigned long long *stats = nullptr;
-    Plan plans[8];
-    int nplans = 0;
-    int blocks_a = 0, blocks_b = 0, blocks_long = 0;
-};
 
 int bits_for(long long n)
 {
@@ -1196,12 +1283,32 @@ int bits_for(long long n)
     return b;
 }
 
+// Control block rounded to 256 bytes so the seeds that follow it stay aligned.
+constexpr size_t kCtlBytes = (sizeof(Ctl) + 255) / 256 * 256;
+constexpr int kStampCount = 3 * kMaxRounds + 1;
+
+struct PushState {
+    uint8_t *col = nullptr;
+    int2 *req = nullptr;
+    unsigned long long *best = nullptr;
+    unsigned long long *part_key = nullptr;
+    int *part_cnt = nullptr;
+    int4 *list_mem = nullptr;
+    int4 *lists[2][kParityLists] = {};
+    int4 *staged = nullptr;
+    int *seg_first = nullptr;
+    uint32_t *seeds = nullptr;        // device: right after ctl in one allocation
+    Ctl *ctl = nullptr;
+    unsigned char *host_stage = nullptr;  // pinned: control block + seeds, uploaded in one copy
+    unsigned char *host_back = nullptr;   // pinned: control block read back
+    unsigned long long *stats = nullptr;
+    unsigned long long *tstamp = nullptr;
+    unsigned *bar = nullptr;
+    int grid[2][2] = {{0, 0}, {0, 0}};    // co-resident blocks of k_rounds<weighted, stats>
+};
+
 void free_state(PushState *s)
 {
-    for (int i = 0; i < s->nplans; ++i) {
-        if (s->plans[i].exec) cudaGraphExecDestroy(s->plans[i].exec);
-        if (s->plans[i].graph) cudaGraphDestroy(s->plans[i].graph);
-    }
     // callers have synchronised the device (graph destroy or a failed set-up)
     dev_free(s->col, 0);
     dev_free(s->req, 0);
@@ -1209,12 +1316,27 @@ void free_state(PushState *s)
     dev_free(s->part_key, 0);
     dev_free(s->part_cnt, 0);
     dev_free(s->list_mem, 0);
-    dev_free(s->seg_mem, 0);
+    dev_free(s->staged, 0);
+    dev_free(s->seg_first, 0);
     dev_free(s->ctl, 0);
     pinned_put(s->host_stage, kCtlBytes + 256 * sizeof(uint32_t));
     pinned_put(s->host_back, kCtlBytes);
     dev_free(s->stats, 0);
+    dev_free(s->tstamp, 0);
+    dev_free(s->bar, 0);
     delete s;
+}
+
+template <bool kW, bool kStats>
+int coresident_blocks(int sms)
+{
+    int occ = 0;
+    if (cudaFuncSetAttribute(k_rounds<kW, kStats>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem)) !=
+        cudaSuccess)
+        return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rounds<kW, kStats>, kThreads, sizeof(Smem)) != cudaSuccess)
+        return 0;
+    return occ * sms;
 }
 
 mm_status alloc_state(mm_graph *g, PushState **out)
@@ -1225,12 +1347,10 @@ mm_status alloc_state(mm_graph *g, PushState **out)
         return MM_ERR_NOMEM;
     }
     const size_t n = (size_t)(g->n > 0 ? g->n : 1);
-    // list capacities: every vertex is in at most one list per parity
-    const size_t cap[kLists] = {(size_t)g->short_count, (size_t)g->short_count, (size_t)g->long_count,
-                                (size_t)g->long_count};
-    size_t per_parity = 0;
-    for (int l = 0; l < kLists; ++l) per_parity += cap[l];
+    // list capacities: every vertex is in at most one list per parity; only
+    // lists longer than the window can fall back
     const size_t nseg_cap = (size_t)(g->long_entries / kSegEntries) + 2;
+    const size_t nstaged = (size_t)(g->long_count > 0 ? g->long_count : 1);
     // pooled on the legacy stream, then synchronised so that any stream may use them
     cudaError_t e = cudaSuccess;
     if (e == cudaSuccess) e = dev_alloc((void **)&s->col, n, 0);
@@ -1238,14 +1358,17 @@ mm_status alloc_state(mm_graph *g, PushState **out)
     if (e == cudaSuccess) e = dev_alloc((void **)&s->best, n * sizeof(unsigned long long), 0);
     if (e == cudaSuccess) e = dev_alloc((void **)&s->part_key, n * sizeof(unsigned long long), 0);
     if (e == cudaSuccess) e = dev_alloc((void **)&s->part_cnt, n * sizeof(int), 0);
-    if (e == cudaSuccess) e = dev_alloc((void **)&s->list_mem, (2 * per_parity + 1) * sizeof(int4), 0);
-    if (e == cudaSuccess) e = dev_alloc((void **)&s->seg_mem, 2 * nseg_cap * sizeof(int), 0);
+    if (e == cudaSuccess) e = dev_alloc((void **)&s->list_mem, 4 * n * sizeof(int4), 0);
+    if (e == cudaSuccess) e = dev_alloc((void **)&s->staged, nstaged * sizeof(int4), 0);
+    if (e == cudaSuccess) e = dev_alloc((void **)&s->seg_first, nseg_cap * sizeof(int), 0);
     if (e == cudaSuccess) e = dev_alloc((void **)&s->ctl, kCtlBytes + 256 * sizeof(uint32_t), 0);
     if (e == cudaSuccess) s->seeds = reinterpret_cast<uint32_t *>(reinterpret_cast<unsigned char *>(s->ctl) + kCtlBytes);
     if (e == cudaSuccess) e = pinned_get((void **)&s->host_stage, kCtlBytes + 256 * sizeof(uint32_t));
     if (e == cudaSuccess) e = pinned_get((void **)&s->host_back, kCtlBytes);
     if (e == cudaSuccess)
         e = dev_alloc((void **)&s->stats, sizeof(unsigned long long) * kMaxRounds * MM_STATS_COLS, 0);
+    if (e == cudaSuccess) e = dev_alloc((void **)&s->tstamp, sizeof(unsigned long long) * kStampCount, 0);
+    if (e == cudaSuccess) e = dev_alloc((void **)&s->bar, sizeof(unsigned) * kBarWords, 0);
     if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) {
         cudaDeviceSynchronize();
@@ -1254,34 +1377,37 @@ mm_status alloc_state(mm_graph *g, PushState **out)
         set_error(std::string("push: device allocation failed: ") + cudaGetErrorString(e));
         return MM_ERR_NOMEM;
     }
-    size_t off = 0;
-    for (int par = 0; par < 2; ++par) {
-        for (int l = 0; l < kLists; ++l) {
-            s->lists[par][l] = s->list_mem + off;
-            off += cap[l];
-        }
-        s->seg_first[par] = s->seg_mem + par * nseg_cap;
-    }
-    int sms = 148, dev = 0;
+    for (int par = 0; par < 2; ++par)
+        for (int l = 0; l < kParityLists; ++l) s->lists[par][l] = s->list_mem + (2 * par + l) * n;
+    int sms = 0, dev = 0, coop = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int occ_a = 0, occ_l = 0, occ_b = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_phase_a_short<true, false>, kBlockA, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_l, k_phase_a_long<true, false>, kWarpsL * 32, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_phase_b<true, false>, kBlockT, 0);
-    s->blocks_a = sms * (occ_a > 0 ? occ_a : 4);
-    s->blocks_long = sms * (occ_l > 0 ? occ_l : 4);
-    s->blocks_b = sms * (occ_b > 0 ? occ_b : 4);
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    s->grid[0][0] = coresident_blocks<false, false>(sms);
+    s->grid[0][1] = coresident_blocks<false, true>(sms);
+    s->grid[1][0] = coresident_blocks<true, false>(sms);
+    s->grid[1][1] = coresident_blocks<true, true>(sms);
     cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) {
         free_state(s);
         return cuda_fail(le, "push: kernel attributes");
     }
+    const int most = kBarMaxGroups * kBarGroup;
+    if (s->grid[0][0] > most || s->grid[0][1] > most || s->grid[1][0] > most || s->grid[1][1] > most) {
+        free_state(s);
+        set_error("push: more co-resident blocks than the grid barrier supports");
+        return MM_ERR_UNSUPPORTED;
+    }
+    if (!coop || s->grid[0][0] < 1 || s->grid[0][1] < 1 || s->grid[1][0] < 1 || s->grid[1][1] < 1) {
+        free_state(s);
+        set_error("push: the device cannot run the cooperative round kernel");
+        return MM_ERR_UNSUPPORTED;
+    }
     *out = s;
     return MM_OK;
 }
 
-Params make_params(mm_graph *g, PushState *s, bool weighted, bool stats, cudaGraphConditionalHandle h)
+Params make_params(mm_graph *g, PushState *s, bool weighted, bool stats, bool timing)
 {
     Params p;
     p.n = g->n;
@@ -1291,103 +1417,33 @@ Params make_params(mm_graph *g, PushState *s, bool weighted, bool stats, cudaGra
     p.w = g->d_w;
     p.revkey = g->d_revkey[weighted ? 1 : 0];
     p.slot_off = g->d_slot_off;
+    p.pwin = g->d_pwin;
+    p.pwin_off = g->d_pwin_off;
     p.col = s->col;
     p.req = s->req;
     p.best = s->best;
     p.part_key = s->part_key;
     p.part_cnt = s->part_cnt;
-    for (int par = 0; par < 2; ++par) {
-        for (int l = 0; l < kLists; ++l) p.lists[par][l] = s->lists[par][l];
-        p.seg_first[par] = s->seg_first[par];
-    }
+    for (int par = 0; par < 2; ++par)
+        for (int l = 0; l < kParityLists; ++l) p.lists[par][l] = s->lists[par][l];
+    p.staged = s->staged;
+    p.seg_first = s->seg_first;
     p.seeds = s->seeds;
     p.ctl = s->ctl;
     p.stats = stats ? s->stats : nullptr;
-    p.loop = h;
+    p.tstamp = timing ? s->tstamp : nullptr;
+    p.bar = s->bar;
     return p;
 }
 
 template <bool kW, bool kStats>
-mm_status build_plan(mm_graph *g, PushState *s, Plan *plan)
+mm_status launch_rounds(mm_graph *g, PushState *s, bool timing, cudaStream_t stream)
 {
-    cudaGraph_t graph = nullptr;
-    MM_CUDA_TRY(cudaGraphCreate(&graph, 0), "graph create");
-    cudaGraphConditionalHandle h;
-    cudaError_t e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault);
-    if (e != cudaSuccess) {
-        cudaGraphDestroy(graph);
-        return cuda_fail(e, "conditional handle");
-    }
-    Params prm = make_params(g, s, kW, kStats, h);
+    Params prm = make_params(g, s, kW, kStats, timing);
     void *args[] = {&prm};
-    const int blocks_init = grid_for(g->n, kTileItems, s->blocks_b);
-
-    cudaKernelNodeParams kp = {};
-    kp.func = (void *)k_init<kStats>;
-    kp.gridDim = dim3(blocks_init);
-    kp.blockDim = dim3(kBlockT);
-    kp.kernelParams = args;
-    cudaGraphNode_t n_init, n_loop, n_fin, n_a, n_l, n_b;
-    e = cudaGraphAddKernelNode(&n_init, graph, nullptr, 0, &kp);
-
-    cudaGraphNodeParams cp = {};
-    cp.type = cudaGraphNodeTypeConditional;
-    cp.conditional.handle = h;
-    cp.conditional.type = cudaGraphCondTypeWhile;
-    cp.conditional.size = 1;
-    if (e == cudaSuccess) e = cudaGraphAddNode(&n_loop, graph, &n_init, 1, &cp);
-    if (e == cudaSuccess) {
-        // loop body: the two phase-A scans run side by side, then phase B
-        cudaGraph_t body = cp.conditional.phGraph_out[0];
-        cudaKernelNodeParams ka = {};
-        ka.func = (void *)k_phase_a_short<kW, kStats>;
-        ka.gridDim = dim3(s->blocks_a);
-        ka.blockDim = dim3(kBlockA);
-        ka.kernelParams = args;
-        e = cudaGraphAddKernelNode(&n_a, body, nullptr, 0, &ka);
-        if (e == cudaSuccess) {
-            cudaKernelNodeParams kl = {};
-            kl.func = (void *)k_phase_a_long<kW, kStats>;
-            kl.gridDim = dim3(s->blocks_long);
-            kl.blockDim = dim3(kWarpsL * 32);
-            kl.kernelParams = args;
-            e = cudaGraphAddKernelNode(&n_l, body, nullptr, 0, &kl);
-        }
-        if (e == cudaSuccess) {
-            cudaKernelNodeParams kb = {};
-            kb.func = (void *)k_phase_b<kW, kStats>;
-            kb.gridDim = dim3(s->blocks_b);
-            kb.blockDim = dim3(kBlockT);
-            kb.kernelParams = args;
-            const cudaGraphNode_t deps[2] = {n_a, n_l};
-            e = cudaGraphAddKernelNode(&n_b, body, deps, 2, &kb);
-        }
-    }
-    cudaGraphNode_t n_tail;
-    if (e == cudaSuccess) {
-        cudaKernelNodeParams kt = {};
-        kt.func = (void *)k_tail<kW, kStats>;
-        kt.gridDim = dim3(1);
-        kt.blockDim = dim3(kTailThreads);
-        kt.kernelParams = args;
-        e = cudaGraphAddKernelNode(&n_tail, graph, &n_loop, 1, &kt);
-    }
-    if (e == cudaSuccess) {
-        cudaKernelNodeParams kf = {};
-        kf.func = (void *)k_finish;
-        kf.gridDim = dim3(grid_for(g->n, kBlockB, s->blocks_b));
-        kf.blockDim = dim3(kBlockB);
-        kf.kernelParams = args;
-        e = cudaGraphAddKernelNode(&n_fin, graph, &n_tail, 1, &kf);
-    }
-    cudaGraphExec_t exec = nullptr;
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
-    if (e != cudaSuccess) {
-        cudaGraphDestroy(graph);
-        return cuda_fail(e, "round-loop graph");
-    }
-    plan->graph = graph;
-    plan->exec = exec;
+    MM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)k_rounds<kW, kStats>, dim3(s->grid[kW][kStats]), dim3(kThreads),
+                                            args, sizeof(Smem), stream),
+                "round kernel launch");
     return MM_OK;
 }
 
@@ -1421,7 +1477,7 @@ mm_status begin_call(mm_graph *g, int type, uint32_t barrier, const uint32_t *se
 }
 
 mm_status end_call(mm_graph *g, PushState *s, int nseeds, int *rounds_out, long long *stats, int stats_rounds,
-                   cudaStream_t stream)
+                   unsigned long long *stamps, cudaStream_t stream)
 {
     MM_CUDA_TRY(cudaMemcpyAsync(s->host_back, s->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, stream), "control read");
     if (stats && stats_rounds > 0)
@@ -1430,11 +1486,15 @@ mm_status end_call(mm_graph *g, PushState *s, int nseeds, int *rounds_out, long 
                                         (size_t)(stats_rounds < kMaxRounds ? stats_rounds : kMaxRounds),
                                     cudaMemcpyDeviceToHost, stream),
                     "stats read");
+    if (stamps)
+        MM_CUDA_TRY(cudaMemcpyAsync(stamps, s->tstamp, sizeof(unsigned long long) * kStampCount,
+                                    cudaMemcpyDeviceToHost, stream),
+                    "timestamps read");
     MM_CUDA_TRY(cudaStreamSynchronize(stream), "round loop");
     Ctl out;
     std::memcpy(&out, s->host_back, sizeof out);
     if (out.status == 2) {
-        set_error("mm_match: a bounded device wait gave up (staged copy did not complete)");
+        set_error("mm_match: a bounded grid-barrier wait in the round kernel gave up");
         return MM_ERR_DEVICE;
     }
     if (out.status == 1 || out.rounds > nseeds) {
@@ -1445,70 +1505,24 @@ mm_status end_call(mm_graph *g, PushState *s, int nseeds, int *rounds_out, long 
     return MM_OK;
 }
 
-template <bool kW>
-mm_status stepped_rounds(mm_graph *g, PushState *s, int *rounds_done, float *ms_kernels, int cap_rounds,
-                         cudaStream_t stream)
+mm_status run_rounds(mm_graph *g, PushState *s, int type, bool stats, bool timing, cudaStream_t stream)
 {
-    Params p = make_params(g, s, kW, false, 0);
-    const int blocks_init = grid_for(g->n, kTileItems, s->blocks_b);
-    cudaEvent_t ev[4];
-    for (int i = 0; i < 4; ++i) MM_CUDA_TRY(cudaEventCreate(&ev[i]), "event create");
-    mm_status st = MM_OK;
-    k_init<false><<<blocks_init, kBlockT, 0, stream>>>(p);
-    int r = 0;
-    for (;; ++r) {
-        cudaEventRecord(ev[0], stream);
-        k_phase_a_short<kW, false><<<s->blocks_a, kBlockA, 0, stream>>>(p);
-        cudaEventRecord(ev[1], stream);
-        k_phase_a_long<kW, false><<<s->blocks_long, kWarpsL * 32, 0, stream>>>(p);
-        cudaEventRecord(ev[2], stream);
-        k_phase_b<kW, false><<<s->blocks_b, kBlockT, 0, stream>>>(p);
-        cudaEventRecord(ev[3], stream);
-        int cont = 0;
-        cudaError_t e = cudaGetLastError();
-        if (e == cudaSuccess) e = cudaMemcpyAsync(&cont, &s->ctl->cont, sizeof(int), cudaMemcpyDeviceToHost, stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-        if (e != cudaSuccess) {
-            st = cuda_fail(e, "stepped round");
-            break;
-        }
-        if (r < cap_rounds && ms_kernels) {
-            for (int k = 0; k < 3; ++k) {
-                float ms = 0.f;
-                cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
-                ms_kernels[(size_t)r * MM_PROFILE_KERNELS + k] = ms;
-            }
-            ms_kernels[(size_t)r * MM_PROFILE_KERNELS + 3] = 0.f;
-        }
-        if (!cont) {
-            ++r;
-            break;
-        }
-    }
-    if (st == MM_OK) {
-        cudaEventRecord(ev[0], stream);
-        k_tail<kW, false><<<1, kTailThreads, 0, stream>>>(p);
-        cudaEventRecord(ev[1], stream);
-        k_finish<<<grid_for(g->n, kBlockB, s->blocks_b), kBlockB, 0, stream>>>(p);
-        cudaError_t e = cudaGetLastError();
-        if (e == cudaSuccess) e = cudaEventSynchronize(ev[1]);
-        if (e != cudaSuccess) {
-            st = cuda_fail(e, "tail / finish");
-        } else if (r < cap_rounds && ms_kernels) {
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, ev[0], ev[1]);
-            for (int k = 0; k < MM_PROFILE_KERNELS; ++k) ms_kernels[(size_t)r * MM_PROFILE_KERNELS + k] = 0.f;
-            ms_kernels[(size_t)r * MM_PROFILE_KERNELS + 3] = ms;
-        }
-    }
-    for (int i = 0; i < 4; ++i) cudaEventDestroy(ev[i]);
-    *rounds_done = r;
-    return st;
+    const bool w = is_weighted(type);
+    MM_CUDA_TRY(cudaMemsetAsync(s->bar, 0, sizeof(unsigned) * kBarWords, stream), "barrier clear");
+    if (stats)
+        MM_CUDA_TRY(cudaMemsetAsync(s->stats, 0, sizeof(unsigned long long) * kMaxRounds * MM_STATS_COLS, stream),
+                    "stats clear");
+    if (w) return stats ? launch_rounds<true, true>(g, s, timing, stream) : launch_rounds<true, false>(g, s, timing, stream);
+    return stats ? launch_rounds<false, true>(g, s, timing, stream) : launch_rounds<false, false>(g, s, timing, stream);
 }
 
 }  // namespace
 
-mm_status push_prepare(mm_graph *g, int weighted, cudaStream_t stream)
+
+namespace {
+
+// Reverse proposal keys of one weighting (built once per graph).
+mm_status build_revkey(mm_graph *g, int weighted, cudaStream_t stream)
 {
     const int wi = weighted ? 1 : 0;
     if (g->d_revkey[wi]) return MM_OK;
@@ -1653,10 +1667,68 @@ mm_status push_prepare(mm_graph *g, int weighted, cudaStream_t stream)
     return MM_OK;
 }
 
+// Preference windows of the weighted types (built once per graph).
+mm_status build_windows(mm_graph *g, cudaStream_t stream)
+{
+    const int n = g->n;
+    long long *slots = nullptr, *off = nullptr;
+    void *tmp = nullptr;
+    size_t tmp_bytes = 0;
+    MM_CUDA_TRY(dev_alloc((void **)&slots, sizeof(long long) * ((size_t)n + 1), stream), "window sizes");
+    cudaError_t e = dev_alloc((void **)&off, sizeof(long long) * ((size_t)n + 1), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(slots + n, 0, sizeof(long long), stream);
+    if (e == cudaSuccess) {
+        k_win_sizes<<<grid_for(n, 256, 148 * 8), 256, 0, stream>>>(g->d_ranges, n, slots);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, slots, off, n + 1, stream);
+    if (e == cudaSuccess) e = dev_alloc(&tmp, tmp_bytes, stream);
+    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, slots, off, n + 1, stream);
+    long long total = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&total, off + n, sizeof total, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    dev_free(tmp, stream);
+    dev_free(slots, stream);
+    if (e != cudaSuccess) {
+        dev_free(off, stream);
+        return cuda_fail(e, "window offsets");
+    }
+    if (total >= (1ll << 31)) {
+        dev_free(off, stream);
+        set_error("push: more than 2^31 - 1 preference-window slots are not supported");
+        return MM_ERR_UNSUPPORTED;
+    }
+    int2 *win = nullptr;
+    e = dev_alloc((void **)&win, sizeof(int2) * (size_t)(total > 0 ? total : 1), stream);
+    if (e == cudaSuccess) {
+        k_win_build<<<grid_for((long long)n * 32, 256, 148 * 16), 256, 0, stream>>>(g->d_ranges, g->d_nbrs, g->d_w, n,
+                                                                                  off, win);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+        dev_free(win, stream);
+        dev_free(off, stream);
+        return cuda_fail(e, "preference windows");
+    }
+    g->d_pwin = win;
+    g->d_pwin_off = off;
+    return MM_OK;
+}
+
+}  // namespace
+
+mm_status push_prepare(mm_graph *g, int weighted, cudaStream_t stream)
+{
+    mm_status st = build_revkey(g, weighted, stream);
+    if (st == MM_OK && weighted && g->n > 0 && !g->d_pwin) st = build_windows(g, stream);
+    return st;
+}
+
 mm_status push_match(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds, int *d_match,
                      int *rounds_out, long long *stats, int stats_rounds, cudaStream_t stream)
 {
-    const bool weighted = is_weighted(type), maximal = is_maximal(type);
+    const bool maximal = is_maximal(type);
     if (g->n == 0) {
         // The reference still runs (and draws a seed for) its first round.
         *rounds_out = maximal ? 1 : max_rounds_of(type);
@@ -1669,47 +1741,44 @@ mm_status push_match(mm_graph *g, int type, uint32_t barrier, const uint32_t *se
     PushState *s = nullptr;
     mm_status st = begin_call(g, type, barrier, seeds, nseeds, d_match, stream, &s);
     if (st != MM_OK) return st;
-    const bool want_stats = stats != nullptr;
-    Plan *plan = nullptr;
-    for (int i = 0; i < s->nplans; ++i)
-        if (s->plans[i].type == type && s->plans[i].stats == want_stats) plan = &s->plans[i];
-    if (!plan) {
-        if (s->nplans == 8) {
-            set_error("push: plan cache full");
-            return MM_ERR_UNSUPPORTED;
-        }
-        plan = &s->plans[s->nplans];
-        if (weighted) st = want_stats ? build_plan<true, true>(g, s, plan) : build_plan<true, false>(g, s, plan);
-        else st = want_stats ? build_plan<false, true>(g, s, plan) : build_plan<false, false>(g, s, plan);
-        if (st != MM_OK) return st;
-        plan->type = type;
-        plan->stats = want_stats;
-        ++s->nplans;
-    }
-    if (want_stats)
-        MM_CUDA_TRY(cudaMemsetAsync(s->stats, 0, sizeof(unsigned long long) * kMaxRounds * MM_STATS_COLS, stream),
-                    "stats clear");
-    MM_CUDA_TRY(cudaGraphLaunch(plan->exec, stream), "round loop launch");
-    return end_call(g, s, nseeds, rounds_out, stats, stats_rounds, stream);
+    st = run_rounds(g, s, type, stats != nullptr, false, stream);
+    if (st != MM_OK) return st;
+    return end_call(g, s, nseeds, rounds_out, stats, stats_rounds, nullptr, stream);
 }
 
-// Same kernels as push_match, launched one by one from the host with CUDA
-// events around each phase, so the duration of every phase-A and phase-B
-// launch can be read.  For measurement only (it synchronises every round).
+// Same launch as push_match with barrier timestamps on: block 0 reads the
+// global timer as each grid barrier completes, giving every round's window
+// scan (A1), fallback scan (A2) and commit (B) durations.
 mm_status push_profile(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds, int *d_match,
-                       int *rounds_out, float *ms_kernels, int cap_rounds, int *launched, cudaStream_t stream)
+                       int *rounds_out, float *ms_phases, int cap_rounds, int *launched, cudaStream_t stream)
 {
     if (g->n == 0) return push_match(g, type, barrier, seeds, nseeds, d_match, rounds_out, nullptr, 0, stream);
     PushState *s = nullptr;
     mm_status st = begin_call(g, type, barrier, seeds, nseeds, d_match, stream, &s);
     if (st != MM_OK) return st;
-    int executed = 0;
-    st = is_weighted(type) ? stepped_rounds<true>(g, s, &executed, ms_kernels, cap_rounds, stream)
-                           : stepped_rounds<false>(g, s, &executed, ms_kernels, cap_rounds, stream);
+    MM_CUDA_TRY(cudaMemsetAsync(s->tstamp, 0, sizeof(unsigned long long) * kStampCount, stream), "timestamps clear");
+    st = run_rounds(g, s, type, false, true, stream);
     if (st != MM_OK) return st;
-    st = end_call(g, s, nseeds, rounds_out, nullptr, 0, stream);
-    if (st == MM_OK && launched) *launched = 3 + 3 * executed;  // init, rounds, tail, finish
-    return st;
+    unsigned long long stamps[kStampCount];
+    st = end_call(g, s, nseeds, rounds_out, nullptr, 0, stamps, stream);
+    if (st != MM_OK) return st;
+    if (ms_phases) {
+        const int r_exec = *rounds_out;
+        for (int r = 0; r < cap_rounds; ++r) {
+            float a = 0.f, b = 0.f, c = 0.f;
+            if (r < r_exec && stamps[3 * r] && stamps[3 * r + 1] && stamps[3 * r + 2] && stamps[3 * r + 3]) {
+                a = (float)((double)(stamps[3 * r + 1] - stamps[3 * r]) * 1e-6);
+                b = (float)((double)(stamps[3 * r + 2] - stamps[3 * r + 1]) * 1e-6);
+                c = (float)((double)(stamps[3 * r + 3] - stamps[3 * r + 2]) * 1e-6);
+            }
+            ms_phases[(size_t)r * MM_PROFILE_KERNELS + 0] = a;
+            ms_phases[(size_t)r * MM_PROFILE_KERNELS + 1] = b;
+            ms_phases[(size_t)r * MM_PROFILE_KERNELS + 2] = c;
+            ms_phases[(size_t)r * MM_PROFILE_KERNELS + 3] = a + b + c;
+        }
+    }
+    if (launched) *launched = 1;
+    return MM_OK;
 }
 
 void push_release(mm_graph *g)
@@ -1725,6 +1794,10 @@ void push_release(mm_graph *g)
     }
     dev_free(g->d_slot_off, 0);
     g->d_slot_off = nullptr;
+    dev_free(g->d_pwin, 0);
+    g->d_pwin = nullptr;
+    dev_free(g->d_pwin_off, 0);
+    g->d_pwin_off = nullptr;
 }
 
 }  // namespace mm
