@@ -144,27 +144,161 @@ mm_status ensure_scratch(mm_graph *g, size_t bytes)
 
 namespace {
 
-// Check every range and every neighbour id a kernel will read: a non-empty
+// ---- validation ----
+//
+// Every range and neighbour id a kernel will read is checked: a non-empty
 // range must lie in [0, nnz) and its ids in [0, n).  Empty or reversed ranges
-// are never read (the reference's loops run zero times), so they pass.
-__global__ void k_validate(const int2 *ranges, const int *nbrs, int n, long long nnz, int *bad)
+// are never read (the reference's loops run zero times), so they pass.  The
+// same passes establish the graph properties the push path can use:
+//   contiguous   ranges tile [0, nnz) in vertex order;
+//   sorted       every list is strictly increasing (no duplicate entries);
+//   symmetric    the multiset of entries (v, u) equals that of (u, v), and
+//                with weights, of (v, u, w) and (u, v, w).
+// Symmetry is tested with two pairs of 64-bit sums of a hash of the ordered
+// entry (splitmix64's finalizer): a transposed multiset has equal sums, a
+// different one has equal sums only by a 64-bit coincidence.
+struct GraphCheck {
+    unsigned long long fwd_s, rev_s;  // structure: sum F(v, u), sum F(u, v)
+    unsigned long long fwd_w, rev_w;  // with weight bits
+    int bad;        // 1: a range outside [0, nnz); 2: an id outside [0, n)
+    int noncontig;  // ranges do not tile [0, nnz) in vertex order
+    int unsorted;   // some list is not strictly increasing
+    int pad;
+};
+
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z)
+{
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__device__ __forceinline__ unsigned long long hash_s(unsigned a, unsigned b)
+{
+    return mix64((((unsigned long long)a << 32) | b) + 0x9E3779B97F4A7C15ull);
+}
+__device__ __forceinline__ unsigned long long hash_w(unsigned a, unsigned b, unsigned wbits)
+{
+    return mix64((((unsigned long long)a << 32) | b) ^ mix64((unsigned long long)wbits + 0xD1B54A32D192ED03ull));
+}
+
+__global__ void k_check_ranges(const int2 *ranges, int n, long long nnz, GraphCheck *c)
+{
+    int bad = 0, nc = 0;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const int2 r = ranges[v];
+        if (r.y > r.x && (r.x < 0 || (long long)r.y > nnz)) bad = 1;
+        if (r.y < r.x) nc = 1;
+        if (v == 0 && r.x != 0) nc = 1;
+        if (v + 1 < n && ranges[v + 1].x != r.y) nc = 1;
+        if (v == n - 1 && (long long)r.y != nnz) nc = 1;
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&c->bad, 1);
+    if (__any_sync(0xffffffffu, nc) && (threadIdx.x & 31) == 0) atomicOr(&c->noncontig, 1);
+}
+
+// Contiguous CSR: slots [j0, j1) in chunks of kChk, a block per chunk; the
+// owner of each slot comes from a table of the chunk's list starts.
+constexpr int kChk = 2048;
+
+__device__ __forceinline__ int first_owner(const int2 *ranges, int n, long long s)
+{
+    int lo = 0, hi = n - 1;  // largest v with ranges[v].x <= s
+    while (lo < hi) {
+        const int mid = (int)(((long long)lo + hi + 1) >> 1);
+        if ((long long)ranges[mid].x <= s) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <bool kWeights>
+__global__ void __launch_bounds__(256) k_check_entries(const int2 *ranges, const int *nbrs, const float *w, int n,
+                                                       long long j0, long long j1, GraphCheck *c)
+{
+    __shared__ int start[kChk + 1];
+    __shared__ int s_v0, s_cnt;
+    unsigned long long fs = 0, rs = 0, fw = 0, rw = 0;
+    int bad = 0, uns = 0;
+    const long long chunks = (j1 - j0 + kChk - 1) / kChk;
+    for (long long ch = blockIdx.x; ch < chunks; ch += gridDim.x) {
+        const long long c0 = j0 + ch * kChk, c1 = min(c0 + kChk, j1);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int v0 = first_owner(ranges, n, c0), v1 = first_owner(ranges, n, c1 - 1);
+            s_v0 = v0;
+            s_cnt = v1 - v0 + 1;
+        }
+        __syncthreads();
+        const int v0 = s_v0, cnt = s_cnt;
+        const bool table = cnt <= kChk + 1;
+        if (table)
+            for (int i = threadIdx.x; i < cnt; i += blockDim.x) start[i] = ranges[v0 + i].x;
+        __syncthreads();
+        for (long long j = c0 + threadIdx.x; j < c1; j += blockDim.x) {
+            int v;
+            if (table) {
+                int lo = 0, hi = cnt - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if ((long long)start[mid] <= j) lo = mid;
+                    else hi = mid - 1;
+                }
+                v = v0 + lo;
+            } else {
+                v = first_owner(ranges, n, j);
+            }
+            const int u = nbrs[j];
+            if (u < 0 || u >= n) {
+                bad = 1;
+                continue;
+            }
+            // compared with the entry before (earlier chunks have arrived; later ones may not have)
+            if (j > (long long)ranges[v].x && nbrs[j - 1] >= u) uns = 1;
+            fs += hash_s((unsigned)v, (unsigned)u);
+            rs += hash_s((unsigned)u, (unsigned)v);
+            if (kWeights) {
+                const unsigned wb = __float_as_uint(w[j]);
+                fw += hash_w((unsigned)v, (unsigned)u, wb);
+                rw += hash_w((unsigned)u, (unsigned)v, wb);
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        fs += __shfl_down_sync(0xffffffffu, fs, o);
+        rs += __shfl_down_sync(0xffffffffu, rs, o);
+        fw += __shfl_down_sync(0xffffffffu, fw, o);
+        rw += __shfl_down_sync(0xffffffffu, rw, o);
+    }
+    bad = __any_sync(0xffffffffu, bad);
+    uns = __any_sync(0xffffffffu, uns);
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&c->fwd_s, fs);
+        atomicAdd(&c->rev_s, rs);
+        if (kWeights) {
+            atomicAdd(&c->fwd_w, fw);
+            atomicAdd(&c->rev_w, rw);
+        }
+        if (bad) atomicOr(&c->bad, 2);
+        if (uns) atomicOr(&c->unsorted, 1);
+    }
+}
+
+// Any CSR: bounds of every id, a warp per list.
+__global__ void k_validate(const int2 *ranges, const int *nbrs, int n, long long nnz, GraphCheck *c)
 {
     const int lane = threadIdx.x & 31;
     const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     for (long long v = warp0; v < n; v += nwarps) {
         const int2 r = ranges[v];
-        if (r.y <= r.x) continue;
-        if (r.x < 0 || (long long)r.y > nnz) {
-            if (lane == 0) atomicOr(bad, 1);
-            continue;
-        }
+        if (r.y <= r.x || r.x < 0 || (long long)r.y > nnz) continue;
         int local = 0;
         for (int j = r.x + lane; j < r.y; j += 32) {
             const int u = nbrs[j];
             local |= (u < 0 || u >= n);
         }
-        if (__any_sync(0xffffffffu, local) && lane == 0) atomicOr(bad, 2);
+        if (__any_sync(0xffffffffu, local) && lane == 0) atomicOr(&c->bad, 2);
     }
 }
 
@@ -193,34 +327,83 @@ void free_graph(mm_graph *g)
     delete g;
 }
 
-// Shared tail of both create entry points: fill weights if absent, validate.
-mm_status finish_create(mm_graph *g, bool have_weights)
+// Graph upload and validation.  The ranges go first and are checked; for a
+// contiguous CSR the neighbour ids and weights then follow in chunks on a copy
+// stream while a second stream checks each chunk that has arrived, so the
+// checks hide under the transfer.
+constexpr long long kUploadChunk = 1ll << 24;  // entries per chunk
+
+mm_status upload_and_check(mm_graph *g, const int *ranges, const int *nbrs, const float *w,
+                           cudaMemcpyKind kind)
 {
-    const size_t m = (size_t)(g->nnz > 0 ? g->nnz : 1);
-    if (!have_weights) {
-        k_fill_one<<<grid_for((long long)m, 256, 148 * 8), 256>>>(g->d_w, (long long)m);
-        MM_CUDA_TRY(cudaGetLastError(), "unit weights");
-    }
-    g->has_weights = have_weights;
-    int *d_bad = nullptr;
-    MM_CUDA_TRY(dev_alloc((void **)&d_bad, sizeof(int), 0), "validation flag");
-    cudaError_t e = cudaMemset(d_bad, 0, sizeof(int));
-    if (e == cudaSuccess && g->n > 0) {
-        k_validate<<<grid_for((long long)g->n * 32, 256, 148 * 16), 256>>>(g->d_ranges, g->d_nbrs, g->n, g->nnz, d_bad);
+    const int n = g->n;
+    const long long nnz = g->nnz;
+    GraphCheck *d_c = nullptr;
+    MM_CUDA_TRY(dev_alloc((void **)&d_c, sizeof(GraphCheck), 0), "validation state");
+    cudaError_t e = cudaMemsetAsync(d_c, 0, sizeof(GraphCheck), 0);
+    if (e == cudaSuccess && n > 0) e = cudaMemcpyAsync(g->d_ranges, ranges, (size_t)n * sizeof(int2), kind, 0);
+    if (e == cudaSuccess && n > 0) {
+        k_check_ranges<<<grid_for(n, 256, 148 * 8), 256>>>(g->d_ranges, n, nnz, d_c);
         e = cudaGetLastError();
     }
-    int bad = 0;
-    if (e == cudaSuccess) e = cudaMemcpy(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost);
-    dev_free(d_bad, 0);
-    if (e != cudaSuccess) return cuda_fail(e, "graph validation");
-    if (bad & 1) {
+    GraphCheck c = {};
+    if (e == cudaSuccess) e = cudaMemcpy(&c, d_c, sizeof c, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && (c.bad & 1)) {
+        dev_free(d_c, 0);
         set_error("mm_graph_create: a neighbour range lies outside [0, nnz)");
         return MM_ERR_GRAPH;
     }
-    if (bad & 2) {
+    const bool contiguous = n > 0 && !c.noncontig;
+    const bool have_w = w != nullptr;
+    if (e == cudaSuccess && contiguous && nnz > 0) {
+        cudaStream_t cs = nullptr, ks = nullptr;
+        cudaEvent_t ev = nullptr;
+        e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ks, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        for (long long j0 = 0; e == cudaSuccess && j0 < nnz; j0 += kUploadChunk) {
+            const long long j1 = j0 + kUploadChunk < nnz ? j0 + kUploadChunk : nnz;
+            const size_t cnt = (size_t)(j1 - j0);
+            e = cudaMemcpyAsync(g->d_nbrs + j0, nbrs + j0, cnt * sizeof(int), kind, cs);
+            if (e == cudaSuccess && have_w) e = cudaMemcpyAsync(g->d_w + j0, w + j0, cnt * sizeof(float), kind, cs);
+            if (e == cudaSuccess) e = cudaEventRecord(ev, cs);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(ks, ev, 0);
+            if (e == cudaSuccess) {
+                const int grid = grid_for((long long)cnt, kChk, 148 * 8);
+                if (have_w) k_check_entries<true><<<grid, 256, 0, ks>>>(g->d_ranges, g->d_nbrs, g->d_w, n, j0, j1, d_c);
+                else k_check_entries<false><<<grid, 256, 0, ks>>>(g->d_ranges, g->d_nbrs, g->d_w, n, j0, j1, d_c);
+                e = cudaGetLastError();
+            }
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ks);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
+        if (ev) cudaEventDestroy(ev);
+        if (cs) cudaStreamDestroy(cs);
+        if (ks) cudaStreamDestroy(ks);
+    } else if (e == cudaSuccess) {
+        if (nnz > 0) e = cudaMemcpy(g->d_nbrs, nbrs, (size_t)nnz * sizeof(int), kind);
+        if (e == cudaSuccess && nnz > 0 && have_w) e = cudaMemcpy(g->d_w, w, (size_t)nnz * sizeof(float), kind);
+        if (e == cudaSuccess && n > 0) {
+            k_validate<<<grid_for((long long)n * 32, 256, 148 * 16), 256>>>(g->d_ranges, g->d_nbrs, n, nnz, d_c);
+            e = cudaGetLastError();
+        }
+    }
+    if (e == cudaSuccess && !have_w) {
+        const size_t m = (size_t)(nnz > 0 ? nnz : 1);
+        k_fill_one<<<grid_for((long long)m, 256, 148 * 8), 256>>>(g->d_w, (long long)m);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(&c, d_c, sizeof c, cudaMemcpyDeviceToHost);
+    dev_free(d_c, 0);
+    if (e != cudaSuccess) return cuda_fail(e, "graph upload and validation");
+    if (c.bad & 2) {
         set_error("mm_graph_create: a neighbour id lies outside [0, n)");
         return MM_ERR_GRAPH;
     }
+    g->has_weights = have_w;
+    g->sym_struct = contiguous && !c.unsorted && c.fwd_s == c.rev_s;
+    // unit weights are symmetric whenever the structure is
+    g->sym_weights = g->sym_struct && (!have_w || c.fwd_w == c.rev_w);
     return MM_OK;
 }
 
@@ -258,14 +441,13 @@ mm_status create_common(int n, const int *ranges, long long nnz, const int *nbrs
     cudaError_t e = dev_alloc((void **)&g->d_ranges, nv * sizeof(int2), 0);
     if (e == cudaSuccess) e = dev_alloc((void **)&g->d_nbrs, ne * sizeof(int), 0);
     if (e == cudaSuccess) e = dev_alloc((void **)&g->d_w, ne * sizeof(float), 0);
-    if (e == cudaSuccess) e = cudaMemset(g->d_nbrs + nnz, 0, (ne - (size_t)nnz) * sizeof(int));
-    if (e == cudaSuccess) e = cudaMemset(g->d_w + nnz, 0, (ne - (size_t)nnz) * sizeof(float));
-    if (e == cudaSuccess && n > 0) e = cudaMemcpy(g->d_ranges, ranges, (size_t)n * sizeof(int2), kind);
-    if (e == cudaSuccess && nnz > 0) e = cudaMemcpy(g->d_nbrs, nbrs, (size_t)nnz * sizeof(int), kind);
-    if (e == cudaSuccess && nnz > 0 && w) e = cudaMemcpy(g->d_w, w, (size_t)nnz * sizeof(float), kind);
+    if (e == cudaSuccess) e = cudaMemsetAsync(g->d_nbrs + nnz, 0, (ne - (size_t)nnz) * sizeof(int), 0);
+    if (e == cudaSuccess) e = cudaMemsetAsync(g->d_w + nnz, 0, (ne - (size_t)nnz) * sizeof(float), 0);
+    // the non-blocking upload streams do not wait for the legacy stream: settle the pool first
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     mm_status s = MM_OK;
-    if (e != cudaSuccess) s = cuda_fail(e, "graph upload");
-    if (s == MM_OK) s = finish_create(g, w != nullptr);
+    if (e != cudaSuccess) s = cuda_fail(e, "graph allocation");
+    if (s == MM_OK) s = upload_and_check(g, ranges, nbrs, w, kind);
     if (s != MM_OK) {
         free_graph(g);
         if (prev >= 0) cudaSetDevice(prev);

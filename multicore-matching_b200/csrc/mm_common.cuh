@@ -76,6 +76,12 @@ struct mm_graph {
     long long nnz = 0;
     bool has_weights = false;
     bool contiguous = false;  // ranges tile [0, nnz) in vertex order
+    // Set at upload: ranges tile [0, nnz), every list is strictly increasing and
+    // the entries (v, u) are those (u, v) transposed -- with the weights too for
+    // sym_weights.  Then a red vertex's order of preference over its proposers is
+    // (weight, smaller proposer id) and the push path needs no reverse index.
+    bool sym_struct = false;
+    bool sym_weights = false;
     int2 *d_ranges = nullptr;
     int *d_nbrs = nullptr;
     float *d_w = nullptr;     // unit weights when the graph came without any

@@ -90,6 +90,7 @@ struct Ctl {
 struct Params {
     int n;
     int contiguous;
+    int sym;                        // proposal keys computed from the proposer's entry (no reverse index)
     const int2 *ranges;
     const int *nbrs;
     const float *w;
@@ -255,10 +256,23 @@ __device__ __forceinline__ void fold_entry(uint8_t c, float w, int j, float &bw,
 
 // Blue vertex v proposes to `target`, the neighbour at position j of its list
 // (begin = first position): the reverse key of that slot goes to best[target].
+template <bool kW>
 __device__ __forceinline__ void propose_to(const Params &p, int v, int begin, int j, int target)
 {
-    const long long slot = p.contiguous ? (long long)j : __ldg(p.slot_off + v) + (j - begin);
-    const unsigned long long rk = __ldg(p.revkey + slot);
+    unsigned long long rk;
+    if (p.sym) {
+        // target's entry for v has v's weight, and earlier positions in its
+        // strictly increasing list hold smaller ids
+        if (kW) {
+            const float x = __ldg(p.w + j);
+            rk = x > -1.0f ? (((unsigned long long)weight_order(x) << 32) | (uint32_t)~v) : 0ull;
+        } else {
+            rk = (unsigned long long)(uint32_t)~v;
+        }
+    } else {
+        const long long slot = p.contiguous ? (long long)j : __ldg(p.slot_off + v) + (j - begin);
+        rk = __ldg(p.revkey + slot);
+    }
     if (rk) atomicMax(&p.best[target], rk);
     p.req[v] = make_int2(target, (int)(uint32_t)rk);
 }
@@ -277,6 +291,7 @@ __device__ __forceinline__ void no_proposal(const Params &p, int v, bool alive)
 }
 
 // Finish blue vertex v after a full scan whose result is `key`.
+template <bool kW>
 __device__ __forceinline__ void propose(const Params &p, int v, int begin, unsigned long long key)
 {
     if (key < 2) {
@@ -284,7 +299,7 @@ __device__ __forceinline__ void propose(const Params &p, int v, int begin, unsig
         return;
     }
     const int j = (int)~(uint32_t)key;
-    propose_to(p, v, begin, j, __ldg(p.nbrs + j));
+    propose_to<kW>(p, v, begin, j, __ldg(p.nbrs + j));
 }
 
 // Adjacency entries the reference's request loop inspects for this vertex
@@ -304,7 +319,7 @@ __device__ __forceinline__ void propose_counted(const Params &p, int4 it, unsign
         atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_REQ_ENTRIES], request_seen<kW>(it.y, degree_of(it), j));
         atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_BLUE_DEG], (unsigned long long)degree_of(it));
     }
-    propose(p, it.x, it.y, key);
+    propose<kW>(p, it.x, it.y, key);
 }
 
 constexpr int kRows = 4;    // fallback scan: rows of 32 entries per iteration
@@ -538,7 +553,7 @@ __device__ void scan_window(const Params &p, int t, int par)
                               request_seen<kW>(it[k].y, deg, cj[k]));
                     atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_BLUE_DEG], (unsigned long long)deg);
                 }
-                if (cj[k] >= 0) propose_to(p, v, it[k].y, cj[k] & 0x7fffffff, ct[k]);
+                if (cj[k] >= 0) propose_to<kW>(p, v, it[k].y, cj[k] & 0x7fffffff, ct[k]);
                 else no_proposal(p, v, alive[k]);
             } else {
                 // fallback: the whole list is scanned in phase A2
@@ -814,7 +829,9 @@ __device__ void commit_phase(const Params &p, Smem &sm, int t, bool has_next)
             if (blue[k]) {
                 if (q[k].y != 0 && (uint32_t)key[k] == (uint32_t)q[k].y) partner[k] = q[k].x;
             } else if (key[k]) {
-                partner[k] = __ldg(p.nbrs + (int)~(uint32_t)key[k]);
+                // the low half of the key names the proposer: its id on the
+                // symmetric path, else the position of the red's entry for it
+                partner[k] = p.sym ? (int)~(uint32_t)key[k] : __ldg(p.nbrs + (int)~(uint32_t)key[k]);
             }
         }
         int dest[kPer];
@@ -827,7 +844,22 @@ __device__ void commit_phase(const Params &p, Smem &sm, int t, bool has_next)
             const int deg = degree_of(it[k]);
             if (kStats && !blue[k]) {
                 rdeg += deg;
-                seen += kW ? deg : (key[k] ? (unsigned long long)((int)~(uint32_t)key[k] - it[k].y + 1) : deg);
+                // random mode: grRespond stops at its first proposer, whose position
+                // is the key's low half (symmetric path: found in the sorted list)
+                int first = -1;
+                if (!kW && key[k]) {
+                    first = (int)~(uint32_t)key[k];
+                    if (p.sym) {
+                        int lo = it[k].y, hi = it[k].z;
+                        while (lo < hi) {
+                            const int mid = (int)(((long long)lo + hi) >> 1);
+                            if (__ldg(p.nbrs + mid) < first) lo = mid + 1;
+                            else hi = mid;
+                        }
+                        first = lo;
+                    }
+                }
+                seen += first >= 0 ? (unsigned long long)(first - it[k].y + 1) : (unsigned long long)deg;
             }
             if (partner[k] >= 0) {
                 match[v] = 4 + min(v, partner[k]);
@@ -1099,12 +1131,71 @@ __global__ void k_win_sizes(const int2 *ranges, int n, long long *slots)
         slots[v] = (win_len(degree_of(ranges[v])) + 1) & ~1;
 }
 
-constexpr int kWinRows = 8;  // rows of 32 entries tested against the window threshold per step
+constexpr int kWinRows = 8;       // rows of 32 entries tested against the window threshold per step
+constexpr int kWinChunk = 4096;   // lists longer than this are split into chunks of this many entries
 
-// A warp per vertex keeps the best 32 entries seen so far sorted across its
-// lanes; a row can change them only if one of its keys beats the 32nd.
+// Merge entries [from, to) of a list into its sorted best 32 (k, nb, j): a row
+// can change them only if one of its keys beats the 32nd.
+__device__ __forceinline__ void win_merge_range(const int *nbrs, const float *w, int from, int to, int lane,
+                                                unsigned long long &k, int &nb, int &j)
+{
+    for (int base = from; base < to; base += 32 * kWinRows) {
+        float wr[kWinRows];
+#pragma unroll
+        for (int q = 0; q < kWinRows; ++q) {
+            const int jj = base + q * 32 + lane;
+            wr[q] = jj < to ? __ldg(w + jj) : 0.0f;
+        }
+#pragma unroll
+        for (int q = 0; q < kWinRows; ++q) {
+            const int jj = base + q * 32 + lane;
+            if (base + q * 32 >= to) break;
+            const unsigned long long thr = __shfl_sync(kFull, k, 31);
+            unsigned long long k2 = jj < to ? pref_key(wr[q], jj) : 0ull;
+            if (!__any_sync(kFull, k2 > thr)) continue;
+            int nb2 = jj < to ? __ldg(nbrs + jj) : 0, j2 = jj;
+            warp_sort_desc(k2, nb2, j2, lane);
+            // the larger of T[l] and R[31 - l] is a bitonic sequence holding
+            // the best 32 of both; sort it descending
+            const unsigned long long rk = __shfl_sync(kFull, k2, 31 - lane);
+            const int rnb = __shfl_sync(kFull, nb2, 31 - lane), rj = __shfl_sync(kFull, j2, 31 - lane);
+            if (rk > k) {
+                k = rk;
+                nb = rnb;
+                j = rj;
+            }
+#pragma unroll
+            for (int stride = 16; stride > 0; stride >>= 1) cas_step(k, nb, j, lane, stride, true);
+        }
+    }
+}
+
+// Best 32 entries of [from, to): the first 32 sorted, then the rest merged in.
+__device__ __forceinline__ void win_top32(const int *nbrs, const float *w, int from, int to, int lane,
+                                          unsigned long long &k, int &nb, int &j)
+{
+    k = 0ull;
+    nb = 0;
+    j = 0;
+    if (from + lane < to) {
+        j = from + lane;
+        nb = __ldg(nbrs + j);
+        k = pref_key(__ldg(w + j), j);
+    }
+    warp_sort_desc(k, nb, j, lane);
+    if (to - from > 32) win_merge_range(nbrs, w, from + 32, to, lane, k, nb, j);
+}
+
+__device__ __forceinline__ void win_store(int2 *pwin, long long off, int deg, int lane, unsigned long long k, int nb, int j)
+{
+    if (lane < win_len(deg)) pwin[off + lane] = make_int2(nb, k >= (1ull << 32) ? j : (int)((unsigned)j | 0x80000000u));
+}
+
+// Windows of lists of at most kWinChunk entries, a warp per list (vertices
+// dealt round-robin, so long lists spread over the grid); longer lists are
+// queued for the chunked kernels.
 __global__ void __launch_bounds__(256) k_win_build(const int2 *ranges, const int *nbrs, const float *w, int n,
-                                                   const long long *pwin_off, int2 *pwin)
+                                                   const long long *pwin_off, int2 *pwin, int *big, int *nbig)
 {
     const int lane = threadIdx.x & 31;
     const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -1113,44 +1204,81 @@ __global__ void __launch_bounds__(256) k_win_build(const int2 *ranges, const int
         const int2 r = ranges[v];
         const int deg = degree_of(r);
         if (deg == 0) continue;
-        unsigned long long k = 0ull;
-        int nb = 0, j = 0;
-        if (lane < deg) {
-            j = r.x + lane;
-            nb = __ldg(nbrs + j);
-            k = pref_key(__ldg(w + j), j);
+        if (deg > kWinChunk) {
+            if (lane == 0) big[atomicAdd(nbig, 1)] = (int)v;
+            continue;
         }
-        warp_sort_desc(k, nb, j, lane);
-        for (int base = r.x + 32; base < r.y; base += 32 * kWinRows) {
-            float wr[kWinRows];
-#pragma unroll
-            for (int q = 0; q < kWinRows; ++q) {
-                const int jj = base + q * 32 + lane;
-                wr[q] = jj < r.y ? __ldg(w + jj) : 0.0f;
+        unsigned long long k;
+        int nb, j;
+        win_top32(nbrs, w, r.x, r.y, lane, k, nb, j);
+        win_store(pwin, pwin_off[v], deg, lane, k, nb, j);
+    }
+}
+
+// Chunked lists, step 1: the best 32 of every kWinChunk-entry chunk of every
+// queued list, a warp per chunk.  cand holds 32 {key, nb, j} per chunk.
+struct WinCand {
+    unsigned long long k;
+    int nb;
+    int j;
+};
+
+__global__ void __launch_bounds__(256) k_win_chunks(const int2 *ranges, const int *nbrs, const float *w,
+                                                    const int *big, int nbig, const long long *chunk_off,
+                                                    WinCand *cand)
+{
+    const int lane = threadIdx.x & 31;
+    const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const long long total = chunk_off[nbig];
+    for (long long c = gwarp; c < total; c += nwarps) {
+        int lo = 0, hi = nbig - 1;  // the list holding chunk c: largest i with chunk_off[i] <= c
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (chunk_off[mid] <= c) lo = mid;
+            else hi = mid - 1;
+        }
+        const int2 r = ranges[big[lo]];
+        const int from = r.x + (int)(c - chunk_off[lo]) * kWinChunk;
+        const int to = min(from + kWinChunk, r.y);
+        unsigned long long k;
+        int nb, j;
+        win_top32(nbrs, w, from, to, lane, k, nb, j);
+        cand[c * 32 + lane] = WinCand{k, nb, j};
+    }
+}
+
+__global__ void k_win_chunk_counts(const int2 *ranges, const int *big, int nbig, long long *counts)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nbig; i += gridDim.x * blockDim.x)
+        counts[i] = (degree_of(ranges[big[i]]) + kWinChunk - 1) / kWinChunk;
+}
+
+// Chunked lists, step 2: a warp per list merges its chunks' sorted best 32s.
+__global__ void __launch_bounds__(256) k_win_chunk_merge(const int2 *ranges, const int *big, int nbig,
+                                                         const long long *chunk_off, const WinCand *cand,
+                                                         const long long *pwin_off, int2 *pwin)
+{
+    const int lane = threadIdx.x & 31;
+    const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long i = gwarp; i < nbig; i += nwarps) {
+        const long long c0 = chunk_off[i], c1 = chunk_off[i + 1];
+        WinCand x = cand[c0 * 32 + lane];
+        unsigned long long k = x.k;
+        int nb = x.nb, j = x.j;
+        for (long long c = c0 + 1; c < c1; ++c) {
+            const WinCand y = cand[c * 32 + (31 - lane)];  // reversed: the pairwise larger is bitonic
+            if (y.k > k) {
+                k = y.k;
+                nb = y.nb;
+                j = y.j;
             }
 #pragma unroll
-            for (int q = 0; q < kWinRows; ++q) {
-                const int jj = base + q * 32 + lane;
-                if (base + q * 32 >= r.y) break;
-                const unsigned long long thr = __shfl_sync(kFull, k, 31);
-                unsigned long long k2 = jj < r.y ? pref_key(wr[q], jj) : 0ull;
-                if (!__any_sync(kFull, k2 > thr)) continue;
-                int nb2 = jj < r.y ? __ldg(nbrs + jj) : 0, j2 = jj;
-                warp_sort_desc(k2, nb2, j2, lane);
-                // merge: the larger of T[l] and R[31 - l] is a bitonic sequence
-                // holding the best 32 of both; sort it descending
-                const unsigned long long rk = __shfl_sync(kFull, k2, 31 - lane);
-                const int rnb = __shfl_sync(kFull, nb2, 31 - lane), rj = __shfl_sync(kFull, j2, 31 - lane);
-                if (rk > k) {
-                    k = rk;
-                    nb = rnb;
-                    j = rj;
-                }
-#pragma unroll
-                for (int stride = 16; stride > 0; stride >>= 1) cas_step(k, nb, j, lane, stride, true);
-            }
+            for (int stride = 16; stride > 0; stride >>= 1) cas_step(k, nb, j, lane, stride, true);
         }
-        if (lane < win_len(deg)) pwin[pwin_off[v] + lane] = make_int2(nb, k >= (1ull << 32) ? j : (int)((unsigned)j | 0x80000000u));
+        const int v = big[i];
+        win_store(pwin, pwin_off[v], degree_of(ranges[v]), lane, k, nb, j);
     }
 }
 
@@ -1412,6 +1540,7 @@ Params make_params(mm_graph *g, PushState *s, bool weighted, bool stats, bool ti
     Params p;
     p.n = g->n;
     p.contiguous = g->contiguous ? 1 : 0;
+    p.sym = (weighted ? g->sym_weights : g->sym_struct) ? 1 : 0;
     p.ranges = g->d_ranges;
     p.nbrs = g->d_nbrs;
     p.w = g->d_w;
@@ -1521,16 +1650,12 @@ mm_status run_rounds(mm_graph *g, PushState *s, int type, bool stats, bool timin
 
 namespace {
 
-// Reverse proposal keys of one weighting (built once per graph).
-mm_status build_revkey(mm_graph *g, int weighted, cudaStream_t stream)
+// Degrees, classes, contiguity, slot offsets (once per graph).
+mm_status scan_graph(mm_graph *g, cudaStream_t stream)
 {
-    const int wi = weighted ? 1 : 0;
-    if (g->d_revkey[wi]) return MM_OK;
     const int n = g->n;
-    if (n == 0) return MM_OK;
-
-    // Degrees, classes, contiguity, slot offsets.
-    if (!g->scanned) {
+    if (n == 0 || g->scanned) return MM_OK;
+    {
         PrepInfo *d_info = nullptr;
         long long *d_deg = nullptr;
         MM_CUDA_TRY(dev_alloc((void **)&d_info, sizeof(PrepInfo), stream), "prep info");
@@ -1577,6 +1702,16 @@ mm_status build_revkey(mm_graph *g, int weighted, cudaStream_t stream)
         dev_free(d_deg, stream);
         g->scanned = true;
     }
+    return MM_OK;
+}
+
+// Reverse proposal keys of one weighting (built once per graph).
+mm_status build_revkey(mm_graph *g, int weighted, cudaStream_t stream)
+{
+    const int wi = weighted ? 1 : 0;
+    if (g->d_revkey[wi]) return MM_OK;
+    const int n = g->n;
+    if (n == 0) return MM_OK;
     const long long S = g->sum_degree;
 
     unsigned long long *revkey = nullptr;
@@ -1699,13 +1834,55 @@ mm_status build_windows(mm_graph *g, cudaStream_t stream)
         return MM_ERR_UNSUPPORTED;
     }
     int2 *win = nullptr;
+    int *big = nullptr;  // [n + 1]: queued long lists, then their count
     e = dev_alloc((void **)&win, sizeof(int2) * (size_t)(total > 0 ? total : 1), stream);
+    if (e == cudaSuccess) e = dev_alloc((void **)&big, sizeof(int) * ((size_t)n + 1), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(big + n, 0, sizeof(int), stream);
     if (e == cudaSuccess) {
         k_win_build<<<grid_for((long long)n * 32, 256, 148 * 16), 256, 0, stream>>>(g->d_ranges, g->d_nbrs, g->d_w, n,
-                                                                                  off, win);
+                                                                                  off, win, big, big + n);
         e = cudaGetLastError();
     }
+    int nbig = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&nbig, big + n, sizeof(int), cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess && nbig > 0) {
+        long long *coff = nullptr, *ccnt = nullptr;
+        WinCand *cand = nullptr;
+        void *tmp2 = nullptr;
+        size_t tmp2_bytes = 0;
+        long long nchunks = 0;
+        e = dev_alloc((void **)&coff, sizeof(long long) * ((size_t)nbig + 1), stream);
+        if (e == cudaSuccess) e = dev_alloc((void **)&ccnt, sizeof(long long) * ((size_t)nbig + 1), stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(ccnt + nbig, 0, sizeof(long long), stream);
+        if (e == cudaSuccess) {
+            k_win_chunk_counts<<<grid_for(nbig, 256, 148 * 4), 256, 0, stream>>>(g->d_ranges, big, nbig, ccnt);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tmp2_bytes, ccnt, coff, nbig + 1, stream);
+        if (e == cudaSuccess) e = dev_alloc(&tmp2, tmp2_bytes, stream);
+        if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp2, tmp2_bytes, ccnt, coff, nbig + 1, stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&nchunks, coff + nbig, sizeof nchunks, cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        dev_free(tmp2, stream);
+        if (e == cudaSuccess) e = dev_alloc((void **)&cand, sizeof(WinCand) * 32 * (size_t)(nchunks > 0 ? nchunks : 1), stream);
+        if (e == cudaSuccess) {
+            k_win_chunks<<<grid_for(nchunks * 32, 256, 148 * 16), 256, 0, stream>>>(g->d_ranges, g->d_nbrs, g->d_w, big,
+                                                                                  nbig, coff, cand);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) {
+            k_win_chunk_merge<<<grid_for((long long)nbig * 32, 256, 148 * 16), 256, 0, stream>>>(
+                g->d_ranges, big, nbig, coff, cand, off, win);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        dev_free(cand, stream);
+        dev_free(ccnt, stream);
+        dev_free(coff, stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    dev_free(big, stream);
     if (e != cudaSuccess) {
         dev_free(win, stream);
         dev_free(off, stream);
@@ -1720,7 +1897,10 @@ mm_status build_windows(mm_graph *g, cudaStream_t stream)
 
 mm_status push_prepare(mm_graph *g, int weighted, cudaStream_t stream)
 {
-    mm_status st = build_revkey(g, weighted, stream);
+    // the symmetric path computes each proposal's key: no reverse index
+    const bool sym = weighted ? g->sym_weights : g->sym_struct;
+    mm_status st = scan_graph(g, stream);
+    if (st == MM_OK && !sym) st = build_revkey(g, weighted, stream);
     if (st == MM_OK && weighted && g->n > 0 && !g->d_pwin) st = build_windows(g, stream);
     return st;
 }
