@@ -66,7 +66,7 @@ constexpr int kThreads = 512;            // threads per block of the round kerne
 constexpr int kWarps = kThreads / 32;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kWin = 32;                 // preference window: the first min(deg, 32) choices
-constexpr int kSegEntries = 992;         // entries per fallback segment: 31 rows of 32; at most 32
+constexpr int kSegEntries = 256;         // entries per fallback segment: 8 rows of 32; at most 9
                                          // pieces of lists > 32 entries overlap one segment
 
 // Worklists: blue and red vertices by round parity; the staged list holds the round's
@@ -574,7 +574,7 @@ __device__ void scan_window(const Params &p, int t, int par)
 // and cut into kSegEntries-entry segments; seg_first[s] is the first item
 // overlapping segment s.  Items are numbered in offset order: one 64-bit
 // atomic hands out both.  A warp takes a segment: lane l describes the l-th
-// list piece in it (at most 32), then the warp walks the segment in rows of
+// list piece in it (at most 9), then the warp walks the segment in rows of
 // 32 consecutive entries.  Every piece but the segment's first and last is a
 // whole list of more than 32 entries, so a row holds at most one piece
 // boundary and the piece being scanned is the same for the whole warp: each
