@@ -355,12 +355,18 @@ mm_status upload_and_check(mm_graph *g, const int *ranges, const int *nbrs, cons
     }
     const bool contiguous = n > 0 && !c.noncontig;
     const bool have_w = w != nullptr;
+    // Weighted graphs from host memory also get their preference windows here:
+    // a chunk's check is followed by the windows of the vertices whose lists
+    // end in it (host ranges say which), so they too hide under the transfer.
+    bool windows = e == cudaSuccess && contiguous && nnz > 0 && have_w && kind == cudaMemcpyHostToDevice;
+    if (windows && windows_begin(g, 0) != MM_OK) windows = false;
     if (e == cudaSuccess && contiguous && nnz > 0) {
         cudaStream_t cs = nullptr, ks = nullptr;
         cudaEvent_t ev = nullptr;
         e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ks, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        int va = 0;  // first vertex whose window is not built yet
         for (long long j0 = 0; e == cudaSuccess && j0 < nnz; j0 += kUploadChunk) {
             const long long j1 = j0 + kUploadChunk < nnz ? j0 + kUploadChunk : nnz;
             const size_t cnt = (size_t)(j1 - j0);
@@ -374,9 +380,24 @@ mm_status upload_and_check(mm_graph *g, const int *ranges, const int *nbrs, cons
                 else k_check_entries<false><<<grid, 256, 0, ks>>>(g->d_ranges, g->d_nbrs, g->d_w, n, j0, j1, d_c);
                 e = cudaGetLastError();
             }
+            if (e == cudaSuccess && windows) {
+                // vertices whose lists end at or before j1 (ends rise with v)
+                int lo = va, hi = n;
+                while (lo < hi) {
+                    const int mid = lo + (hi - lo) / 2;
+                    if ((long long)ranges[2 * (size_t)mid + 1] <= j1) lo = mid + 1;
+                    else hi = mid;
+                }
+                const int vb = j1 == nnz ? n : lo;
+                if (windows_range(g, va, vb, ks) != MM_OK) windows = false;
+                va = vb;
+            }
         }
-        if (e == cudaSuccess) e = cudaStreamSynchronize(ks);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
+        if (e == cudaSuccess && windows && windows_end(g, ks) != MM_OK) windows = false;
+        // both streams are drained on every path: buffers may be freed next
+        const cudaError_t eks = ks ? cudaStreamSynchronize(ks) : cudaSuccess;
+        const cudaError_t ecs = cs ? cudaStreamSynchronize(cs) : cudaSuccess;
+        if (e == cudaSuccess) e = eks != cudaSuccess ? eks : ecs;
         if (ev) cudaEventDestroy(ev);
         if (cs) cudaStreamDestroy(cs);
         if (ks) cudaStreamDestroy(ks);
@@ -395,6 +416,8 @@ mm_status upload_and_check(mm_graph *g, const int *ranges, const int *nbrs, cons
     }
     if (e == cudaSuccess) e = cudaMemcpy(&c, d_c, sizeof c, cudaMemcpyDeviceToHost);
     dev_free(d_c, 0);
+    if (!windows) windows_discard(g);  // built later, on demand, if the upload could not
+    cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "graph upload and validation");
     if (c.bad & 2) {
         set_error("mm_graph_create: a neighbour id lies outside [0, n)");

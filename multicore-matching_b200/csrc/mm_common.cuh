@@ -104,6 +104,8 @@ struct mm_graph {
     long long *d_slot_off = nullptr;  // non-contiguous CSR: slot index of vertex v's first entry
     int2 *d_pwin = nullptr;           // weighted types: preference windows {neighbour, position | flag}
     long long *d_pwin_off = nullptr;  // weighted types: first window slot of each vertex; [n] = total
+    int2 *win_build = nullptr;        // windows while being built (d_pwin once complete)
+    int *win_big = nullptr;           // while being built: queued lists longer than a window chunk
 
     // push path: captured CUDA graph of the round loop
     void *push_exec = nullptr;  // internal (mm::PushPlan *)
@@ -143,6 +145,11 @@ mm_status push_match(mm_graph *g, int type, uint32_t barrier, const uint32_t *se
 mm_status push_profile(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds, int *d_match,
                        int *rounds_out, float *ms_kernels, int cap_rounds, int *launched, cudaStream_t stream);
 void push_release(mm_graph *g);
+// Preference windows of the weighted types, in steps (see mm_push.cu).
+mm_status windows_begin(mm_graph *g, cudaStream_t stream);
+mm_status windows_range(mm_graph *g, int va, int vb, cudaStream_t stream);
+mm_status windows_end(mm_graph *g, cudaStream_t stream);
+void windows_discard(mm_graph *g);
 
 inline int max_rounds_of(int type)
 {

@@ -1194,13 +1194,13 @@ __device__ __forceinline__ void win_store(int2 *pwin, long long off, int deg, in
 // Windows of lists of at most kWinChunk entries, a warp per list (vertices
 // dealt round-robin, so long lists spread over the grid); longer lists are
 // queued for the chunked kernels.
-__global__ void __launch_bounds__(256) k_win_build(const int2 *ranges, const int *nbrs, const float *w, int n,
+__global__ void __launch_bounds__(256) k_win_build(const int2 *ranges, const int *nbrs, const float *w, int va, int vb,
                                                    const long long *pwin_off, int2 *pwin, int *big, int *nbig)
 {
     const int lane = threadIdx.x & 31;
     const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long v = gwarp; v < n; v += nwarps) {
+    for (long long v = va + gwarp; v < vb; v += nwarps) {
         const int2 r = ranges[v];
         const int deg = degree_of(r);
         if (deg == 0) continue;
@@ -1802,8 +1802,15 @@ mm_status build_revkey(mm_graph *g, int weighted, cudaStream_t stream)
     return MM_OK;
 }
 
-// Preference windows of the weighted types (built once per graph).
-mm_status build_windows(mm_graph *g, cudaStream_t stream)
+}  // namespace
+
+// Preference windows of the weighted types, built once per graph in three
+// steps so that the upload can build the windows of the lists that have
+// arrived while later chunks are still in transfer: windows_begin sizes and
+// allocates them (it needs only the ranges), windows_range builds those of
+// vertices [va, vb) and queues lists longer than kWinChunk, windows_end builds
+// the queued lists and publishes d_pwin.
+mm_status windows_begin(mm_graph *g, cudaStream_t stream)
 {
     const int n = g->n;
     long long *slots = nullptr, *off = nullptr;
@@ -1838,13 +1845,36 @@ mm_status build_windows(mm_graph *g, cudaStream_t stream)
     e = dev_alloc((void **)&win, sizeof(int2) * (size_t)(total > 0 ? total : 1), stream);
     if (e == cudaSuccess) e = dev_alloc((void **)&big, sizeof(int) * ((size_t)n + 1), stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(big + n, 0, sizeof(int), stream);
-    if (e == cudaSuccess) {
-        k_win_build<<<grid_for((long long)n * 32, 256, 148 * 16), 256, 0, stream>>>(g->d_ranges, g->d_nbrs, g->d_w, n,
-                                                                                  off, win, big, big + n);
-        e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) {
+        dev_free(win, stream);
+        dev_free(big, stream);
+        dev_free(off, stream);
+        return cuda_fail(e, "window buffers");
     }
+    g->win_build = win;
+    g->win_big = big;
+    g->d_pwin_off = off;
+    return MM_OK;
+}
+
+mm_status windows_range(mm_graph *g, int va, int vb, cudaStream_t stream)
+{
+    if (vb <= va) return MM_OK;
+    k_win_build<<<grid_for((long long)(vb - va) * 32, 256, 148 * 16), 256, 0, stream>>>(
+        g->d_ranges, g->d_nbrs, g->d_w, va, vb, g->d_pwin_off, g->win_build, g->win_big, g->win_big + g->n);
+    MM_CUDA_TRY(cudaGetLastError(), "preference windows");
+    return MM_OK;
+}
+
+mm_status windows_end(mm_graph *g, cudaStream_t stream)
+{
+    const int n = g->n;
+    int *big = g->win_big;
+    int2 *win = g->win_build;
+    const long long *off = g->d_pwin_off;
     int nbig = 0;
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&nbig, big + n, sizeof(int), cudaMemcpyDeviceToHost, stream);
+    cudaError_t e = cudaMemcpyAsync(&nbig, big + n, sizeof(int), cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e == cudaSuccess && nbig > 0) {
         long long *coff = nullptr, *ccnt = nullptr;
@@ -1883,14 +1913,36 @@ mm_status build_windows(mm_graph *g, cudaStream_t stream)
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     dev_free(big, stream);
+    g->win_big = nullptr;
     if (e != cudaSuccess) {
-        dev_free(win, stream);
-        dev_free(off, stream);
+        windows_discard(g);
         return cuda_fail(e, "preference windows");
     }
     g->d_pwin = win;
-    g->d_pwin_off = off;
+    g->win_build = nullptr;
     return MM_OK;
+}
+
+void windows_discard(mm_graph *g)
+{
+    dev_free(g->win_build, 0);
+    dev_free(g->win_big, 0);
+    if (!g->d_pwin) {
+        dev_free(g->d_pwin_off, 0);
+        g->d_pwin_off = nullptr;
+    }
+    g->win_build = nullptr;
+    g->win_big = nullptr;
+}
+
+namespace {
+
+mm_status build_windows(mm_graph *g, cudaStream_t stream)
+{
+    mm_status st = windows_begin(g, stream);
+    if (st == MM_OK) st = windows_range(g, 0, g->n, stream);
+    if (st == MM_OK) st = windows_end(g, stream);
+    return st;
 }
 
 }  // namespace
@@ -1974,6 +2026,7 @@ void push_release(mm_graph *g)
     }
     dev_free(g->d_slot_off, 0);
     g->d_slot_off = nullptr;
+    windows_discard(g);
     dev_free(g->d_pwin, 0);
     g->d_pwin = nullptr;
     dev_free(g->d_pwin_off, 0);
