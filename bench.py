@@ -220,7 +220,7 @@ def cpu_baseline(mm, g, t, gpu_match, workload):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -312,6 +312,9 @@ def main():
     # the round kernel is the only kernel of a matching: its bytes over the whole step's device time
     achieved = kernel_bytes / (ms / 1e3) / 1e9
     peak, peak_kind = load_peaks()
+    # the scans are bound by random single-sector reads: their measured ceiling on this device
+    gather_peak = mm.probe_gather_rate(local, max(g.n, 1))
+    colour_gathers = float(st[:, mm.ST_WINDOW_ENTRIES].sum() + st[:, mm.ST_STAGED_DEG].sum())
     traffic = None
     tfile = ROOT / "profiles" / f"traffic_{args.workload}.json"
     if tfile.exists():
@@ -398,7 +401,10 @@ def main():
                          "per_round_ms": {"window": [round(float(x), 4) for x in ms_k[:, 0]],
                                           "fallback": [round(float(x), 4) for x in ms_k[:, 1]],
                                           "commit": [round(float(x), 4) for x in ms_k[:, 2]]},
-                         "reference_formula_gbs": work["reference_bytes"] / (ms / 1e3) / 1e9},
+                         "reference_formula_gbs": work["reference_bytes"] / (ms / 1e3) / 1e9,
+                         "random_reads": {"ceiling_per_s": gather_peak, "ceiling": "mm_probe_gather_rate, table of n bytes",
+                                          "colour_gathers_per_step": colour_gathers,
+                                          "colour_gathers_per_s": colour_gathers / (ms / 1e3)}},
             "gpu_launches": gpu_launches,
             "clocks": clocks.summary(),
         }

@@ -191,6 +191,15 @@ mm_status mm_match_noalloc(int n, const int *d_ranges, long long nnz, const int 
                            const float *d_weights, int type, uint32_t barrier, const uint32_t *seeds,
                            int nseeds, int *d_match_out, int *rounds_out, void *stream);
 
+/*
+ * Measurement entry, no counterpart in the reference: the device's rate of
+ * random one-byte reads (2^27 gathers from a table of table_bytes bytes,
+ * indices streamed coalesced), in gathers per second, best of four runs.
+ * The round kernel's scans are bound by such reads rather than by streaming
+ * bandwidth, so this is the ceiling their rate is reported against.
+ */
+mm_status mm_probe_gather_rate(int device, long long table_bytes, double *gathers_per_s);
+
 /* Message of the calling thread's most recent failure ("" if none). */
 const char *mm_last_error(void);
 

@@ -83,6 +83,7 @@ _MM_SIGS = {
     "mm_match_device": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P]),
     "mm_match_ex": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _I, _P]),
     "mm_match_stats": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P, _I, _I, _P]),
+    "mm_probe_gather_rate": (_I, [_I, _LL, ctypes.POINTER(ctypes.c_double)]),
     "mm_match_profile": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P, _I, ctypes.POINTER(_I), _P]),
     "mm_match_noalloc": (_I, [_I, _P, _LL, _P, _P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P]),
     "mm_last_error": (ctypes.c_char_p, []),
@@ -302,6 +303,13 @@ class DeviceGraph:
                                           stream or None))
         executed = int(np.count_nonzero(ms[:, 3] > 0))
         return rounds.value, ms[:executed], launches.value
+
+
+def probe_gather_rate(device: int = 0, table_bytes: int = 8 << 20) -> float:
+    """Random one-byte gathers per second the device sustains (mm_probe_gather_rate)."""
+    rate = ctypes.c_double(0.0)
+    _check(lib().mm_probe_gather_rate(device, table_bytes, ctypes.byref(rate)))
+    return rate.value
 
 
 def roofline_bytes(stats: np.ndarray, weighted: bool) -> dict:

@@ -514,6 +514,37 @@ mm_status check_match_args(mm_graph *g, int type, const uint32_t *seeds, int nse
     return MM_OK;
 }
 
+// ---- measurement: random-gather ceiling ----
+//
+// The round kernel's scans are bound by random single-sector reads (colour
+// gathers, window and key loads), not by streaming bandwidth.  This probe
+// times the device's rate for them: every thread reads a coalesced stream of
+// random indices and gathers one byte per index from a table.
+__global__ void k_probe_indices(int *idx, long long m, int range, unsigned long long seed)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x) {
+        unsigned long long z = (unsigned long long)i * 0x9E3779B97F4A7C15ull + seed;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        idx[i] = (int)((z >> 32) % (unsigned long long)range);
+    }
+}
+
+__global__ void k_probe_gather(const int *__restrict__ idx, long long m, const uint8_t *table, unsigned *sink)
+{
+    unsigned acc = 0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += 4 * stride) {
+        int j[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) j[k] = i + k * stride < m ? __ldcs(idx + i + k * stride) : 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) acc += table[j[k]];
+    }
+    if (acc == 0xffffffffu) sink[0] = acc;  // keeps the gathers live
+}
+
 }  // namespace
 }  // namespace mm
 
@@ -627,3 +658,54 @@ MM_API mm_status mm_match_profile(mm_graph *g, int type, uint32_t barrier, const
 MM_API const char *mm_last_error(void) { return g_last_error.c_str(); }
 
 MM_API const char *mm_version(void) { return "mmatch 0.1 (sm_100a)"; }
+
+MM_API mm_status mm_probe_gather_rate(int device, long long table_bytes, double *gathers_per_s)
+{
+    if (!gathers_per_s || table_bytes < 1 || table_bytes > (1ll << 30)) {
+        set_error("mm_probe_gather_rate: table_bytes must be in [1, 2^30] and the output non-null");
+        return MM_ERR_ARG;
+    }
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (device >= 0) MM_CUDA_TRY(cudaSetDevice(device), "set device");
+    const long long m = 1ll << 27;  // indices (512 MB, more than L2 holds)
+    int *idx = nullptr;
+    uint8_t *table = nullptr;
+    unsigned *sink = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaError_t e = dev_alloc((void **)&idx, sizeof(int) * (size_t)m, 0);
+    if (e == cudaSuccess) e = dev_alloc((void **)&table, (size_t)table_bytes, 0);
+    if (e == cudaSuccess) e = dev_alloc((void **)&sink, sizeof(unsigned), 0);
+    if (e == cudaSuccess) e = cudaMemsetAsync(table, 1, (size_t)table_bytes, 0);
+    if (e == cudaSuccess) e = cudaEventCreate(&a);
+    if (e == cudaSuccess) e = cudaEventCreate(&b);
+    int sms = 148;
+    if (e == cudaSuccess) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        k_probe_indices<<<sms * 8, 256>>>(idx, m, (int)(table_bytes < (1ll << 31) ? table_bytes : (1ll << 31) - 1), 12345);
+        e = cudaGetLastError();
+    }
+    float best = 1e30f;
+    for (int rep = 0; e == cudaSuccess && rep < 4; ++rep) {
+        cudaEventRecord(a, 0);
+        k_probe_gather<<<sms * 8, 256>>>(idx, m, table, sink);
+        cudaEventRecord(b, 0);
+        e = cudaEventSynchronize(b);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+        if (e == cudaSuccess && ms < best) best = ms;
+    }
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    dev_free(idx, 0);
+    dev_free(table, 0);
+    dev_free(sink, 0);
+    cudaStreamSynchronize(0);
+    if (prev >= 0 && device >= 0) cudaSetDevice(prev);
+    if (e != cudaSuccess) return cuda_fail(e, "gather probe");
+    *gathers_per_s = (double)m / (best * 1e-3);
+    return MM_OK;
+}
+
