@@ -192,6 +192,28 @@ mm_status mm_match_noalloc(int n, const int *d_ranges, long long nnz, const int 
                            int nseeds, int *d_match_out, int *rounds_out, void *stream);
 
 /*
+ * Weight and size of a matching, computed on the device exactly as
+ * GraphMatching::getWeight does (src/matchcpu.cu:64-97): a matched vertex adds
+ * the weight of the first entry of its list whose neighbour carries the same
+ * match value, and counts one; weight is half the sum (double), size the
+ * count of such vertices.  d_match: n ints on g's device.  The sum is taken in
+ * a fixed tree, not the reference's vertex order: it agrees to rounding.
+ */
+mm_status mm_matching_weight(mm_graph *g, const int *d_match, double *weight, long long *size, void *stream);
+
+/*
+ * GraphMatching::testMatching (src/matchcpu.cu:127-246) on the device.
+ * counts[0] under-matched (matched to themselves), [1] matched to more than
+ * one vertex, [2] not matched to a neighbour, [3] can still be matched,
+ * [4] unmatched; *valid = 1 iff counts[0..2] are all 0 (the reference's return
+ * value: maximality is reported, not enforced).  The counts follow the
+ * reference's walk over the vertices sorted by match value.  Where a value is
+ * shared by three or more vertices, the reference's order among them is
+ * std::sort's; here it is ascending id.
+ */
+mm_status mm_matching_check(mm_graph *g, const int *d_match, long long counts[5], int *valid, void *stream);
+
+/*
  * Measurement entry, no counterpart in the reference: the device's rate of
  * random one-byte reads (2^27 gathers from a table of table_bytes bytes,
  * indices streamed coalesced), in gathers per second, best of four runs.

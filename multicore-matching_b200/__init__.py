@@ -83,6 +83,8 @@ _MM_SIGS = {
     "mm_match_device": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P]),
     "mm_match_ex": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _I, _P]),
     "mm_match_stats": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P, _I, _I, _P]),
+    "mm_matching_weight": (_I, [_P, _P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_LL), _P]),
+    "mm_matching_check": (_I, [_P, _P, _P, ctypes.POINTER(_I), _P]),
     "mm_probe_gather_rate": (_I, [_I, _LL, ctypes.POINTER(ctypes.c_double)]),
     "mm_match_profile": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P, _I, ctypes.POINTER(_I), _P]),
     "mm_match_noalloc": (_I, [_I, _P, _LL, _P, _P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P]),
@@ -286,6 +288,21 @@ class DeviceGraph:
                                         ctypes.byref(rounds), _ptr(st), 255, path, stream or None))
         return rounds.value, st[: rounds.value]
 
+
+    def weight(self, d_match: int, stream: int = 0):
+        """(weight, size) of the device matching at d_match, as getWeight computes them."""
+        wt = ctypes.c_double(0.0)
+        sz = ctypes.c_longlong(0)
+        _check(self._lib.mm_matching_weight(self.handle, d_match, ctypes.byref(wt), ctypes.byref(sz), stream or None))
+        return wt.value, sz.value
+
+    def check(self, d_match: int, stream: int = 0) -> dict:
+        """testMatching's counters for the device matching at d_match."""
+        counts = np.zeros(5, dtype=np.int64)
+        valid = ctypes.c_int(0)
+        _check(self._lib.mm_matching_check(self.handle, d_match, _ptr(counts), ctypes.byref(valid), stream or None))
+        return {"valid": bool(valid.value), "under": int(counts[0]), "multi": int(counts[1]),
+                "invalid": int(counts[2]), "matchable": int(counts[3]), "unmatched": int(counts[4])}
 
     def profile(self, type_: int, seeds: np.ndarray, d_out: int, barrier: int = DEFAULT_BARRIER, stream: int = 0):
         """Timed run of the round kernel with barrier timestamps.

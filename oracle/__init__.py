@@ -62,6 +62,7 @@ _REF_SIGS = {
     "mmref_run": (_I, [_I, _I, _P, _LL, _P, _P, _U, _U, _I, _P, ctypes.POINTER(ctypes.c_double),
                        ctypes.POINTER(_U)]),
     "mmref_check": (_I, [_I, _P, _LL, _P, _P, _P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_LL)]),
+    "mmref_check_counts": (_I, [_I, _P, _LL, _P, _P, _P, _P]),
     "mmref_read": (_I, [ctypes.c_char_p, _I, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_LL), _P, _P,
                         _P]),
     "mmref_cli": (_I, [ctypes.c_char_p, _I, _I, _U, _U, _I, _I, _P, ctypes.POINTER(_U)]),
@@ -158,6 +159,16 @@ def ref_check(g, m: np.ndarray):
     ok = ref_lib().mmref_check(g.n, _p(ranges), g.nnz, _p(nbrs), _p(w), _p(m), ctypes.byref(wt),
                                ctypes.byref(sz))
     return bool(ok), wt.value, sz.value
+
+
+def ref_check_counts(g, m: np.ndarray) -> dict:
+    """The reference's own testMatching counters (src/matchcpu.cu:127-246), as it prints them."""
+    ranges, nbrs, w = _arrays(g)
+    m = np.ascontiguousarray(m, dtype=np.int32)
+    out = np.full(4, -1, dtype=np.int64)
+    ok = ref_lib().mmref_check_counts(g.n, _p(ranges), g.nnz, _p(nbrs), _p(w), _p(m), _p(out))
+    return {"valid": bool(ok), "under": int(out[0]), "multi": int(out[1]), "invalid": int(out[2]),
+            "matchable": int(out[3])}
 
 
 def _is_mtx(path) -> int:

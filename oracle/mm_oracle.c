@@ -274,40 +274,48 @@ void mmo_weight(int n, const int *ranges, const int *nbrs, const float *w, const
     *size_out = size;
 }
 
-/*
- * Matching validity and maximality counters, following testMatching
- * (matchcpu.cu:127-246) without its sort: groups vertices by match value.
- * out[0] under-matched (a matched value held by one vertex), out[1]
- * multi-matched (extra holders beyond two), out[2] pairs that are not
- * neighbours in both directions, out[3] unmatched vertices that still have an
- * unmatched neighbour other than themselves (maximality; 0 for a maximal
- * matching).  Returns 1 iff out[0..2] are all zero.
- */
+/* testMatching (src/matchcpu.cu:127-246): the matched vertices sorted by match
+ * value (ties by id here; the reference's std::sort leaves that order open) are
+ * walked two at a time.  i1, then i2: if i2's value differs, i1 is
+ * under-matched and i2 is consumed with it; else the pair must be in each
+ * other's lists (else invalidly matched) and every further vertex of the value
+ * is multi-matched.  Then every unmatched vertex with an unmatched neighbour
+ * other than itself can still be matched.  out: under, multi, invalid,
+ * matchable; returns the verdict (the first three are zero). */
+static const int *g_sort_match;
+static int by_value_then_id(const void *pa, const void *pb)
+{
+    const int a = *(const int *)pa, b = *(const int *)pb;
+    const int ma = g_sort_match[a], mb = g_sort_match[b];
+    if (ma != mb) return ma < mb ? -1 : 1;
+    return a < b ? -1 : (a > b);
+}
+
+static int in_span(const int *ranges, const int *nbrs, int a, int b)
+{
+    for (int j = span_begin(ranges, a); j < span_end(ranges, a); ++j)
+        if (nbrs[j] == b) return 1;
+    return 0;
+}
+
 int mmo_check(int n, const int *ranges, const int *nbrs, const int *match, long long out[4])
 {
-    /* holder count and first two holders per matched value 4 + v */
-    int *count = (int *)calloc((size_t)(n > 0 ? n : 1), sizeof(int));
-    int *first = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
-    int *second = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    int *order = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    int cnt = 0;
+    for (int v = 0; v < n; ++v)
+        if (match[v] >= 4) order[cnt++] = v;
+    g_sort_match = match;
+    qsort(order, (size_t)cnt, sizeof(int), by_value_then_id);
     long long under = 0, multi = 0, invalid = 0, matchable = 0;
-    for (int v = 0; v < n; ++v) {
-        const int m = match[v];
-        if (m < 4) continue;
-        const long long slot = (long long)m - 4;
-        if (slot >= n) { ++invalid; continue; }
-        if (count[slot] == 0) first[slot] = v;
-        else if (count[slot] == 1) second[slot] = v;
-        ++count[slot];
-    }
-    for (int s = 0; s < n; ++s) {
-        if (count[s] == 0) continue;
-        if (count[s] == 1) { ++under; continue; }
-        if (count[s] > 2) multi += count[s] - 2;
-        const int a = first[s], b = second[s];
-        int fa = 0, fb = 0;
-        for (int j = span_begin(ranges, a); j < span_end(ranges, a) && !fa; ++j) fa = nbrs[j] == b;
-        for (int j = span_begin(ranges, b); j < span_end(ranges, b) && !fb; ++j) fb = nbrs[j] == a;
-        if (!fa || !fb) ++invalid;
+    int p = 0;
+    while (p < cnt) {
+        const int i1 = order[p++];
+        const int cur = match[i1];
+        if (p == cnt) { ++under; continue; }
+        const int i2 = order[p++];
+        if (match[i2] != cur) { ++under; continue; }
+        if (!in_span(ranges, nbrs, i1, i2) || !in_span(ranges, nbrs, i2, i1)) ++invalid;
+        while (p < cnt && match[order[p]] == cur) { ++multi; ++p; }
     }
     for (int v = 0; v < n; ++v) {
         if (match[v] >= 4) continue;
@@ -316,7 +324,7 @@ int mmo_check(int n, const int *ranges, const int *nbrs, const int *match, long 
             if (u != v && match[u] < 4) { ++matchable; break; }
         }
     }
-    free(count); free(first); free(second);
+    free(order);
     out[0] = under; out[1] = multi; out[2] = invalid; out[3] = matchable;
     return under == 0 && multi == 0 && invalid == 0;
 }

@@ -16,6 +16,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <sstream>
+#include <cstdio>
 #include <string>
 #include <vector>
 
@@ -113,6 +115,31 @@ MMREF_API int mmref_check(int n, const int *ranges, long long nnz, const int *nb
     *weight = wt;
     *size = sz;
     return mtc::GraphMatching::testMatching(m, g) ? 1 : 0;
+}
+
+/*
+ * testMatching's four counters (matchcpu.cu:239-243), read from the lines it
+ * prints: matched to themselves, to more than one vertex, not to a
+ * neighbour, can still be matched.  Returns its verdict.
+ */
+MMREF_API int mmref_check_counts(int n, const int *ranges, long long nnz, const int *nbrs, const float *w,
+                                 const int *match, long long counts[4])
+{
+    mtc::Graph g;
+    build_graph(g, n, ranges, nnz, nbrs, w, false);
+    std::vector<int> m(match, match + n);
+    std::ostringstream text;
+    std::streambuf *saved = std::cout.rdbuf(text.rdbuf());
+    const bool ok = mtc::GraphMatching::testMatching(m, g);
+    std::cout.rdbuf(saved);
+    std::istringstream lines(text.str());
+    std::string line;
+    int k = 0;
+    while (std::getline(lines, line) && k < 4) {
+        long long v = 0;
+        if (line.rfind("    ", 0) == 0 && std::sscanf(line.c_str(), " %lld", &v) == 1) counts[k++] = v;
+    }
+    return ok ? 1 : 0;
 }
 
 /*

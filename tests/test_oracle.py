@@ -104,6 +104,30 @@ def test_checker_flags_planted_mistakes(mm, orc):
 
 
 @pytest.mark.skipif("not __import__('oracle').ref_available()")
+def test_checker_counts_equal_reference(mm, orc):
+    """Pin of the restated testMatching counters against the reference's own,
+    on matchings broken in each of its ways (the walk over values sorted by
+    match value shifts after an unpaired vertex; the counters must follow it).
+    Where a value has three or more holders the reference's order among them
+    is std::sort's, so 'invalid' is compared only when no value has."""
+    rng = np.random.default_rng(4)
+    for g in (mm.Graph.grid(16, 16), mm.Graph.rmat(10, 8, seed=2), mm.Graph.er(300, 5.0, seed=3)):
+        m, _, _ = orc.match(g, 9, orc.rand_seeds(7), BARRIER)
+        cases = [m]
+        for trial in range(12):
+            x = m.copy()
+            idx = rng.choice(g.n, size=1 + trial % 5, replace=False)
+            x[idx] = rng.integers(-2, g.n + 8, size=len(idx))
+            cases.append(x)
+        for x in cases:
+            got, want = orc.check(g, x), orc.ref_check_counts(g, x)
+            vals, counts = np.unique(x[x >= 4], return_counts=True)
+            keys = ("valid", "under", "multi", "matchable") + (("invalid",) if (counts < 3).all() else ())
+            for k in keys:
+                assert got[k] == want[k], (g.name, k, got, want)
+
+
+@pytest.mark.skipif("not __import__('oracle').ref_available()")
 def test_oracle_equals_reference_live(mm, orc):
     """Live pin: restatement vs the reference's TBB matchers on fresh graphs."""
     rng = np.random.default_rng(77)
