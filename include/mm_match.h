@@ -124,6 +124,13 @@ const void *mm_graph_device_ranges(const mm_graph *g);
 const int *mm_graph_device_neighbours(const mm_graph *g);
 const float *mm_graph_device_weights(const mm_graph *g);
 
+/*
+ * Copy g's CSR to host arrays: ranges (2n ints), neighbours (nnz ints) and
+ * weights (nnz floats; unit weights if g was created without), each may be
+ * NULL to skip it.  For graphs the library made, such as coarse graphs.
+ */
+mm_status mm_graph_copy_out(const mm_graph *g, int *ranges, int *neighbours, float *weights);
+
 /* Round cap of a type: 20 (types 6, 8) or 255 (types 7, 9); -1 if unknown. */
 int mm_max_rounds(int type);
 
@@ -212,6 +219,21 @@ mm_status mm_matching_weight(mm_graph *g, const int *d_match, double *weight, lo
  * std::sort's; here it is ascending id.
  */
 mm_status mm_matching_check(mm_graph *g, const int *d_match, long long counts[5], int *valid, void *stream);
+
+/*
+ * One level of multilevel coarsening; no counterpart in the reference, which
+ * stops at the matching.  Contracts each matched pair of d_match (n ints on
+ * g's device, values 4 + min(v, partner) as mm_match writes them) into one
+ * vertex; unmatched vertices stay.  Coarse vertex ids follow the smaller
+ * member's id order.  The coarse lists hold the members' entries mapped to
+ * coarse ids, in increasing id, without self-loops.  An edge that several fine
+ * entries map to carries their weights' sum, taken in double and rounded once
+ * (unit weights when g has none).  *coarse is a new graph on the same device,
+ * to be freed with mm_graph_destroy.  d_cmap (n ints on the device, or NULL)
+ * receives each vertex's coarse id.  A match array whose value names no
+ * partner that names it back gives MM_ERR_ARG.
+ */
+mm_status mm_graph_contract(mm_graph *g, const int *d_match, mm_graph **coarse, int *d_cmap);
 
 /*
  * Measurement entry, no counterpart in the reference: the device's rate of

@@ -85,6 +85,8 @@ _MM_SIGS = {
     "mm_match_stats": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P, _I, _I, _P]),
     "mm_matching_weight": (_I, [_P, _P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_LL), _P]),
     "mm_matching_check": (_I, [_P, _P, _P, ctypes.POINTER(_I), _P]),
+    "mm_graph_contract": (_I, [_P, _P, ctypes.POINTER(_P), _P]),
+    "mm_graph_copy_out": (_I, [_P, _P, _P, _P]),
     "mm_probe_gather_rate": (_I, [_I, _LL, ctypes.POINTER(ctypes.c_double)]),
     "mm_match_profile": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P, _I, ctypes.POINTER(_I), _P]),
     "mm_match_noalloc": (_I, [_I, _P, _LL, _P, _P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P]),
@@ -289,6 +291,30 @@ class DeviceGraph:
         return rounds.value, st[: rounds.value]
 
 
+    def contract(self, d_match: int, d_cmap: int = 0) -> "DeviceGraph":
+        """The coarse graph of the device matching at d_match (mm_graph_contract)."""
+        h = ctypes.c_void_p()
+        _check(self._lib.mm_graph_contract(self.handle, d_match, ctypes.byref(h), d_cmap or None))
+        return DeviceGraph.adopt(h.value, self._lib)
+
+    @classmethod
+    def adopt(cls, handle: int, library=None) -> "DeviceGraph":
+        """Wrap a graph the library created (it is destroyed with this object)."""
+        obj = cls.__new__(cls)
+        obj._lib = library or lib()
+        obj.handle = handle
+        obj.n = int(obj._lib.mm_graph_n(handle))
+        obj.nnz = int(obj._lib.mm_graph_nnz(handle))
+        return obj
+
+    def to_host(self):
+        """(ranges int32[n, 2], neighbours int32[nnz], weights float32[nnz]) copied to the host."""
+        r = np.empty((max(self.n, 1), 2), dtype=np.int32)
+        nb = np.empty(max(self.nnz, 1), dtype=np.int32)
+        w = np.empty(max(self.nnz, 1), dtype=np.float32)
+        _check(self._lib.mm_graph_copy_out(self.handle, _ptr(r), _ptr(nb), _ptr(w)))
+        return r[: self.n], nb[: self.nnz], w[: self.nnz]
+
     def weight(self, d_match: int, stream: int = 0):
         """(weight, size) of the device matching at d_match, as getWeight computes them."""
         wt = ctypes.c_double(0.0)
@@ -320,6 +346,48 @@ class DeviceGraph:
                                           stream or None))
         executed = int(np.count_nonzero(ms[:, 3] > 0))
         return rounds.value, ms[:executed], launches.value
+
+
+def multilevel(g, type_: int, seeds: np.ndarray, target: float = 0.01, device: int = 0,
+               barrier: int = DEFAULT_BARRIER, max_levels: int = 64) -> list:
+    """Multilevel coarsening: match (type_), contract, repeat until at most
+    target * n vertices remain (or a level matches nothing).  Returns one dict per
+    level: n, nnz, and for every level but the last rounds, matched vertices,
+    weight, valid, maximal, ms_match (device time of the matching) and
+    ms_contract."""
+    import torch
+
+    levels = []
+    dg = DeviceGraph(g, device=device)
+    n0 = g.n
+    try:
+        while True:
+            info = {"n": dg.n, "nnz": dg.nnz}
+            if dg.n <= target * n0 or len(levels) >= max_levels:
+                levels.append(info)
+                break
+            out = torch.empty(max(dg.n, 1), dtype=torch.int32, device="cuda")
+            a, b, c = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            a.record()
+            rounds = dg.match_device(type_, seeds, out.data_ptr(), barrier)
+            b.record()
+            coarse = dg.contract(out.data_ptr())
+            c.record()
+            torch.cuda.synchronize()
+            chk = dg.check(out.data_ptr())
+            wt, sz = dg.weight(out.data_ptr())
+            info.update(rounds=rounds, matched=sz, weight=wt, valid=chk["valid"], maximal=chk["matchable"] == 0,
+                        ms_match=a.elapsed_time(b), ms_contract=b.elapsed_time(c))
+            levels.append(info)
+            stuck = coarse.n == dg.n
+            dg.close()
+            dg = coarse
+            if stuck:
+                levels.append({"n": dg.n, "nnz": dg.nnz})
+                break
+    finally:
+        dg.close()
+    return levels
 
 
 def probe_gather_rate(device: int = 0, table_bytes: int = 8 << 20) -> float:

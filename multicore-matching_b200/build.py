@@ -29,7 +29,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fvisibility=hidden", f"-I{INCLUDE}",
              "-I/usr/local/cuda/include"]
 
-CUDA_SOURCES = ["mm_capi.cu", "mm_pull.cu", "mm_push.cu", "mm_noalloc.cu", "mm_check.cu"]
+CUDA_SOURCES = ["mm_capi.cu", "mm_pull.cu", "mm_push.cu", "mm_noalloc.cu", "mm_check.cu", "mm_contract.cu"]
 MTC_SOURCES = ["mtc_graph.cpp", "mtc_matching.cpp", "mtc_gpu.cpp"]
 
 

@@ -562,6 +562,27 @@ MM_API mm_status mm_graph_create_device(int n, const int *d_ranges, long long nn
     return create_common(n, d_ranges, nnz, d_neighbours, d_weights, -1, true, out);
 }
 
+MM_API mm_status mm_graph_copy_out(const mm_graph *g, int *ranges, int *neighbours, float *weights)
+{
+    if (!g) {
+        set_error("mm_graph_copy_out: null graph");
+        return MM_ERR_ARG;
+    }
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != g->device) MM_CUDA_TRY(cudaSetDevice(g->device), "set device");
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess && ranges && g->n > 0)
+        e = cudaMemcpy(ranges, g->d_ranges, sizeof(int2) * (size_t)g->n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && neighbours && g->nnz > 0)
+        e = cudaMemcpy(neighbours, g->d_nbrs, sizeof(int) * (size_t)g->nnz, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && weights && g->nnz > 0)
+        e = cudaMemcpy(weights, g->d_w, sizeof(float) * (size_t)g->nnz, cudaMemcpyDeviceToHost);
+    if (prev >= 0 && prev != g->device) cudaSetDevice(prev);
+    if (e != cudaSuccess) return cuda_fail(e, "mm_graph_copy_out");
+    return MM_OK;
+}
+
 MM_API mm_status mm_graph_prepare(mm_graph *g, int type)
 {
     if (!g || max_rounds_of(type) < 0) {
