@@ -199,6 +199,22 @@ mm_status mm_match_noalloc(int n, const int *d_ranges, long long nnz, const int 
                            int nseeds, int *d_match_out, int *rounds_out, void *stream);
 
 /*
+ * Batches of independent graphs, matched in one launch; no counterpart in the
+ * reference, whose matcher takes one graph per call.  g holds the disjoint
+ * union: graph i owns vertices [offsets[i], offsets[i + 1]) (ngraphs + 1 host
+ * ints from 0 to n) and no entry may join two graphs (MM_ERR_GRAPH).  Each
+ * graph is coloured and numbered in its own ids (v - offsets[i]), so its
+ * slice of the result, and its round count, are exactly what a matching of
+ * that graph alone with the same seeds would give.  mm_match_batch writes
+ * d_match_out (n ints on the device, values in each graph's own numbering)
+ * and rounds_out[i] per graph (host, ngraphs ints).  After set_batch, the
+ * other match entries also number per graph and report the largest count.
+ */
+mm_status mm_graph_set_batch(mm_graph *g, int ngraphs, const int *offsets);
+mm_status mm_match_batch(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds,
+                         int *d_match_out, int *rounds_out, void *stream);
+
+/*
  * Weight and size of a matching, computed on the device exactly as
  * GraphMatching::getWeight does (src/matchcpu.cu:64-97): a matched vertex adds
  * the weight of the first entry of its list whose neighbour carries the same

@@ -87,6 +87,8 @@ _MM_SIGS = {
     "mm_matching_check": (_I, [_P, _P, _P, ctypes.POINTER(_I), _P]),
     "mm_graph_contract": (_I, [_P, _P, ctypes.POINTER(_P), _P]),
     "mm_graph_copy_out": (_I, [_P, _P, _P, _P]),
+    "mm_graph_set_batch": (_I, [_P, _I, _P]),
+    "mm_match_batch": (_I, [_P, _I, _U, _P, _I, _P, _P, _P]),
     "mm_probe_gather_rate": (_I, [_I, _LL, ctypes.POINTER(ctypes.c_double)]),
     "mm_match_profile": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P, _I, ctypes.POINTER(_I), _P]),
     "mm_match_noalloc": (_I, [_I, _P, _LL, _P, _P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P]),
@@ -213,6 +215,48 @@ class Graph:
     def er(n: int, avg_deg: float = 8.0, seed: int = 1, unit: bool = False) -> "Graph":
         return Graph.from_generated(genlib().mmg_er(n, avg_deg, seed, int(unit)), f"er{n}")
 
+    def with_pair_weights(self, seed: int = 1) -> "Graph":
+        """The same lists with weights in (0, 1] from a hash of the unordered
+        endpoint pair, so both entries of an edge carry the same weight."""
+        deg = self.degrees()
+        owner = np.repeat(np.arange(self.n, dtype=np.uint64), deg)
+        r = np.asarray(self.ranges, dtype=np.int64).reshape(-1, 2)
+        if self.n and r[0, 0] == 0 and (r[1:, 0] == r[:-1, 1]).all() and r[-1, 1] == self.nnz:
+            pos = np.arange(self.nnz, dtype=np.int64)  # contiguous lists
+        else:
+            pos = np.concatenate([np.arange(b, b + d) for (b, _), d in zip(r, deg)]) if self.n else []
+            pos = np.asarray(pos, dtype=np.int64)
+        other = self.nbrs[pos].astype(np.uint64)
+        lo, hi = np.minimum(owner, other), np.maximum(owner, other)
+        x = ((lo << np.uint64(32)) | hi) ^ np.uint64((0x9E3779B97F4A7C15 * (seed + 1)) & 0xFFFFFFFFFFFFFFFF)
+        with np.errstate(over="ignore"):
+            x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+            x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+            x ^= x >> np.uint64(31)
+        w = np.zeros(self.nnz, dtype=np.float32)
+        w[pos] = ((x >> np.uint64(40)).astype(np.float64) + 1.0) / 16777216.0
+        return Graph(self.n, self.ranges, self.nbrs, w, self.name)
+
+    @staticmethod
+    def union(graphs) -> tuple:
+        """Disjoint union of graphs (vertex and entry ids shifted), and the vertex
+        offsets of each graph: the input of mm_graph_set_batch."""
+        ns = np.array([g.n for g in graphs], dtype=np.int64)
+        ms = np.array([g.nnz for g in graphs], dtype=np.int64)
+        voff = np.concatenate([[0], np.cumsum(ns)])
+        eoff = np.concatenate([[0], np.cumsum(ms)])
+        if voff[-1] >= (1 << 31) or eoff[-1] >= (1 << 31):
+            raise ValueError("the union exceeds int32 vertex or entry ids")
+        ranges = np.empty((int(voff[-1]), 2), dtype=np.int32)
+        nbrs = np.empty(int(eoff[-1]), dtype=np.int32)
+        weights = np.empty(int(eoff[-1]), dtype=np.float32)
+        for g, v0, e0 in zip(graphs, voff[:-1], eoff[:-1]):
+            r = np.asarray(g.ranges, dtype=np.int64).reshape(-1, 2)
+            ranges[v0:v0 + g.n] = r + e0
+            nbrs[e0:e0 + g.nnz] = np.asarray(g.nbrs, dtype=np.int64) + v0
+            weights[e0:e0 + g.nnz] = 1.0 if g.weights is None else g.weights
+        return Graph(int(voff[-1]), ranges, nbrs, weights, f"union{len(graphs)}"), voff.astype(np.int32)
+
 
 def rand_seeds(seed: int, count: int = 255) -> np.ndarray:
     """The host rand() values the reference draws per round after srand(seed)
@@ -314,6 +358,21 @@ class DeviceGraph:
         w = np.empty(max(self.nnz, 1), dtype=np.float32)
         _check(self._lib.mm_graph_copy_out(self.handle, _ptr(r), _ptr(nb), _ptr(w)))
         return r[: self.n], nb[: self.nnz], w[: self.nnz]
+
+    def set_batch(self, offsets: np.ndarray) -> None:
+        """Mark the graph as a disjoint union of independent graphs (mm_graph_set_batch)."""
+        offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+        _check(self._lib.mm_graph_set_batch(self.handle, len(offsets) - 1, _ptr(offsets)))
+        self.ngraphs = len(offsets) - 1
+
+    def match_batch(self, type_: int, seeds: np.ndarray, d_out: int, barrier: int = DEFAULT_BARRIER,
+                    stream: int = 0) -> np.ndarray:
+        """One launch matching every graph of the batch; returns each graph's rounds."""
+        seeds = np.ascontiguousarray(seeds, dtype=np.uint32)
+        rounds = np.zeros(self.ngraphs, dtype=np.int32)
+        _check(self._lib.mm_match_batch(self.handle, type_, barrier, _ptr(seeds), len(seeds), d_out, _ptr(rounds),
+                                        stream or None))
+        return rounds
 
     def weight(self, d_match: int, stream: int = 0):
         """(weight, size) of the device matching at d_match, as getWeight computes them."""

@@ -322,6 +322,9 @@ void free_graph(mm_graph *g)
     dev_free(g->d_w, 0);
     cudaFree(g->scratch);
     dev_free(g->d_out, 0);
+    dev_free(g->d_goff, 0);
+    dev_free(g->d_vbase, 0);
+    dev_free(g->d_last, 0);
     cudaStreamSynchronize(0);
     if (prev >= 0) cudaSetDevice(prev);
     delete g;
@@ -514,6 +517,32 @@ mm_status check_match_args(mm_graph *g, int type, const uint32_t *seeds, int nse
     return MM_OK;
 }
 
+// ---- batches of independent graphs ----
+// vbase[v] = first vertex of v's graph (a warp per graph), then every entry
+// must stay inside its vertex's graph: the union is disjoint.
+__global__ void k_batch_vbase(const int *goff, int ngraphs, int *vbase)
+{
+    const int lane = threadIdx.x & 31;
+    const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long gi = gwarp; gi < ngraphs; gi += nwarps)
+        for (int v = goff[gi] + lane; v < goff[gi + 1]; v += 32) vbase[v] = goff[gi];
+}
+
+__global__ void k_batch_edges(const int2 *ranges, const int *nbrs, const int *vbase, int n, int *bad)
+{
+    const int lane = threadIdx.x & 31;
+    const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long v = warp0; v < n; v += nwarps) {
+        const int2 r = ranges[v];
+        const int b = vbase[v];
+        int cross = 0;
+        for (int j = r.x + lane; j < r.y; j += 32) cross |= vbase[nbrs[j]] != b;
+        if (__any_sync(0xffffffffu, cross) && lane == 0) atomicOr(bad, 1);
+    }
+}
+
 // ---- measurement: random-gather ceiling ----
 //
 // The round kernel's scans are bound by random single-sector reads (colour
@@ -613,8 +642,13 @@ MM_API mm_status mm_match_ex(mm_graph *g, int type, uint32_t barrier, const uint
     if (s != MM_OK) return s;
     DeviceGuard guard(g->device);
     cudaStream_t st = (cudaStream_t)stream;
-    if (path == MM_PATH_PULL)
+    if (path == MM_PATH_PULL) {
+        if (g->ngraphs > 0) {
+            set_error("mm_match_ex: the reference-structured path matches single graphs only");
+            return MM_ERR_UNSUPPORTED;
+        }
         return pull_match(g, type, barrier, seeds, nseeds, d_match_out, rounds_out, nullptr, 0, st);
+    }
     if (path == MM_PATH_AUTO || path == MM_PATH_PUSH)
         return push_match(g, type, barrier, seeds, nseeds, d_match_out, rounds_out, nullptr, 0, st);
     set_error("mm_match_ex: unknown path");
@@ -658,9 +692,14 @@ MM_API mm_status mm_match_stats(mm_graph *g, int type, uint32_t barrier, const u
         return MM_ERR_ARG;
     }
     DeviceGuard guard(g->device);
-    if (path == MM_PATH_PULL)
+    if (path == MM_PATH_PULL) {
+        if (g->ngraphs > 0) {
+            set_error("mm_match_stats: the reference-structured path matches single graphs only");
+            return MM_ERR_UNSUPPORTED;
+        }
         return pull_match(g, type, barrier, seeds, nseeds, d_match_out, rounds_out, stats, stats_rounds,
                           (cudaStream_t)stream);
+    }
     return push_match(g, type, barrier, seeds, nseeds, d_match_out, rounds_out, stats, stats_rounds,
                       (cudaStream_t)stream);
 }
@@ -674,6 +713,78 @@ MM_API mm_status mm_match_profile(mm_graph *g, int type, uint32_t barrier, const
     DeviceGuard guard(g->device);
     return push_profile(g, type, barrier, seeds, nseeds, d_match_out, rounds_out, ms_per_kernel, cap_rounds, launches,
                         (cudaStream_t)stream);
+}
+
+MM_API mm_status mm_graph_set_batch(mm_graph *g, int ngraphs, const int *offsets)
+{
+    if (!g || ngraphs < 1 || !offsets) {
+        set_error("mm_graph_set_batch: bad argument");
+        return MM_ERR_ARG;
+    }
+    if (offsets[0] != 0 || offsets[ngraphs] != g->n) {
+        set_error("mm_graph_set_batch: offsets must run from 0 to n");
+        return MM_ERR_ARG;
+    }
+    for (int i = 0; i < ngraphs; ++i)
+        if (offsets[i + 1] < offsets[i]) {
+            set_error("mm_graph_set_batch: offsets must not decrease");
+            return MM_ERR_ARG;
+        }
+    DeviceGuard guard(g->device);
+    int *goff = nullptr, *vbase = nullptr, *bad = nullptr;
+    uint8_t *last = nullptr;
+    const size_t nv = (size_t)(g->n > 0 ? g->n : 1);
+    cudaError_t e = dev_alloc((void **)&goff, sizeof(int) * ((size_t)ngraphs + 1), 0);
+    if (e == cudaSuccess) e = dev_alloc((void **)&vbase, sizeof(int) * nv, 0);
+    if (e == cudaSuccess) e = dev_alloc((void **)&last, nv, 0);
+    if (e == cudaSuccess) e = dev_alloc((void **)&bad, sizeof(int), 0);
+    if (e == cudaSuccess) e = cudaMemsetAsync(bad, 0, sizeof(int), 0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(goff, offsets, sizeof(int) * ((size_t)ngraphs + 1), cudaMemcpyHostToDevice, 0);
+    if (e == cudaSuccess) {
+        k_batch_vbase<<<grid_for((long long)ngraphs * 32, 256, 148 * 8), 256>>>(goff, ngraphs, vbase);
+        if (g->n > 0)
+            k_batch_edges<<<grid_for((long long)g->n * 32, 256, 148 * 16), 256>>>(g->d_ranges, g->d_nbrs, vbase, g->n,
+                                                                                bad);
+        e = cudaGetLastError();
+    }
+    int hbad = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost);
+    dev_free(bad, 0);
+    if (e != cudaSuccess || hbad) {
+        dev_free(goff, 0);
+        dev_free(vbase, 0);
+        dev_free(last, 0);
+        cudaStreamSynchronize(0);
+        if (e != cudaSuccess) return cuda_fail(e, "mm_graph_set_batch");
+        set_error("mm_graph_set_batch: an edge joins two graphs of the batch");
+        return MM_ERR_GRAPH;
+    }
+    dev_free(g->d_goff, 0);
+    dev_free(g->d_vbase, 0);
+    dev_free(g->d_last, 0);
+    g->d_goff = goff;
+    g->d_vbase = vbase;
+    g->d_last = last;
+    g->ngraphs = ngraphs;
+    MM_CUDA_TRY(cudaStreamSynchronize(0), "mm_graph_set_batch");
+    return MM_OK;
+}
+
+MM_API mm_status mm_match_batch(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds,
+                                int *d_match_out, int *rounds_out, void *stream)
+{
+    if (g && g->ngraphs < 1) {
+        set_error("mm_match_batch: the graph is not a batch (mm_graph_set_batch)");
+        return MM_ERR_ARG;
+    }
+    int overall = 0;
+    mm_status s = check_match_args(g, type, seeds, nseeds, d_match_out, rounds_out ? &overall : nullptr);
+    if (s != MM_OK) return s;
+    DeviceGuard guard(g->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    s = push_match(g, type, barrier, seeds, nseeds, d_match_out, &overall, nullptr, 0, st);
+    if (s == MM_OK) s = push_batch_rounds(g, type, rounds_out, st);
+    return s;
 }
 
 MM_API const char *mm_last_error(void) { return g_last_error.c_str(); }

@@ -107,8 +107,16 @@ struct mm_graph {
     int2 *win_build = nullptr;        // windows while being built (d_pwin once complete)
     int *win_big = nullptr;           // while being built: queued lists longer than a window chunk
 
-    // push path: captured CUDA graph of the round loop
-    void *push_exec = nullptr;  // internal (mm::PushPlan *)
+    // push path: per-call state of the round kernel
+    void *push_exec = nullptr;  // internal (mm::PushState *)
+
+    // a batch of independent graphs (mm_graph_set_batch): graph i holds
+    // vertices [goff[i], goff[i + 1]); vbase[v] = goff of v's graph; last[v]
+    // = last round at whose colouring v was unmatched
+    int ngraphs = 0;
+    int *d_goff = nullptr;
+    int *d_vbase = nullptr;
+    uint8_t *d_last = nullptr;
 };
 
 namespace mm {
@@ -145,6 +153,7 @@ mm_status push_match(mm_graph *g, int type, uint32_t barrier, const uint32_t *se
 mm_status push_profile(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds, int *d_match,
                        int *rounds_out, float *ms_kernels, int cap_rounds, int *launched, cudaStream_t stream);
 void push_release(mm_graph *g);
+mm_status push_batch_rounds(mm_graph *g, int type, int *rounds_host, cudaStream_t stream);
 // Preference windows of the weighted types, in steps (see mm_push.cu).
 mm_status windows_begin(mm_graph *g, cudaStream_t stream);
 mm_status windows_range(mm_graph *g, int va, int vb, cudaStream_t stream);

@@ -111,7 +111,16 @@ struct Params {
     unsigned long long *stats;      // [kMaxRounds][MM_STATS_COLS] or null
     unsigned long long *tstamp;     // [3 * kMaxRounds + 1] barrier times (ns) or null
     unsigned *bar;                  // [kBarWords] grid barrier words, zero at launch
+    // A batch of independent graphs (a disjoint union, edges never cross): each
+    // vertex's graph starts at vbase[v], and the graph's own numbering (v -
+    // vbase[v]) drives the colouring and the match values, so every graph gets
+    // the matching a call on it alone would give.  last[v] is the last round
+    // at whose colouring v was still unmatched.  Both null for one graph.
+    const int *vbase;
+    uint8_t *last;
 };
+
+__device__ __forceinline__ int base_of(const Params &p, int v) { return p.vbase ? __ldg(p.vbase + v) : 0; }
 
 __device__ __forceinline__ int degree_of(int2 r) { return r.y > r.x ? r.y - r.x : 0; }
 __device__ __forceinline__ int degree_of(int4 it) { return it.z > it.y ? it.z - it.y : 0; }
@@ -417,7 +426,8 @@ __device__ void init_phase(const Params &p, Smem &sm)
                 item[k].z = r.y;
                 if (kW) item[k].w = (int)__ldg(p.pwin_off + v);
                 const int deg = degree_of(r);
-                const bool blue = colour_of((uint32_t)v, seed, barrier) == kBlue;
+                const bool blue = colour_of((uint32_t)(v - base_of(p, v)), seed, barrier) == kBlue;
+                if (p.last) p.last[v] = 0;
                 p.best[v] = 0ull;
                 if (deg > kWin) {
                     p.part_key[v] = 0ull;
@@ -862,7 +872,7 @@ __device__ void commit_phase(const Params &p, Smem &sm, int t, bool has_next)
                 seen += first >= 0 ? (unsigned long long)(first - it[k].y + 1) : (unsigned long long)deg;
             }
             if (partner[k] >= 0) {
-                match[v] = 4 + min(v, partner[k]);
+                match[v] = 4 + min(v, partner[k]) - base_of(p, v);
                 p.col[v] = kMatched;
                 ++matched;
                 continue;
@@ -873,7 +883,8 @@ __device__ void commit_phase(const Params &p, Smem &sm, int t, bool has_next)
                 dest[k] = blue[k] ? kBlue : kRed;
                 continue;
             }
-            const bool nb = colour_of((uint32_t)v, next_seed, barrier) == kBlue;
+            const bool nb = colour_of((uint32_t)(v - base_of(p, v)), next_seed, barrier) == kBlue;
+            if (p.last) p.last[v] = (uint8_t)(t + 1);
             ++act;
             nblue += nb;
             if (nb && deg == 0) {  // no neighbours: unmatchable as soon as it is blue
@@ -1411,6 +1422,24 @@ int bits_for(long long n)
     return b;
 }
 
+// Rounds of each graph of a batch: the reference's loop for a graph runs
+// until a round finds none of its vertices unmatched at the colouring, so it
+// executes its last active round and one more (at most the cap; an empty
+// graph runs one round).  A warp per graph takes the max of last[].
+__global__ void k_batch_rounds(const uint8_t *last, const int *goff, int ngraphs, int cap, int fixed, int *rounds)
+{
+    const int lane = threadIdx.x & 31;
+    const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long gi = gwarp; gi < ngraphs; gi += nwarps) {
+        int mx = -1;
+        for (int v = goff[gi] + lane; v < goff[gi + 1]; v += 32) mx = max(mx, (int)last[v]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(kFull, mx, o));
+        if (lane == 0) rounds[gi] = fixed ? cap : min(mx + 2, cap);
+    }
+}
+
 // Control block rounded to 256 bytes so the seeds that follow it stay aligned.
 constexpr size_t kCtlBytes = (sizeof(Ctl) + 255) / 256 * 256;
 constexpr int kStampCount = 3 * kMaxRounds + 1;
@@ -1557,6 +1586,8 @@ Params make_params(mm_graph *g, PushState *s, bool weighted, bool stats, bool ti
         for (int l = 0; l < kParityLists; ++l) p.lists[par][l] = s->lists[par][l];
     p.staged = s->staged;
     p.seg_first = s->seg_first;
+    p.vbase = g->ngraphs > 0 ? g->d_vbase : nullptr;
+    p.last = g->ngraphs > 0 ? g->d_last : nullptr;
     p.seeds = s->seeds;
     p.ctl = s->ctl;
     p.stats = stats ? s->stats : nullptr;
@@ -2010,6 +2041,21 @@ mm_status push_profile(mm_graph *g, int type, uint32_t barrier, const uint32_t *
         }
     }
     if (launched) *launched = 1;
+    return MM_OK;
+}
+
+// Per-graph round counts of the last matching of a batch (after push_match).
+mm_status push_batch_rounds(mm_graph *g, int type, int *rounds_host, cudaStream_t stream)
+{
+    int *d = nullptr;
+    MM_CUDA_TRY(dev_alloc((void **)&d, sizeof(int) * (size_t)g->ngraphs, stream), "batch rounds");
+    k_batch_rounds<<<grid_for((long long)g->ngraphs * 32, 256, 148 * 8), 256, 0, stream>>>(
+        g->d_last, g->d_goff, g->ngraphs, max_rounds_of(type), is_maximal(type) ? 0 : 1, d);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(rounds_host, d, sizeof(int) * (size_t)g->ngraphs, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    dev_free(d, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "batch rounds");
     return MM_OK;
 }
 
