@@ -61,10 +61,43 @@ WORKLOADS = {
     "rgg20_weighted_maximal": dict(kind="rgg", n=1 << 20, deg=13.0, seed=7, type=9),
     "grid512_random_maximal": dict(kind="grid", w=512, h=512, type=7),
     "rmat20_weighted_maximal": dict(kind="rmat", scale=20, ef=16, seed=1, type=9),
+    "batch4096_weighted_maximal": dict(kind="batch", count=4096, seed=3, type=9),
 }
+BATCH_SAMPLE = 48  # graphs of a batch the CPU baseline and the parity check run
+
+
+def make_batch(mm, count, seed):
+    """Independent graphs, vertex counts log-uniform in [2^10, 2^18], each a 2D grid,
+    a random geometric graph (average degree 13) or an Erdos-Renyi graph (average
+    degree 8), weights in (0, 1] from a hash of the endpoint pair; their disjoint
+    union, its offsets, and an evenly spaced sample of (index, graph)."""
+    rng = np.random.default_rng(seed)
+    graphs = []
+    for i in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(1 << 10), np.log(1 << 18)))))
+        kind = int(rng.integers(3))
+        gs = seed * 100003 + i
+        if kind == 0:
+            wd = int(np.sqrt(n))
+            graphs.append(mm.Graph.grid(wd, max(1, n // wd)).with_pair_weights(gs))
+        elif kind == 1:
+            graphs.append(mm.Graph.rgg(n, 13.0, seed=gs))
+        else:
+            graphs.append(mm.Graph.er(n, 8.0, seed=gs))
+    u, off = mm.Graph.union(graphs)
+    pick = np.linspace(0, count - 1, min(BATCH_SAMPLE, count)).astype(int)
+    sample = [(int(i), graphs[int(i)]) for i in pick]
+    return u, {"offsets": off, "sample": sample, "count": count}
 
 
 def make_graph(mm, spec):
+    """(graph, batch): batch is None, or the offsets and sample of a batch workload."""
+    if spec["kind"] == "batch":
+        return make_batch(mm, spec["count"], spec["seed"])
+    return make_single(mm, spec), None
+
+
+def make_single(mm, spec):
     if spec["kind"] == "rmat":
         return mm.Graph.rmat(spec["scale"], spec["ef"], 0.57, 0.19, 0.19, seed=spec["seed"])
     if spec["kind"] == "rgg":
@@ -151,28 +184,35 @@ def run_reference(args, spec, workload):
     mm = load_package()
     import oracle  # the CPU baseline leg is the one place bench.py runs oracle/
 
-    g = make_graph(mm, spec)
+    g, batch = make_graph(mm, spec)
     t = spec["type"]
     ref_type = {6: 10, 7: 10, 8: 11, 9: 11}[t]
     fixed = t in (6, 8)
     cores = os.cpu_count() or 1
     seeds = oracle.rand_seeds(MATCH_SEED, 256)
     kind = "reference" if oracle.ref_available() else "port"
-    times, edges = [], None
-    _, _, ost = oracle.match(g, t, seeds, BARRIER, nthreads=cores)
-    edges = float(ost[:, oracle.ST_REQ_ENTRIES].sum() + ost[:, oracle.ST_RESP_ENTRIES].sum())
+    # a batch is timed on its sample of graphs, one reference call per graph
+    work = [g] if batch is None else [x for _, x in batch["sample"]]
+    edges = 0.0
+    for x in work:
+        _, _, ost = oracle.match(x, t, seeds, BARRIER, nthreads=cores)
+        edges += float(ost[:, oracle.ST_REQ_ENTRIES].sum() + ost[:, oracle.ST_RESP_ENTRIES].sum())
+    times = []
     for i in range(args.warmup + args.steps):
-        if kind == "reference":
-            _, ms, _ = oracle.ref_run(g, ref_type, BARRIER, MATCH_SEED, nthreads=cores, fixed_rounds=fixed)
-        else:
-            t0 = time.perf_counter()
-            oracle.match(g, t, seeds, BARRIER, nthreads=cores)
-            ms = (time.perf_counter() - t0) * 1e3
+        ms = 0.0
+        for x in work:
+            if kind == "reference":
+                ms += oracle.ref_run(x, ref_type, BARRIER, MATCH_SEED, nthreads=cores, fixed_rounds=fixed)[1]
+            else:
+                t0 = time.perf_counter()
+                oracle.match(x, t, seeds, BARRIER, nthreads=cores)
+                ms += (time.perf_counter() - t0) * 1e3
         if i >= args.warmup:
             times.append(ms)
     ms = statistics.mean(times)
     value = edges / (ms / 1e3)
-    sample = f"full {workload} graph, one maximal matching per step"
+    sample = (f"full {workload} graph, one maximal matching per step" if batch is None else
+              f"{len(work)} of the batch's {batch['count']} graphs (evenly spaced), one reference call each per step")
     line = {"metric": METRIC, "value": value, "unit": "edges/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+int32", "data": "synthetic",
@@ -186,34 +226,51 @@ def run_reference(args, spec, workload):
     return 0
 
 
-def cpu_baseline(mm, g, t, gpu_match, workload):
-    """Reference TBB matcher on all host cores + parity of the GPU result (rank 0, N=1 only)."""
+def cpu_baseline(mm, g, t, gpu_match, workload, batch=None):
+    """Reference TBB matcher on all host cores + parity of the GPU result (rank 0, N=1 only).
+
+    For a batch: the reference runs each graph of the batch's sample on its own,
+    and the GPU's slice of each is compared with it."""
     import oracle  # the CPU baseline leg is the one place bench.py runs oracle/
 
     cores = os.cpu_count() or 1
     ref_type = {6: 10, 7: 10, 8: 11, 9: 11}[t]
     fixed = t in (6, 8)
-    if oracle.ref_available():
-        kind = "reference"
-        ref_m, ms, _ = oracle.ref_run(g, ref_type, BARRIER, MATCH_SEED, nthreads=cores, fixed_rounds=fixed)
+    seeds = oracle.rand_seeds(MATCH_SEED, 256)
+    kind = "reference" if oracle.ref_available() else "port"
+    if batch is None:
+        items = [(g, gpu_match)]
     else:
-        kind = "port"
-        seeds = oracle.rand_seeds(MATCH_SEED, 256)
-        t0 = time.perf_counter()
-        ref_m, _, _ = oracle.match(g, t, seeds, BARRIER, nthreads=cores)
-        ms = (time.perf_counter() - t0) * 1e3
+        off = batch["offsets"]
+        items = [(x, gpu_match[off[i]:off[i + 1]]) for i, x in batch["sample"]]
+    ms_total, edges, parity, valid, maximal, w_gpu, s_gpu = 0.0, 0.0, True, True, True, 0.0, 0
+    for x, got in items:
+        _, _, ost = oracle.match(x, t, seeds, BARRIER, nthreads=cores)
+        edges += float(ost[:, oracle.ST_REQ_ENTRIES].sum() + ost[:, oracle.ST_RESP_ENTRIES].sum())
+        if kind == "reference":
+            ref_m, ms, _ = oracle.ref_run(x, ref_type, BARRIER, MATCH_SEED, nthreads=cores, fixed_rounds=fixed)
+        else:
+            t0 = time.perf_counter()
+            ref_m, _, _ = oracle.match(x, t, seeds, BARRIER, nthreads=cores)
+            ms = (time.perf_counter() - t0) * 1e3
+        ms_total += ms
+        parity &= bool(np.array_equal(ref_m, got))
+        chk = oracle.check(x, got)
+        valid &= chk["valid"]
+        maximal &= chk["matchable"] == 0
+        wx, sx = oracle.weight(x, got)
+        w_gpu += wx
+        s_gpu += sx
     # sequential weighted greedy (type 4) on one core: the reference's quality yardstick
     seq = None
-    if oracle.ref_available() and t in (8, 9):
+    if oracle.ref_available() and t in (8, 9) and batch is None:
         seq_m, seq_ms, _ = oracle.ref_run(g, 4, BARRIER, MATCH_SEED, nthreads=1)
         w_seq, s_seq = oracle.weight(g, seq_m)
         seq = {"type": 4, "ms": seq_ms, "weight": w_seq, "size": s_seq}
-    parity = bool(np.array_equal(ref_m, gpu_match))
-    chk = oracle.check(g, gpu_match)
-    w_gpu, s_gpu = oracle.weight(g, gpu_match)
-    return {"kind": kind, "cores": cores, "ms": ms,
-            "sample": f"full {workload} graph, one matching", "parity": parity,
-            "valid": chk["valid"], "maximal": chk["matchable"] == 0,
+    sample = (f"full {workload} graph, one matching" if batch is None else
+              f"{len(items)} of the batch's {batch['count']} graphs (evenly spaced), one reference call each")
+    return {"kind": kind, "cores": cores, "ms": ms_total, "value": edges / (ms_total / 1e3),
+            "sample": sample, "parity": parity, "valid": valid, "maximal": maximal,
             "gpu_weight": w_gpu, "gpu_size": s_gpu, "sequential": seq}
 
 
@@ -248,12 +305,14 @@ def main():
     mm = load_package()
     t = spec["type"]
     weighted = t in (8, 9)
-    g = make_graph(mm, spec)
+    g, batch = make_graph(mm, spec)
     seeds = mm.rand_seeds(MATCH_SEED, 255)
     stream = torch.cuda.Stream()
     sptr = stream.cuda_stream
 
     dg = mm.DeviceGraph(g, device=local)
+    if batch is not None:
+        dg.set_batch(batch["offsets"])
     dg.prepare(t)
     out = torch.empty(g.n, dtype=torch.int32, device="cuda")
     if args.ncu_case:
@@ -335,6 +394,8 @@ def main():
         h = ctypes.c_void_p()
         mm._check(lib.mm_graph_create(g.n, ranges_h.data_ptr(), g.nnz, nbrs_h.data_ptr(),
                                       None if w_h is None else w_h.data_ptr(), local, ctypes.byref(h)))
+        if batch is not None:
+            mm._check(lib.mm_graph_set_batch(h, len(batch["offsets"]) - 1, batch["offsets"].ctypes.data))
         t1 = time.perf_counter()
         rr = ctypes.c_int()
         sd = np.ascontiguousarray(seeds)
@@ -353,6 +414,8 @@ def main():
     h = ctypes.c_void_p()
     mm._check(lib.mm_graph_create(g.n, ranges_h.data_ptr(), g.nnz, nbrs_h.data_ptr(),
                                   None if w_h is None else w_h.data_ptr(), local, ctypes.byref(h)))
+    if batch is not None:
+        mm._check(lib.mm_graph_set_batch(h, len(batch["offsets"]) - 1, batch["offsets"].ctypes.data))
     tp = [time.perf_counter()]
     mm._check(lib.mm_graph_prepare(h, t))
     tp.append(time.perf_counter())
@@ -371,7 +434,7 @@ def main():
         gpu_m = torch.empty(g.n, dtype=torch.int32, device="cuda")
         dg.match_device(t, seeds, gpu_m.data_ptr(), stream=sptr)
         torch.cuda.synchronize()
-        cpu = cpu_baseline(mm, g, t, gpu_m.cpu().numpy(), args.workload)
+        cpu = cpu_baseline(mm, g, t, gpu_m.cpu().numpy(), args.workload, batch)
     dg.close()
 
     if rank == 0:
@@ -380,6 +443,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+int32", "data": "synthetic",
             "config": {"workload": args.workload, "n": g.n, "nnz": g.nnz, "type": t, "barrier": BARRIER,
+                       "graphs": 1 if batch is None else batch["count"],
                        "srand": MATCH_SEED, "rounds": rounds, "parallelism": f"replicas x{world}",
                        "l2": "inputs > L2 (CSR > 1 GB) and a 512 MB L2 flush between steps"},
             "ms_to_maximal": ms, "edges_per_step": edges,
@@ -409,7 +473,7 @@ def main():
             "clocks": clocks.summary(),
         }
         if cpu is not None:
-            line["cpu_baseline"] = {"value": edges / (cpu["ms"] / 1e3), "unit": "edges/s", "cores": cpu["cores"],
+            line["cpu_baseline"] = {"value": cpu["value"], "unit": "edges/s", "cores": cpu["cores"],
                                     "kind": cpu["kind"], "sample": cpu["sample"], "ms": cpu["ms"]}
             line["parity"] = {"bit_exact_vs_reference": cpu["parity"], "valid": cpu["valid"],
                               "maximal": cpu["maximal"], "weight": cpu["gpu_weight"], "size": cpu["gpu_size"],
