@@ -215,6 +215,32 @@ mm_status mm_match_batch(mm_graph *g, int type, uint32_t barrier, const uint32_t
                          int *d_match_out, int *rounds_out, void *stream);
 
 /*
+ * Learned colouring; no counterpart in the reference, whose select kernel
+ * colours every vertex blue with the same probability (the barrier).  Here a
+ * per-vertex MLP (6 -> 16 -> 1, ReLU, sigmoid) gives each vertex its own blue
+ * probability from local features: log2(1 + degree), log2(1 + live entries:
+ * list entries whose neighbour is still unmatched, kept exact on graphs whose
+ * structure is symmetric, else the degree), max and mean weight it could
+ * pick, min(round, 32) / 32 and level / 16 (the caller's coarsening level).
+ * The probability is clamped to [1/16, 15/16], so the maximal types finish
+ * inside the round cap whatever the weights.  On symmetric graphs a vertex
+ * with no live entry leaves at its next colouring whatever its colour (the
+ * reference waits until it is coloured blue); the matching is the same as
+ * the one the same colours give without that.  mlp: MM_POLICY_FLOATS host
+ * floats, W1[16][6], b1[16], W2[16], b2.  The result is a valid matching
+ * (maximal for types 7, 9) but not the reference's: the reference's path is
+ * mm_match.  d_trace (device, trace_rounds * n * 8 floats, or NULL) receives
+ * for every vertex coloured in round r < trace_rounds, at [(r * n + v) * 8]:
+ * its 6 features, its colour (1 blue, 0 red) and 1 if it left the active set
+ * in that round (matched, or retired as unmatchable: match value 2); entries
+ * of vertices not coloured keep their contents.
+ */
+#define MM_POLICY_FLOATS 129
+mm_status mm_match_policy(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds,
+                          const float *mlp, float level, int *d_match_out, int *rounds_out, float *d_trace,
+                          int trace_rounds, void *stream);
+
+/*
  * Weight and size of a matching, computed on the device exactly as
  * GraphMatching::getWeight does (src/matchcpu.cu:64-97): a matched vertex adds
  * the weight of the first entry of its list whose neighbour carries the same

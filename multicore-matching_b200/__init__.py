@@ -37,6 +37,7 @@ PATH_AUTO, PATH_PULL, PATH_PUSH = 0, 1, 2
 DEFAULT_BARRIER = 0x88B81733
 
 STATS_COLS = 11
+POLICY_FLOATS = 129  # MM_POLICY_FLOATS: W1[16][6], b1[16], W2[16], b2
 PROFILE_KERNELS = 4  # window scan, fallback scan, commit/recolour, their sum
 (ST_ACTIVE, ST_BLUE, ST_RED, ST_REQ_ENTRIES, ST_RESP_ENTRIES, ST_BLUE_DEG, ST_RED_DEG, ST_MATCHED,
  ST_STAGED_DEG, ST_STAGED_ITEMS, ST_WINDOW_ENTRIES) = range(11)
@@ -89,6 +90,7 @@ _MM_SIGS = {
     "mm_graph_copy_out": (_I, [_P, _P, _P, _P]),
     "mm_graph_set_batch": (_I, [_P, _I, _P]),
     "mm_match_batch": (_I, [_P, _I, _U, _P, _I, _P, _P, _P]),
+    "mm_match_policy": (_I, [_P, _I, _U, _P, _I, _P, ctypes.c_float, _P, ctypes.POINTER(_I), _P, _I, _P]),
     "mm_probe_gather_rate": (_I, [_I, _LL, ctypes.POINTER(ctypes.c_double)]),
     "mm_match_profile": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P, _I, ctypes.POINTER(_I), _P]),
     "mm_match_noalloc": (_I, [_I, _P, _LL, _P, _P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P]),
@@ -373,6 +375,19 @@ class DeviceGraph:
         _check(self._lib.mm_match_batch(self.handle, type_, barrier, _ptr(seeds), len(seeds), d_out, _ptr(rounds),
                                         stream or None))
         return rounds
+
+    def match_policy(self, type_: int, seeds: np.ndarray, d_out: int, mlp: np.ndarray, level: float = 0.0,
+                     d_trace: int = 0, trace_rounds: int = 0, barrier: int = DEFAULT_BARRIER, stream: int = 0) -> int:
+        """Matching with the learned colouring (mm_match_policy); returns rounds."""
+        seeds = np.ascontiguousarray(seeds, dtype=np.uint32)
+        mlp = np.ascontiguousarray(mlp, dtype=np.float32)
+        if mlp.shape != (POLICY_FLOATS,):
+            raise ValueError(f"policy weights must be {POLICY_FLOATS} floats")
+        rounds = ctypes.c_int(0)
+        _check(self._lib.mm_match_policy(self.handle, type_, barrier, _ptr(seeds), len(seeds), _ptr(mlp),
+                                         float(level), d_out, ctypes.byref(rounds), d_trace or None, trace_rounds,
+                                         stream or None))
+        return rounds.value
 
     def weight(self, d_match: int, stream: int = 0):
         """(weight, size) of the device matching at d_match, as getWeight computes them."""

@@ -715,6 +715,25 @@ MM_API mm_status mm_match_profile(mm_graph *g, int type, uint32_t barrier, const
                         (cudaStream_t)stream);
 }
 
+MM_API mm_status mm_match_policy(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds,
+                                 const float *mlp, float level, int *d_match_out, int *rounds_out, float *d_trace,
+                                 int trace_rounds, void *stream)
+{
+    mm_status s = check_match_args(g, type, seeds, nseeds, d_match_out, rounds_out);
+    if (s != MM_OK) return s;
+    if (!mlp) {
+        set_error("mm_match_policy: no policy weights");
+        return MM_ERR_ARG;
+    }
+    if (trace_rounds < 0 || trace_rounds > mm::kMaxRounds) {
+        set_error("mm_match_policy: trace_rounds must be in [0, 255]");
+        return MM_ERR_ARG;
+    }
+    DeviceGuard guard(g->device);
+    return push_match_policy(g, type, barrier, seeds, nseeds, mlp, level, d_match_out, rounds_out, d_trace,
+                             trace_rounds, (cudaStream_t)stream);
+}
+
 MM_API mm_status mm_graph_set_batch(mm_graph *g, int ngraphs, const int *offsets)
 {
     if (!g || ngraphs < 1 || !offsets) {

@@ -154,6 +154,9 @@ mm_status push_profile(mm_graph *g, int type, uint32_t barrier, const uint32_t *
                        int *rounds_out, float *ms_kernels, int cap_rounds, int *launched, cudaStream_t stream);
 void push_release(mm_graph *g);
 mm_status push_batch_rounds(mm_graph *g, int type, int *rounds_host, cudaStream_t stream);
+mm_status push_match_policy(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds,
+                            const float *mlp_host, float level, int *d_match, int *rounds_out, float *trace,
+                            int trace_rounds, cudaStream_t stream);
 // Preference windows of the weighted types, in steps (see mm_push.cu).
 mm_status windows_begin(mm_graph *g, cudaStream_t stream);
 mm_status windows_range(mm_graph *g, int va, int vb, cudaStream_t stream);

@@ -118,6 +118,17 @@ struct Params {
     // at whose colouring v was still unmatched.  Both null for one graph.
     const int *vbase;
     uint8_t *last;
+    // Learned colouring (k_rounds<..., kPolicy>): blue iff hash < p_v * 2^32 with
+    // p_v from a per-vertex MLP over local features.  live[v] (symmetric
+    // structure only): list entries of v whose neighbour is not matched yet;
+    // wfeat[v]: (max, mean) incident weight; trace: per round and vertex, the
+    // features, colour and outcome (for training), or null.
+    const float *mlp;
+    float level;
+    int *live;
+    const float2 *wfeat;
+    float *trace;
+    int trace_rounds;
 };
 
 __device__ __forceinline__ int base_of(const Params &p, int v) { return p.vbase ? __ldg(p.vbase + v) : 0; }
@@ -348,7 +359,81 @@ struct Smem {
     LongStage stage[kWarps];
     int tile_warp[kWarps][2];             // compaction: per-warp counts, then offsets
     int tile_base[2];                     // compaction: tile bases
+    float mlp[MM_POLICY_FLOATS];          // learned colouring: the policy's weights
 };
+
+// ---- learned colouring ----
+//
+// The policy is a 6 -> 16 -> 1 MLP (ReLU, sigmoid output) evaluated per vertex
+// when it is coloured; its weights sit in shared memory, laid out as
+// W1[16][6], b1[16], W2[16], b2.  Features: log2(1 + deg), log2(1 + live
+// entries), max and mean incident weight, min(round, 32) / 32, level / 16.  The blue probability is clamped
+// to [1/16, 15/16] and compared with the colouring hash like the select
+// barrier: an unmatched edge then splits blue/red in at least 11.7% of the
+// rounds, so the maximal types finish well inside the 255-round cap whatever
+// the weights (a pair left alone survives 255 rounds with p < 1e-13).
+constexpr int kFeat = 6, kHid = 16;
+static_assert(kHid * kFeat + kHid + kHid + 1 == MM_POLICY_FLOATS, "policy layout");
+constexpr int kTraceCols = 8;  // features, colour (1 blue, 0 red), left the active set in that round
+
+// Trace: vertex v left the active set in round t (matched, or blue with no
+// unmatched neighbour and so retired).
+template <bool kPolicy>
+__device__ __forceinline__ void trace_left(const Params &p, int t, int v)
+{
+    if (kPolicy && p.trace && t < p.trace_rounds) p.trace[((size_t)t * p.n + v) * kTraceCols + kFeat + 1] = 1.0f;
+}
+
+__device__ __forceinline__ void policy_features(const Params &p, int v, int deg, int live, int t,
+                                                float (&x)[kFeat])
+{
+    const float2 wf = __ldg(p.wfeat + v);
+    x[0] = __log2f(1.0f + (float)deg);
+    x[1] = __log2f(1.0f + (float)live);
+    x[2] = wf.x;
+    x[3] = wf.y;
+    x[4] = (float)min(t, 32) * (1.0f / 32.0f);
+    x[5] = p.level * (1.0f / 16.0f);
+}
+
+__device__ __forceinline__ uint32_t policy_barrier(const float *wts, const float (&x)[kFeat])
+{
+    const float *W1 = wts, *b1 = W1 + kHid * kFeat, *W2 = b1 + kHid, *b2 = W2 + kHid;
+    float out = b2[0];
+#pragma unroll
+    for (int j = 0; j < kHid; ++j) {
+        float a = b1[j];
+#pragma unroll
+        for (int i = 0; i < kFeat; ++i) a = fmaf(W1[j * kFeat + i], x[i], a);
+        out = fmaf(W2[j], fmaxf(a, 0.0f), out);
+    }
+    float prob = 1.0f / (1.0f + __expf(-out));
+    prob = fminf(fmaxf(prob, 1.0f / 16.0f), 15.0f / 16.0f);
+    return (uint32_t)(prob * 4294967296.0f);
+}
+
+// Colour of vertex v for round t: the select barrier, or the policy's.
+template <bool kPolicy>
+__device__ __forceinline__ bool colour_blue(const Params &p, const float *wts, int v, int deg, int live, int t,
+                                            uint32_t seed, uint32_t barrier)
+{
+    uint32_t bar = barrier;
+    if (kPolicy) {
+        float x[kFeat];
+        policy_features(p, v, deg, live, t, x);
+        bar = policy_barrier(wts, x);
+        const bool blue = colour_of((uint32_t)(v - base_of(p, v)), seed, bar) == kBlue;
+        if (p.trace && t < p.trace_rounds) {
+            float *row = p.trace + ((size_t)t * p.n + v) * kTraceCols;
+#pragma unroll
+            for (int i = 0; i < kFeat; ++i) row[i] = x[i];
+            row[kFeat] = blue ? 1.0f : 0.0f;
+            row[kFeat + 1] = 0.0f;
+        }
+        return blue;
+    }
+    return colour_of((uint32_t)(v - base_of(p, v)), seed, bar) == kBlue;
+}
 
 // ---- worklist compaction for the set-up and commit passes ----
 //
@@ -404,7 +489,7 @@ __device__ __forceinline__ void compact_tile(const Params &p, Smem &sm, int pari
 // Set-up: colour every vertex with seeds[0] and fill the first worklists.
 // best[] starts at 0 and stays 0 for every vertex that is not matched: a red
 // vertex that receives a proposal is matched in the same round.
-template <bool kW, bool kStats>
+template <bool kW, bool kStats, bool kPolicy>
 __device__ void init_phase(const Params &p, Smem &sm)
 {
     const Ctl *ctl = p.ctl;
@@ -426,7 +511,8 @@ __device__ void init_phase(const Params &p, Smem &sm)
                 item[k].z = r.y;
                 if (kW) item[k].w = (int)__ldg(p.pwin_off + v);
                 const int deg = degree_of(r);
-                const bool blue = colour_of((uint32_t)(v - base_of(p, v)), seed, barrier) == kBlue;
+                if (kPolicy && p.sym) p.live[v] = deg;
+                const bool blue = colour_blue<kPolicy>(p, sm.mlp, v, deg, deg, 0, seed, barrier);
                 if (p.last) p.last[v] = 0;
                 p.best[v] = 0ull;
                 if (deg > kWin) {
@@ -435,9 +521,12 @@ __device__ void init_phase(const Params &p, Smem &sm)
                 }
                 ++act;
                 blue_n += blue;
-                if (blue && deg == 0) {  // no neighbours: unmatchable as soon as it is blue
+                // no neighbours: unmatchable as soon as it is blue (learned
+                // colouring: at once, whatever its colour)
+                if ((blue || kPolicy) && deg == 0) {
                     p.col[v] = kDead;
                     p.ctl->match[v] = 2;
+                    trace_left<kPolicy>(p, 0, v);
                 } else {
                     p.col[v] = blue ? kBlue : kRed;
                     dest[k] = blue ? kBlue : kRed;
@@ -471,7 +560,7 @@ __device__ void init_phase(const Params &p, Smem &sm)
 // per vertex and step.
 constexpr int kPerW = 2;
 
-template <bool kW, bool kStats>
+template <bool kW, bool kStats, bool kPolicy>
 __device__ void scan_window(const Params &p, int t, int par)
 {
     Ctl *ctl = p.ctl;
@@ -793,7 +882,7 @@ __device__ void scan_long(const Params &p, Smem &sm, int t, int gwarp, int nwarp
 
 // Phase B: commit proposals, recolour survivors with the next seed, compact
 // the worklists of round t+1.
-template <bool kW, bool kStats>
+template <bool kW, bool kStats, bool kPolicy>
 __device__ void commit_phase(const Params &p, Smem &sm, int t, bool has_next)
 {
     Ctl *ctl = p.ctl;
@@ -872,28 +961,53 @@ __device__ void commit_phase(const Params &p, Smem &sm, int t, bool has_next)
                 seen += first >= 0 ? (unsigned long long)(first - it[k].y + 1) : (unsigned long long)deg;
             }
             if (partner[k] >= 0) {
+                trace_left<kPolicy>(p, t, v);
                 match[v] = 4 + min(v, partner[k]) - base_of(p, v);
                 p.col[v] = kMatched;
                 ++matched;
                 continue;
             }
-            if (blue[k] && q[k].x == -1) continue;  // unmatchable (marked in phase A)
+            if (blue[k] && q[k].x == -1) {  // unmatchable (marked in phase A)
+                trace_left<kPolicy>(p, t, v);
+                continue;
+            }
             // survivor
             if (!has_next) {
                 dest[k] = blue[k] ? kBlue : kRed;
                 continue;
             }
-            const bool nb = colour_of((uint32_t)(v - base_of(p, v)), next_seed, barrier) == kBlue;
+            // learned colouring: live entries so far (matches of this round may
+            // still arrive; the count only falls, so 0 is final)
+            const int live = kPolicy && p.sym ? __ldcg(p.live + v) : deg;
+            const bool nb = colour_blue<kPolicy>(p, sm.mlp, v, deg, live, t + 1, next_seed, barrier);
             if (p.last) p.last[v] = (uint8_t)(t + 1);
             ++act;
             nblue += nb;
-            if (nb && deg == 0) {  // no neighbours: unmatchable as soon as it is blue
+            // no neighbours: unmatchable as soon as it is blue; learned
+            // colouring: as soon as no neighbour is unmatched, whatever its colour
+            if ((nb && deg == 0) || (kPolicy && live == 0)) {
                 p.col[v] = kDead;
                 match[v] = 2;
                 ++retired;
+                trace_left<kPolicy>(p, t + 1, v);
             } else {
                 p.col[v] = nb ? kBlue : kRed;
                 dest[k] = nb ? kBlue : kRed;
+            }
+        }
+        if (kPolicy && p.sym) {
+            // learned colouring: every vertex matched now takes itself off
+            // its neighbours' live counts (the warp walks each list)
+            const int lane = threadIdx.x & 31;
+#pragma unroll
+            for (int k = 0; k < kPer; ++k) {
+                unsigned todo = __ballot_sync(kFull, partner[k] >= 0);
+                while (todo) {
+                    const int src = __ffs(todo) - 1;
+                    todo &= todo - 1;
+                    const int b = __shfl_sync(kFull, it[k].y, src), e = __shfl_sync(kFull, it[k].z, src);
+                    for (int j = b + lane; j < e; j += 32) atomicSub(p.live + __ldg(p.nbrs + j), 1);
+                }
             }
         }
         if (kStats) {
@@ -920,11 +1034,15 @@ __device__ void commit_phase(const Params &p, Smem &sm, int t, bool has_next)
 // branches and leave the loop at the same round.  Afterwards, vertices that
 // could still be matched keep their last colour as their match value (the
 // reference leaves match[v] = 0 / 1 for them).
-template <bool kW, bool kStats>
+template <bool kW, bool kStats, bool kPolicy>
 __global__ void __launch_bounds__(kThreads, 2) k_rounds(Params p)
 {
     extern __shared__ __align__(16) unsigned char dsmem[];
     Smem &sm = *reinterpret_cast<Smem *>(dsmem);
+    if (kPolicy) {
+        for (int i = threadIdx.x; i < MM_POLICY_FLOATS; i += kThreads) sm.mlp[i] = p.mlp[i];
+        __syncthreads();
+    }
     Ctl *ctl = p.ctl;
     const int cap = ctl->cap;
     const int maximal = ctl->maximal;
@@ -932,7 +1050,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_rounds(Params p)
     const int gwarp = blockIdx.x * kWarps + (threadIdx.x >> 5);
     const int nwarps = gridDim.x * kWarps;
 
-    init_phase<kW, kStats>(p, sm);
+    init_phase<kW, kStats, kPolicy>(p, sm);
     if (!grid_sync(p.bar, p.ctl, p.tstamp, 0)) return;
     int t = 0;
     for (;; ++t) {
@@ -942,7 +1060,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_rounds(Params p)
             ctl->cnt[par ^ 1][threadIdx.x] = 0;
             if (threadIdx.x == 0) ctl->retired[par ^ 1] = 0;
         }
-        scan_window<kW, kStats>(p, t, par);
+        scan_window<kW, kStats, kPolicy>(p, t, par);
         if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 1)) return;
         // phase A2 (all blocks see the same fallback count)
         if (__ldcg(&ctl->staged_pack) != 0ull) {
@@ -954,7 +1072,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_rounds(Params p)
         bool has_next = t + 1 < cap;
         const bool seeds_short = has_next && t + 1 >= nseeds;
         if (seeds_short) has_next = false;
-        commit_phase<kW, kStats>(p, sm, t, has_next);
+        commit_phase<kW, kStats, kPolicy>(p, sm, t, has_next);
         if (blockIdx.x == 0 && threadIdx.x == 0) ctl->staged_pack = 0ull;
         if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 3)) return;
         // close the round (every block decides alike)
@@ -1422,6 +1540,37 @@ int bits_for(long long n)
     return b;
 }
 
+// Weight features of the learned colouring: max and mean of the weights a
+// blue vertex could pick (> -1), 0 without any; a warp per vertex.
+__global__ void k_wfeat(const int2 *ranges, const float *w, int n, float2 *wfeat)
+{
+    const int lane = threadIdx.x & 31;
+    const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long v = gwarp; v < n; v += nwarps) {
+        const int2 r = ranges[v];
+        float mx = 0.0f, sum = 0.0f;
+        int cnt = 0;
+        for (int j = r.x + lane; j < r.y; j += 32) {
+            const float x = __ldg(w + j);
+            if (x > -1.0f) {
+                mx = cnt ? fmaxf(mx, x) : x;
+                sum += x;
+                ++cnt;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float m2 = __shfl_xor_sync(kFull, mx, o);
+            const int c2 = __shfl_xor_sync(kFull, cnt, o);
+            mx = c2 && (!cnt || m2 > mx) ? m2 : mx;
+            sum += __shfl_xor_sync(kFull, sum, o);
+            cnt += c2;
+        }
+        if (lane == 0) wfeat[v] = make_float2(mx, cnt ? sum / (float)cnt : 0.0f);
+    }
+}
+
 // Rounds of each graph of a batch: the reference's loop for a graph runs
 // until a round finds none of its vertices unmatched at the colouring, so it
 // executes its last active round and one more (at most the cap; an empty
@@ -1461,7 +1610,10 @@ struct PushState {
     unsigned long long *stats = nullptr;
     unsigned long long *tstamp = nullptr;
     unsigned *bar = nullptr;
-    int grid[2][2] = {{0, 0}, {0, 0}};    // co-resident blocks of k_rounds<weighted, stats>
+    int grid[2][3] = {{0, 0, 0}, {0, 0, 0}};  // co-resident blocks of k_rounds by weighting and mode
+    float *mlp = nullptr;                 // learned colouring: policy weights (device)
+    int *live = nullptr;                  // learned colouring: unmatched list entries per vertex
+    float2 *wfeat = nullptr;              // learned colouring: (max, mean) incident weight per vertex
 };
 
 void free_state(PushState *s)
@@ -1481,17 +1633,21 @@ void free_state(PushState *s)
     dev_free(s->stats, 0);
     dev_free(s->tstamp, 0);
     dev_free(s->bar, 0);
+    dev_free(s->mlp, 0);
+    dev_free(s->live, 0);
+    dev_free(s->wfeat, 0);
     delete s;
 }
 
-template <bool kW, bool kStats>
+template <bool kW, bool kStats, bool kPolicy>
 int coresident_blocks(int sms)
 {
     int occ = 0;
-    if (cudaFuncSetAttribute(k_rounds<kW, kStats>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem)) !=
-        cudaSuccess)
+    if (cudaFuncSetAttribute(k_rounds<kW, kStats, kPolicy>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(Smem)) != cudaSuccess)
         return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rounds<kW, kStats>, kThreads, sizeof(Smem)) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rounds<kW, kStats, kPolicy>, kThreads, sizeof(Smem)) !=
+        cudaSuccess)
         return 0;
     return occ * sms;
 }
@@ -1526,6 +1682,7 @@ mm_status alloc_state(mm_graph *g, PushState **out)
         e = dev_alloc((void **)&s->stats, sizeof(unsigned long long) * kMaxRounds * MM_STATS_COLS, 0);
     if (e == cudaSuccess) e = dev_alloc((void **)&s->tstamp, sizeof(unsigned long long) * kStampCount, 0);
     if (e == cudaSuccess) e = dev_alloc((void **)&s->bar, sizeof(unsigned) * kBarWords, 0);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->bar, 0, sizeof(unsigned) * kBarWords, 0);
     if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) {
         cudaDeviceSynchronize();
@@ -1540,22 +1697,30 @@ mm_status alloc_state(mm_graph *g, PushState **out)
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-    s->grid[0][0] = coresident_blocks<false, false>(sms);
-    s->grid[0][1] = coresident_blocks<false, true>(sms);
-    s->grid[1][0] = coresident_blocks<true, false>(sms);
-    s->grid[1][1] = coresident_blocks<true, true>(sms);
+    s->grid[0][0] = coresident_blocks<false, false, false>(sms);
+    s->grid[0][1] = coresident_blocks<false, true, false>(sms);
+    s->grid[0][2] = coresident_blocks<false, false, true>(sms);
+    s->grid[1][0] = coresident_blocks<true, false, false>(sms);
+    s->grid[1][1] = coresident_blocks<true, true, false>(sms);
+    s->grid[1][2] = coresident_blocks<true, false, true>(sms);
     cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) {
         free_state(s);
         return cuda_fail(le, "push: kernel attributes");
     }
     const int most = kBarMaxGroups * kBarGroup;
-    if (s->grid[0][0] > most || s->grid[0][1] > most || s->grid[1][0] > most || s->grid[1][1] > most) {
+    bool over = false, under = false;
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 3; ++b) {
+            over |= s->grid[a][b] > most;
+            under |= s->grid[a][b] < 1;
+        }
+    if (over) {
         free_state(s);
         set_error("push: more co-resident blocks than the grid barrier supports");
         return MM_ERR_UNSUPPORTED;
     }
-    if (!coop || s->grid[0][0] < 1 || s->grid[0][1] < 1 || s->grid[1][0] < 1 || s->grid[1][1] < 1) {
+    if (!coop || under) {
         free_state(s);
         set_error("push: the device cannot run the cooperative round kernel");
         return MM_ERR_UNSUPPORTED;
@@ -1588,6 +1753,12 @@ Params make_params(mm_graph *g, PushState *s, bool weighted, bool stats, bool ti
     p.seg_first = s->seg_first;
     p.vbase = g->ngraphs > 0 ? g->d_vbase : nullptr;
     p.last = g->ngraphs > 0 ? g->d_last : nullptr;
+    p.mlp = nullptr;
+    p.level = 0.0f;
+    p.live = s->live;
+    p.wfeat = s->wfeat;
+    p.trace = nullptr;
+    p.trace_rounds = 0;
     p.seeds = s->seeds;
     p.ctl = s->ctl;
     p.stats = stats ? s->stats : nullptr;
@@ -1596,13 +1767,26 @@ Params make_params(mm_graph *g, PushState *s, bool weighted, bool stats, bool ti
     return p;
 }
 
-template <bool kW, bool kStats>
-mm_status launch_rounds(mm_graph *g, PushState *s, bool timing, cudaStream_t stream)
+struct PolicyArgs {
+    float level = 0.0f;
+    float *trace = nullptr;
+    int trace_rounds = 0;
+};
+
+template <bool kW, bool kStats, bool kPolicy>
+mm_status launch_rounds(mm_graph *g, PushState *s, bool timing, cudaStream_t stream, const PolicyArgs *pol = nullptr)
 {
     Params prm = make_params(g, s, kW, kStats, timing);
+    if (kPolicy) {
+        prm.mlp = s->mlp;
+        prm.level = pol->level;
+        prm.trace = pol->trace;
+        prm.trace_rounds = pol->trace_rounds;
+    }
     void *args[] = {&prm};
-    MM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)k_rounds<kW, kStats>, dim3(s->grid[kW][kStats]), dim3(kThreads),
-                                            args, sizeof(Smem), stream),
+    const int mode = kPolicy ? 2 : (kStats ? 1 : 0);
+    MM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)k_rounds<kW, kStats, kPolicy>, dim3(s->grid[kW][mode]),
+                                            dim3(kThreads), args, sizeof(Smem), stream),
                 "round kernel launch");
     return MM_OK;
 }
@@ -1672,8 +1856,11 @@ mm_status run_rounds(mm_graph *g, PushState *s, int type, bool stats, bool timin
     if (stats)
         MM_CUDA_TRY(cudaMemsetAsync(s->stats, 0, sizeof(unsigned long long) * kMaxRounds * MM_STATS_COLS, stream),
                     "stats clear");
-    if (w) return stats ? launch_rounds<true, true>(g, s, timing, stream) : launch_rounds<true, false>(g, s, timing, stream);
-    return stats ? launch_rounds<false, true>(g, s, timing, stream) : launch_rounds<false, false>(g, s, timing, stream);
+    if (w)
+        return stats ? launch_rounds<true, true, false>(g, s, timing, stream)
+                     : launch_rounds<true, false, false>(g, s, timing, stream);
+    return stats ? launch_rounds<false, true, false>(g, s, timing, stream)
+                 : launch_rounds<false, false, false>(g, s, timing, stream);
 }
 
 }  // namespace
@@ -2007,6 +2194,42 @@ mm_status push_match(mm_graph *g, int type, uint32_t barrier, const uint32_t *se
     st = run_rounds(g, s, type, stats != nullptr, false, stream);
     if (st != MM_OK) return st;
     return end_call(g, s, nseeds, rounds_out, stats, stats_rounds, nullptr, stream);
+}
+
+// The round kernel with the learned colouring: each vertex's blue probability
+// comes from the policy (MM_POLICY_FLOATS weights, host) instead of the select
+// barrier.  trace (device, trace_rounds * n * 8 floats, or null) receives the
+// features, colour and outcome of every vertex coloured in those rounds.
+mm_status push_match_policy(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds,
+                            const float *mlp_host, float level, int *d_match, int *rounds_out, float *trace,
+                            int trace_rounds, cudaStream_t stream)
+{
+    if (g->n == 0) return push_match(g, type, barrier, seeds, nseeds, d_match, rounds_out, nullptr, 0, stream);
+    PushState *s = nullptr;
+    mm_status st = begin_call(g, type, barrier, seeds, nseeds, d_match, stream, &s);
+    if (st != MM_OK) return st;
+    if (!s->mlp) {
+        cudaError_t e = dev_alloc((void **)&s->mlp, sizeof(float) * MM_POLICY_FLOATS, stream);
+        if (e == cudaSuccess) e = dev_alloc((void **)&s->live, sizeof(int) * (size_t)g->n, stream);
+        if (e == cudaSuccess) e = dev_alloc((void **)&s->wfeat, sizeof(float2) * (size_t)g->n, stream);
+        if (e == cudaSuccess) {
+            k_wfeat<<<grid_for((long long)g->n * 32, 256, 148 * 16), 256, 0, stream>>>(g->d_ranges, g->d_w, g->n,
+                                                                                    s->wfeat);
+            e = cudaGetLastError();
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "policy state");
+    }
+    MM_CUDA_TRY(cudaMemcpyAsync(s->mlp, mlp_host, sizeof(float) * MM_POLICY_FLOATS, cudaMemcpyHostToDevice, stream),
+                "policy weights");
+    MM_CUDA_TRY(cudaMemsetAsync(s->bar, 0, sizeof(unsigned) * kBarWords, stream), "barrier clear");
+    PolicyArgs pol;
+    pol.level = level;
+    pol.trace = trace;
+    pol.trace_rounds = trace ? trace_rounds : 0;
+    st = is_weighted(type) ? launch_rounds<true, false, true>(g, s, false, stream, &pol)
+                           : launch_rounds<false, false, true>(g, s, false, stream, &pol);
+    if (st != MM_OK) return st;
+    return end_call(g, s, nseeds, rounds_out, nullptr, 0, nullptr, stream);
 }
 
 // Same launch as push_match with barrier timestamps on: block 0 reads the

@@ -1,0 +1,142 @@
+"""Train the learned colouring policy and compare it with the plain method.
+
+    python multicore-matching_b200/train_policy.py [--out PATH] [--report PATH]
+
+Training graphs: a random geometric graph (2^18 vertices, average degree 13)
+and an R-MAT graph (2^18, edge factor 16), each with its plain-method
+multilevel hierarchy, weighted maximal matching (type 9), several seed
+sequences.  Stage 1 fits the policy to traces of the plain colouring (every
+vertex blue with p0) by inverse propensity weighting inside a trust region
+around p0; stage 2 refines it on-policy by evolution strategies on the total
+rounds over the training hierarchies, penalising a matching weight more than
+0.5% below the plain method's.  The weights go to --out (policy_mlp.f32 next
+to this file by default).
+
+Evaluation graphs (held out): RGG and R-MAT with 2^22 vertices and their plain
+hierarchies; per level, rounds, device time and matching weight of the plain
+method, of the policy kernel at the plain probability and of the learned
+colouring, as JSON lines to --report (stdout by default).
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import resource
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent
+sys.path.insert(0, str(ROOT))
+
+from __graft_entry__ import load_package  # noqa: E402
+
+_T0 = time.time()
+
+
+def log(msg):
+    """Progress to stderr: elapsed seconds, peak host memory, stage."""
+    rss = resource.getrusage(resource.RUSAGE_SELF).ru_maxrss / 1024
+    print(f"[{time.time() - _T0:7.1f}s {rss:8.0f} MB] {msg}", file=sys.stderr, flush=True)
+
+
+def level_of(g) -> float:
+    return float(g.name.split("-L")[1]) if "-L" in g.name else 0.0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=str(HERE / "policy_mlp.f32"))
+    ap.add_argument("--report", default="")
+    ap.add_argument("--train-scale", type=int, default=18)
+    ap.add_argument("--eval-scale", type=int, default=22)
+    ap.add_argument("--seeds", type=int, default=3)
+    ap.add_argument("--es-iters", type=int, default=40)
+    args = ap.parse_args()
+    mm = load_package()
+    spec = importlib.util.spec_from_file_location("mm_policy", HERE / "policy.py")
+    pol = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(pol)
+    import torch
+
+    torch.cuda.set_device(0)
+    type_ = 9
+    seed_sets = [mm.rand_seeds(12345 + 1000 * k, 255) for k in range(args.seeds)]
+    n = 1 << args.train_scale
+    train_graphs = pol.hierarchy(mm, mm.Graph.rgg(n, 13.0, seed=101), type_, seed_sets[0])
+    train_graphs += pol.hierarchy(mm, mm.Graph.rmat(args.train_scale, 16, seed=103), type_, seed_sets[0])
+    log(f"training graphs: {[g.n for g in train_graphs]}")
+    dgs = [mm.DeviceGraph(g, device=0) for g in train_graphs]
+    try:
+        # stage 1: plain-colouring traces, trust-region IPS fit
+        plain = pol.constant_policy()
+        X, C, Y = [], [], []
+        for g, dg in zip(train_graphs, dgs):
+            for seeds in seed_sets:
+                x, c, y, r = pol.collect(mm, dg, type_, seeds, plain, level_of(g))
+                X.append(x)
+                C.append(c)
+                Y.append(y)
+        X, C, Y = np.concatenate(X), np.concatenate(C), np.concatenate(Y)
+        log(f"plain traces: {len(X)} rows, leave rate {Y.mean():.4f}")
+        w1 = pol.fit_ips(X, C, Y, np.full(len(X), pol.P0), seed=1)
+        log("stage 1 fitted")
+
+        # stage 2: on-policy evolution strategies on rounds, weight guarded
+        out = torch.empty(max(g.n for g in train_graphs), dtype=torch.int32, device="cuda")
+        es_seeds = seed_sets[1:] or seed_sets
+
+        def run(w):
+            rounds, weight = 0, 0.0
+            for g, dg in zip(train_graphs, dgs):
+                for seeds in es_seeds:
+                    if w is None:
+                        rounds += dg.match_device(type_, seeds, out.data_ptr())
+                    else:
+                        rounds += dg.match_policy(type_, seeds, out.data_ptr(), w, level_of(g))
+                    weight += dg.weight(out.data_ptr())[0]
+            return rounds, weight
+
+        r_plain, w_plain = run(None)
+
+        def objective(w):
+            r, wt = run(w)
+            drop = max(0.0, (0.995 * w_plain - wt) / w_plain)
+            return -r / r_plain - 20.0 * drop
+
+        f_plain = -1.0
+        f_retire = objective(plain)
+        f_stage1 = objective(w1)
+        log(f"objective: plain {f_plain:.4f} retire-only {f_retire:.4f} stage 1 {f_stage1:.4f}")
+        start = w1 if f_stage1 >= f_retire else plain
+        w2, f2 = pol.es_refine(objective, start, iters=args.es_iters, seed=2, log=log)
+        log(f"stage 2: {f2:.4f}")
+    finally:
+        for dg in dgs:
+            dg.close()
+    w2.tofile(args.out)
+    info = {"training_samples": int(len(X)), "training_graphs": [g.name for g in train_graphs],
+            "leave_rate_plain_traces": float(Y.mean()),
+            "objective": {"plain": f_plain, "retire_only": f_retire, "stage1": f_stage1, "stage2": f2}}
+    lines = [json.dumps(info)]
+    ne = 1 << args.eval_scale
+    for g in (mm.Graph.rgg(ne, 13.0, seed=7), mm.Graph.rmat(args.eval_scale, 16, seed=1)):
+        levels = pol.hierarchy(mm, g, type_, seed_sets[0])
+        log(f"evaluation hierarchy {g.name}: {[x.n for x in levels]}")
+        rows = pol.evaluate(mm, levels, type_, mm.rand_seeds(12345, 255), w2)
+        tot = {k: {m: sum(r[k][m] for r in rows) for m in ("rounds", "ms", "weight")}
+               for k in ("plain", "retire", "learned")}
+        lines.append(json.dumps({"graph": g.name, "levels": rows, "total": tot}))
+        log("evaluated")
+    text = "\n".join(lines)
+    if args.report:
+        Path(args.report).write_text(text + "\n")
+    print(text)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,100 @@
+"""Learned colouring (mm_match_policy): whatever the policy, the result must be
+a valid matching, maximal for the maximal types (checked with the oracle's
+restatement of testMatching); the trace must hold one well-formed row per
+coloured vertex and round.  The policy is not the reference's path (mm_match
+is), so there is no bit-exact comparison here."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+BARRIER = 0x88B81733
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    return torch
+
+
+def _policies(mm):
+    rng = np.random.default_rng(0)
+    yield np.zeros(mm.POLICY_FLOATS, np.float32)  # p = 1/2 everywhere
+    w = np.zeros(mm.POLICY_FLOATS, np.float32)
+    w[-1] = 2.5  # mostly blue (p = 0.92): slow but within the round cap
+    yield w
+    yield (rng.standard_normal(mm.POLICY_FLOATS) * 0.5).astype(np.float32)
+
+
+@pytest.mark.parametrize("type_", [6, 7, 8, 9])
+def test_policy_matchings_are_valid_and_maximal(mm, orc, torch_cuda, type_):
+    seeds = orc.rand_seeds(12345, 256)
+    for g in (mm.Graph.rgg(1 << 12, 13.0, seed=4), mm.Graph.rmat(12, 16, seed=2), mm.Graph.grid(40, 30)):
+        with mm.DeviceGraph(g, device=0) as dg:
+            for mlp in _policies(mm):
+                out = torch_cuda.empty(g.n, dtype=torch_cuda.int32, device="cuda")
+                rounds = dg.match_policy(type_, seeds, out.data_ptr(), mlp, 1.0)
+                m = out.cpu().numpy()
+                chk = orc.check(g, m)
+                assert chk["valid"], (g.name, type_, chk)
+                if type_ in (7, 9):
+                    assert chk["matchable"] == 0 and rounds <= 255, (g.name, chk)
+                else:
+                    assert rounds == 20
+
+
+def test_policy_trace_rows(mm, orc, torch_cuda):
+    g = mm.Graph.rgg(1 << 12, 13.0, seed=9)
+    seeds = orc.rand_seeds(5, 256)
+    w = np.zeros(mm.POLICY_FLOATS, np.float32)
+    with mm.DeviceGraph(g, device=0) as dg:
+        rounds_cap = 40
+        tr = torch_cuda.full((rounds_cap * g.n * 8,), float("nan"), dtype=torch_cuda.float32, device="cuda")
+        out = torch_cuda.empty(g.n, dtype=torch_cuda.int32, device="cuda")
+        rounds = dg.match_policy(9, seeds, out.data_ptr(), w, 2.0, tr.data_ptr(), rounds_cap)
+        t = tr.view(rounds_cap, g.n, 8).cpu().numpy()
+        m = out.cpu().numpy()
+    coloured = ~np.isnan(t[:, :, 6])
+    assert coloured[0].all()  # every vertex is coloured in round 0
+    rows = t[coloured]
+    assert set(np.unique(rows[:, 6])) <= {0.0, 1.0} and set(np.unique(rows[:, 7])) <= {0.0, 1.0}
+    assert np.allclose(rows[:, 5], 2.0 / 16)  # the level feature
+    for r in range(rounds_cap):  # the round feature saturates at 32 rounds
+        assert np.allclose(t[r][coloured[r]][:, 4], min(r, 32) / 32)
+    deg = g.degrees()
+    assert np.allclose(t[0, :, 0], np.log2(1 + deg), atol=1e-5)
+    assert np.allclose(t[0, :, 1], np.log2(1 + deg), atol=1e-5)  # every entry is live in round 0
+    assert np.all(t[:, :, 1][coloured] <= t[0, :, 1][None, :].repeat(rounds_cap, 0)[coloured] + 1e-6)
+    # every vertex that left the active set (matched, or retired with match
+    # value 2) is marked in exactly one round, survivors in none
+    marks = np.nansum(t[:, :, 7], axis=0)
+    assert np.array_equal(marks, ((m >= 4) | (m == 2)).astype(np.float64))
+    # a vertex is marked in a round in which it was coloured
+    assert not np.isnan(t[:, :, 6][t[:, :, 7] == 1]).any()
+    assert rounds <= rounds_cap
+
+
+@pytest.mark.parametrize("type_", [6, 7, 8, 9])
+def test_zero_policy_gives_the_plain_matching(mm, orc, torch_cuda, type_):
+    """With all weights 0 the policy's probability is exactly 1/2, the select
+    barrier 0x80000000: the colours are the plain method's, and retiring
+    vertices without live entries early changes no matched pair, only the
+    rounds (maximal types) and the match value of unmatched vertices (2 for
+    retired ones, their colour for survivors of the fixed-round types)."""
+    seeds = orc.rand_seeds(777, 256)
+    w = np.zeros(mm.POLICY_FLOATS, np.float32)
+    for g in (mm.Graph.rgg(1 << 13, 13.0, seed=5), mm.Graph.rmat(13, 16, seed=6), mm.Graph.grid(50, 40)):
+        with mm.DeviceGraph(g, device=0) as dg:
+            a = torch_cuda.empty(g.n, dtype=torch_cuda.int32, device="cuda")
+            b = torch_cuda.empty(g.n, dtype=torch_cuda.int32, device="cuda")
+            r_plain = dg.match_device(type_, seeds, a.data_ptr(), 0x80000000)
+            r_pol = dg.match_policy(type_, seeds, b.data_ptr(), w, 0.0, barrier=0x80000000)
+            ma, mb = a.cpu().numpy(), b.cpu().numpy()
+            assert np.array_equal(ma >= 4, mb >= 4), g.name
+            assert np.array_equal(ma[ma >= 4], mb[mb >= 4]), g.name
+            if type_ in (7, 9):
+                assert np.array_equal(ma, mb) and r_pol <= r_plain, (g.name, r_pol, r_plain)
