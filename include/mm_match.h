@@ -218,15 +218,15 @@ mm_status mm_match_batch(mm_graph *g, int type, uint32_t barrier, const uint32_t
  * Learned colouring; no counterpart in the reference, whose select kernel
  * colours every vertex blue with the same probability (the barrier).  Here a
  * per-vertex MLP (6 -> 16 -> 1, ReLU, sigmoid) gives each vertex its own blue
- * probability from local features: log2(1 + degree), log2(1 + live entries:
- * list entries whose neighbour is still unmatched, kept exact on graphs whose
- * structure is symmetric, else the degree), max and mean weight it could
- * pick, min(round, 32) / 32 and level / 16 (the caller's coarsening level).
- * The probability is clamped to [1/16, 15/16], so the maximal types finish
- * inside the round cap whatever the weights.  On symmetric graphs a vertex
- * with no live entry leaves at its next colouring whatever its colour (the
- * reference waits until it is coloured blue); the matching is the same as
- * the one the same colours give without that.  mlp: MM_POLICY_FLOATS host
+ * probability from local features: log2(1 + degree), its role in the previous
+ * round (0 red or first round, 0.5 blue without a proposal, 1 blue whose
+ * proposal lost), max and mean weight it could pick, min(round, 32) / 32 and
+ * level / 16 (the caller's coarsening level).  The probability is clamped to
+ * [1/16, 15/16], so the maximal types finish inside the round cap whatever
+ * the weights.  From round 3 on, a vertex of at most 32 entries whose
+ * neighbours are all matched leaves at its next colouring whatever its
+ * colour (the reference waits until it is coloured blue); the matching is the
+ * same as the one the same colours give without that.  mlp: MM_POLICY_FLOATS host
  * floats, W1[16][6], b1[16], W2[16], b2.  The result is a valid matching
  * (maximal for types 7, 9) but not the reference's: the reference's path is
  * mm_match.  d_trace (device, trace_rounds * n * 8 floats, or NULL) receives

@@ -119,13 +119,11 @@ struct Params {
     const int *vbase;
     uint8_t *last;
     // Learned colouring (k_rounds<..., kPolicy>): blue iff hash < p_v * 2^32 with
-    // p_v from a per-vertex MLP over local features.  live[v] (symmetric
-    // structure only): list entries of v whose neighbour is not matched yet;
-    // wfeat[v]: (max, mean) incident weight; trace: per round and vertex, the
-    // features, colour and outcome (for training), or null.
+    // p_v from a per-vertex MLP over local features.  wfeat[v]: (max, mean)
+    // incident weight; trace: per round and vertex, the features, colour and
+    // outcome (for training), or null.
     const float *mlp;
     float level;
-    int *live;
     const float2 *wfeat;
     float *trace;
     int trace_rounds;
@@ -366,15 +364,18 @@ struct Smem {
 //
 // The policy is a 6 -> 16 -> 1 MLP (ReLU, sigmoid output) evaluated per vertex
 // when it is coloured; its weights sit in shared memory, laid out as
-// W1[16][6], b1[16], W2[16], b2.  Features: log2(1 + deg), log2(1 + live
-// entries), max and mean incident weight, min(round, 32) / 32, level / 16.  The blue probability is clamped
+// W1[16][6], b1[16], W2[16], b2.  Features: log2(1 + deg), the vertex's role
+// in the previous round (0 red or first round, 0.5 blue without a proposal, 1
+// blue whose proposal lost), max and mean incident weight, min(round, 32) /
+// 32, level / 16.  The blue probability is clamped
 // to [1/16, 15/16] and compared with the colouring hash like the select
 // barrier: an unmatched edge then splits blue/red in at least 11.7% of the
 // rounds, so the maximal types finish well inside the 255-round cap whatever
 // the weights (a pair left alone survives 255 rounds with p < 1e-13).
 constexpr int kFeat = 6, kHid = 16;
 static_assert(kHid * kFeat + kHid + kHid + 1 == MM_POLICY_FLOATS, "policy layout");
-constexpr int kTraceCols = 8;  // features, colour (1 blue, 0 red), left the active set in that round
+constexpr int kTraceCols = 8;
+constexpr int kRetireFrom = 3;  // learned colouring: first round with the pull retirement check  // features, colour (1 blue, 0 red), left the active set in that round
 
 // Trace: vertex v left the active set in round t (matched, or blue with no
 // unmatched neighbour and so retired).
@@ -384,12 +385,12 @@ __device__ __forceinline__ void trace_left(const Params &p, int t, int v)
     if (kPolicy && p.trace && t < p.trace_rounds) p.trace[((size_t)t * p.n + v) * kTraceCols + kFeat + 1] = 1.0f;
 }
 
-__device__ __forceinline__ void policy_features(const Params &p, int v, int deg, int live, int t,
+__device__ __forceinline__ void policy_features(const Params &p, int v, int deg, float role, int t,
                                                 float (&x)[kFeat])
 {
     const float2 wf = __ldg(p.wfeat + v);
     x[0] = __log2f(1.0f + (float)deg);
-    x[1] = __log2f(1.0f + (float)live);
+    x[1] = role;
     x[2] = wf.x;
     x[3] = wf.y;
     x[4] = (float)min(t, 32) * (1.0f / 32.0f);
@@ -414,13 +415,13 @@ __device__ __forceinline__ uint32_t policy_barrier(const float *wts, const float
 
 // Colour of vertex v for round t: the select barrier, or the policy's.
 template <bool kPolicy>
-__device__ __forceinline__ bool colour_blue(const Params &p, const float *wts, int v, int deg, int live, int t,
+__device__ __forceinline__ bool colour_blue(const Params &p, const float *wts, int v, int deg, float role, int t,
                                             uint32_t seed, uint32_t barrier)
 {
     uint32_t bar = barrier;
     if (kPolicy) {
         float x[kFeat];
-        policy_features(p, v, deg, live, t, x);
+        policy_features(p, v, deg, role, t, x);
         bar = policy_barrier(wts, x);
         const bool blue = colour_of((uint32_t)(v - base_of(p, v)), seed, bar) == kBlue;
         if (p.trace && t < p.trace_rounds) {
@@ -511,8 +512,7 @@ __device__ void init_phase(const Params &p, Smem &sm)
                 item[k].z = r.y;
                 if (kW) item[k].w = (int)__ldg(p.pwin_off + v);
                 const int deg = degree_of(r);
-                if (kPolicy && p.sym) p.live[v] = deg;
-                const bool blue = colour_blue<kPolicy>(p, sm.mlp, v, deg, deg, 0, seed, barrier);
+                const bool blue = colour_blue<kPolicy>(p, sm.mlp, v, deg, 0.0f, 0, seed, barrier);
                 if (p.last) p.last[v] = 0;
                 p.best[v] = 0ull;
                 if (deg > kWin) {
@@ -976,16 +976,26 @@ __device__ void commit_phase(const Params &p, Smem &sm, int t, bool has_next)
                 dest[k] = blue[k] ? kBlue : kRed;
                 continue;
             }
-            // learned colouring: live entries so far (matches of this round may
-            // still arrive; the count only falls, so 0 is final)
-            const int live = kPolicy && p.sym ? __ldcg(p.live + v) : deg;
-            const bool nb = colour_blue<kPolicy>(p, sm.mlp, v, deg, live, t + 1, next_seed, barrier);
+            // learned colouring: a list of at most kWin entries whose
+            // neighbours are all matched leaves now, whatever its colour (the
+            // check stops at the first unmatched neighbour; a neighbour matched
+            // in this phase may still read unmatched, which only delays it)
+            bool gone = false;
+            if (kPolicy && deg <= kWin && t + 1 >= kRetireFrom) {
+                gone = true;
+                for (int j = it[k].y; j < it[k].z; ++j)
+                    if (__ldcg(p.col + __ldg(p.nbrs + j)) != kMatched) {
+                        gone = false;
+                        break;
+                    }
+            }
+            const float role = blue[k] ? (q[k].y != 0 ? 1.0f : 0.5f) : 0.0f;
+            const bool nb = colour_blue<kPolicy>(p, sm.mlp, v, deg, role, t + 1, next_seed, barrier);
             if (p.last) p.last[v] = (uint8_t)(t + 1);
             ++act;
             nblue += nb;
-            // no neighbours: unmatchable as soon as it is blue; learned
-            // colouring: as soon as no neighbour is unmatched, whatever its colour
-            if ((nb && deg == 0) || (kPolicy && live == 0)) {
+            // no neighbours: unmatchable as soon as it is blue
+            if ((nb && deg == 0) || gone) {
                 p.col[v] = kDead;
                 match[v] = 2;
                 ++retired;
@@ -993,21 +1003,6 @@ __device__ void commit_phase(const Params &p, Smem &sm, int t, bool has_next)
             } else {
                 p.col[v] = nb ? kBlue : kRed;
                 dest[k] = nb ? kBlue : kRed;
-            }
-        }
-        if (kPolicy && p.sym) {
-            // learned colouring: every vertex matched now takes itself off
-            // its neighbours' live counts (the warp walks each list)
-            const int lane = threadIdx.x & 31;
-#pragma unroll
-            for (int k = 0; k < kPer; ++k) {
-                unsigned todo = __ballot_sync(kFull, partner[k] >= 0);
-                while (todo) {
-                    const int src = __ffs(todo) - 1;
-                    todo &= todo - 1;
-                    const int b = __shfl_sync(kFull, it[k].y, src), e = __shfl_sync(kFull, it[k].z, src);
-                    for (int j = b + lane; j < e; j += 32) atomicSub(p.live + __ldg(p.nbrs + j), 1);
-                }
             }
         }
         if (kStats) {
@@ -1612,7 +1607,6 @@ struct PushState {
     unsigned *bar = nullptr;
     int grid[2][3] = {{0, 0, 0}, {0, 0, 0}};  // co-resident blocks of k_rounds by weighting and mode
     float *mlp = nullptr;                 // learned colouring: policy weights (device)
-    int *live = nullptr;                  // learned colouring: unmatched list entries per vertex
     float2 *wfeat = nullptr;              // learned colouring: (max, mean) incident weight per vertex
 };
 
@@ -1634,7 +1628,6 @@ void free_state(PushState *s)
     dev_free(s->tstamp, 0);
     dev_free(s->bar, 0);
     dev_free(s->mlp, 0);
-    dev_free(s->live, 0);
     dev_free(s->wfeat, 0);
     delete s;
 }
@@ -1755,7 +1748,6 @@ Params make_params(mm_graph *g, PushState *s, bool weighted, bool stats, bool ti
     p.last = g->ngraphs > 0 ? g->d_last : nullptr;
     p.mlp = nullptr;
     p.level = 0.0f;
-    p.live = s->live;
     p.wfeat = s->wfeat;
     p.trace = nullptr;
     p.trace_rounds = 0;
@@ -2210,7 +2202,6 @@ mm_status push_match_policy(mm_graph *g, int type, uint32_t barrier, const uint3
     if (st != MM_OK) return st;
     if (!s->mlp) {
         cudaError_t e = dev_alloc((void **)&s->mlp, sizeof(float) * MM_POLICY_FLOATS, stream);
-        if (e == cudaSuccess) e = dev_alloc((void **)&s->live, sizeof(int) * (size_t)g->n, stream);
         if (e == cudaSuccess) e = dev_alloc((void **)&s->wfeat, sizeof(float2) * (size_t)g->n, stream);
         if (e == cudaSuccess) {
             k_wfeat<<<grid_for((long long)g->n * 32, 256, 148 * 16), 256, 0, stream>>>(g->d_ranges, g->d_w, g->n,

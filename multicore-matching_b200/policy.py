@@ -3,8 +3,8 @@
 The reference colours every vertex blue with one probability, the select
 barrier (0x88B81733 / 2^32 = 0.534, bin/match.cpp:183).  mm_match_policy lets a
 per-vertex MLP (6 -> 16 -> 1) choose that probability from local features
-(FEATURES below), and on graphs with symmetric structure retires a vertex as
-soon as none of its neighbours is unmatched, instead of waiting until it is
+(FEATURES below), and from round 3 on retires a vertex of at most 32 entries
+as soon as none of its neighbours is unmatched, instead of waiting until it is
 coloured blue.
 
 Training has two stages.
@@ -40,8 +40,8 @@ from pathlib import Path
 
 import numpy as np
 
-FEATURES = ("log2(1+degree)", "log2(1+live entries)", "max incident weight", "mean incident weight",
-            "min(round, 32)/32", "level/16")
+FEATURES = ("log2(1+degree)", "previous role (0 red, 0.5 blue unproposed, 1 blue lost)", "max incident weight",
+            "mean incident weight", "min(round, 32)/32", "level/16")
 N_FEAT, N_HID = 6, 16
 N_FLOATS = N_HID * N_FEAT + N_HID + N_HID + 1  # W1[16][6], b1[16], W2[16], b2
 HERE = Path(__file__).resolve().parent
@@ -140,8 +140,9 @@ def fit_ips(X, c, y, prop, delta=0.2, steps=2000, lr=3e-3, seed=0, device="cuda"
 
 def es_refine(objective, w0, iters=40, pairs=12, sigma=0.05, lr=0.03, seed=0, log=None):
     """Stage 2: antithetic evolution strategies with rank-shaped fitness and
-    Adam steps, maximising objective(weights) from w0.  Returns the best
-    weights evaluated and their objective."""
+    Adam steps, maximising objective(weights) from w0.  Returns the final
+    search centre and the best single candidate (the latter is partly luck:
+    choose between them on held-out seeds)."""
     rng = np.random.default_rng(seed)
     w = w0.astype(np.float64)
     m = np.zeros_like(w)
@@ -163,7 +164,7 @@ def es_refine(objective, w0, iters=40, pairs=12, sigma=0.05, lr=0.03, seed=0, lo
         w = w + lr * (m / (1 - 0.9 ** (it + 1))) / (np.sqrt(v / (1 - 0.999 ** (it + 1))) + 1e-8)
         if log:
             log(f"es {it}: mean {f.mean():.4f} best {best_f:.4f}")
-    return best_w.astype(np.float32), best_f
+    return w.astype(np.float32), best_w.astype(np.float32)
 
 
 def hierarchy(mm, g, type_, seeds, target=0.01, min_shrink=0.05, max_levels=64, device=0):

@@ -86,14 +86,16 @@ def main():
         w1 = pol.fit_ips(X, C, Y, np.full(len(X), pol.P0), seed=1)
         log("stage 1 fitted")
 
-        # stage 2: on-policy evolution strategies on rounds, weight guarded
+        # stage 2: on-policy evolution strategies on rounds, weight guarded;
+        # the pick among the candidates is made on held-out seed sequences
         out = torch.empty(max(g.n for g in train_graphs), dtype=torch.int32, device="cuda")
-        es_seeds = seed_sets[1:] or seed_sets
+        es_seeds = [mm.rand_seeds(777 + 31 * k, 255) for k in range(4)]
+        val_seeds = [mm.rand_seeds(99991 + 53 * k, 255) for k in range(4)]
 
-        def run(w):
+        def run(w, seeds_list):
             rounds, weight = 0, 0.0
             for g, dg in zip(train_graphs, dgs):
-                for seeds in es_seeds:
+                for seeds in seeds_list:
                     if w is None:
                         rounds += dg.match_device(type_, seeds, out.data_ptr())
                     else:
@@ -101,27 +103,29 @@ def main():
                     weight += dg.weight(out.data_ptr())[0]
             return rounds, weight
 
-        r_plain, w_plain = run(None)
+        def make_objective(seeds_list):
+            r_plain, w_plain = run(None, seeds_list)
 
-        def objective(w):
-            r, wt = run(w)
-            drop = max(0.0, (0.995 * w_plain - wt) / w_plain)
-            return -r / r_plain - 20.0 * drop
+            def objective(w):
+                r, wt = run(w, seeds_list)
+                drop = max(0.0, (0.995 * w_plain - wt) / w_plain)
+                return -r / r_plain - 20.0 * drop
+            return objective
 
-        f_plain = -1.0
-        f_retire = objective(plain)
-        f_stage1 = objective(w1)
-        log(f"objective: plain {f_plain:.4f} retire-only {f_retire:.4f} stage 1 {f_stage1:.4f}")
-        start = w1 if f_stage1 >= f_retire else plain
-        w2, f2 = pol.es_refine(objective, start, iters=args.es_iters, seed=2, log=log)
-        log(f"stage 2: {f2:.4f}")
+        train_obj, val_obj = make_objective(es_seeds), make_objective(val_seeds)
+        start = w1 if train_obj(w1) >= train_obj(plain) else plain
+        centre, lucky = pol.es_refine(train_obj, start, iters=args.es_iters, seed=2, log=log)
+        cands = {"retire_only": plain, "stage1": w1, "es_centre": centre, "es_best": lucky}
+        scores = {k: val_obj(w) for k, w in cands.items()}
+        log(f"held-out objective (plain = -1): {scores}")
+        pick = max(scores, key=scores.get)
+        w2 = cands[pick]
     finally:
         for dg in dgs:
             dg.close()
     w2.tofile(args.out)
     info = {"training_samples": int(len(X)), "training_graphs": [g.name for g in train_graphs],
-            "leave_rate_plain_traces": float(Y.mean()),
-            "objective": {"plain": f_plain, "retire_only": f_retire, "stage1": f_stage1, "stage2": f2}}
+            "leave_rate_plain_traces": float(Y.mean()), "held_out_objective": scores, "picked": pick}
     lines = [json.dumps(info)]
     ne = 1 << args.eval_scale
     for g in (mm.Graph.rgg(ne, 13.0, seed=7), mm.Graph.rmat(args.eval_scale, 16, seed=1)):

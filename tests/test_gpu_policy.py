@@ -67,8 +67,13 @@ def test_policy_trace_rows(mm, orc, torch_cuda):
         assert np.allclose(t[r][coloured[r]][:, 4], min(r, 32) / 32)
     deg = g.degrees()
     assert np.allclose(t[0, :, 0], np.log2(1 + deg), atol=1e-5)
-    assert np.allclose(t[0, :, 1], np.log2(1 + deg), atol=1e-5)  # every entry is live in round 0
-    assert np.all(t[:, :, 1][coloured] <= t[0, :, 1][None, :].repeat(rounds_cap, 0)[coloured] + 1e-6)
+    assert np.all(t[0, :, 1] == 0.0)  # no previous round
+    assert set(np.unique(rows[:, 1])) <= {0.0, 0.5, 1.0}  # previous role
+    # a vertex red in round r has role 0 in round r + 1
+    for r in range(rounds_cap - 1):
+        both = coloured[r] & coloured[r + 1]
+        assert np.all(t[r + 1, :, 1][both & (t[r, :, 6] == 0.0)] == 0.0)
+        assert np.all(t[r + 1, :, 1][both & (t[r, :, 6] == 1.0)] > 0.0)
     # every vertex that left the active set (matched, or retired with match
     # value 2) is marked in exactly one round, survivors in none
     marks = np.nansum(t[:, :, 7], axis=0)
@@ -82,7 +87,7 @@ def test_policy_trace_rows(mm, orc, torch_cuda):
 def test_zero_policy_gives_the_plain_matching(mm, orc, torch_cuda, type_):
     """With all weights 0 the policy's probability is exactly 1/2, the select
     barrier 0x80000000: the colours are the plain method's, and retiring
-    vertices without live entries early changes no matched pair, only the
+    vertices whose neighbours are all matched early changes no matched pair, only the
     rounds (maximal types) and the match value of unmatched vertices (2 for
     retired ones, their colour for survivors of the fixed-round types)."""
     seeds = orc.rand_seeds(777, 256)
