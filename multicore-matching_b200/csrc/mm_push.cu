@@ -122,12 +122,16 @@ struct Params {
     // p_v from a per-vertex MLP over local features.  wfeat[v]: (max, mean)
     // incident weight; trace: per round and vertex, the features, colour and
     // outcome (for training), or null.
-    const float *mlp;
     float level;
     const float2 *wfeat;
     float *trace;
     int trace_rounds;
+    // The policy's weights travel by value in the launch parameters: every
+    // thread reads the same one, so the unrolled MLP takes them straight from
+    // the constant bank as operands, with no load instruction per weight.
+    float mlp[MM_POLICY_FLOATS];
 };
+static_assert(sizeof(Params) <= 4096, "launch parameters stay within the classic 4 KB limit");
 
 __device__ __forceinline__ int base_of(const Params &p, int v) { return p.vbase ? __ldg(p.vbase + v) : 0; }
 
@@ -357,13 +361,12 @@ struct Smem {
     LongStage stage[kWarps];
     int tile_warp[kWarps][2];             // compaction: per-warp counts, then offsets
     int tile_base[2];                     // compaction: tile bases
-    float mlp[MM_POLICY_FLOATS];          // learned colouring: the policy's weights
 };
 
 // ---- learned colouring ----
 //
 // The policy is a 6 -> 16 -> 1 MLP (ReLU, sigmoid output) evaluated per vertex
-// when it is coloured; its weights sit in shared memory, laid out as
+// when it is coloured; its weights are a launch parameter, laid out as
 // W1[16][6], b1[16], W2[16], b2.  Features: log2(1 + deg), the vertex's role
 // in the previous round (0 red or first round, 0.5 blue without a proposal, 1
 // blue whose proposal lost), max and mean incident weight, min(round, 32) /
@@ -374,8 +377,8 @@ struct Smem {
 // the weights (a pair left alone survives 255 rounds with p < 1e-13).
 constexpr int kFeat = 6, kHid = 16;
 static_assert(kHid * kFeat + kHid + kHid + 1 == MM_POLICY_FLOATS, "policy layout");
-constexpr int kTraceCols = 8;
-constexpr int kRetireFrom = 3;  // learned colouring: first round with the pull retirement check  // features, colour (1 blue, 0 red), left the active set in that round
+constexpr int kTraceCols = 8;  // features, colour (1 blue, 0 red), left the active set in that round
+constexpr int kRetireFrom = 3;  // learned colouring: first round in which red vertices retire
 
 // Trace: vertex v left the active set in round t (matched, or blue with no
 // unmatched neighbour and so retired).
@@ -385,10 +388,9 @@ __device__ __forceinline__ void trace_left(const Params &p, int t, int v)
     if (kPolicy && p.trace && t < p.trace_rounds) p.trace[((size_t)t * p.n + v) * kTraceCols + kFeat + 1] = 1.0f;
 }
 
-__device__ __forceinline__ void policy_features(const Params &p, int v, int deg, float role, int t,
+__device__ __forceinline__ void policy_features(const Params &p, float2 wf, int deg, float role, int t,
                                                 float (&x)[kFeat])
 {
-    const float2 wf = __ldg(p.wfeat + v);
     x[0] = __log2f(1.0f + (float)deg);
     x[1] = role;
     x[2] = wf.x;
@@ -397,16 +399,16 @@ __device__ __forceinline__ void policy_features(const Params &p, int v, int deg,
     x[5] = p.level * (1.0f / 16.0f);
 }
 
-__device__ __forceinline__ uint32_t policy_barrier(const float *wts, const float (&x)[kFeat])
+__device__ __forceinline__ uint32_t policy_barrier(const Params &p, const float (&x)[kFeat])
 {
-    const float *W1 = wts, *b1 = W1 + kHid * kFeat, *W2 = b1 + kHid, *b2 = W2 + kHid;
-    float out = b2[0];
+    constexpr int kB1 = kHid * kFeat, kW2 = kB1 + kHid, kB2 = kW2 + kHid;
+    float out = p.mlp[kB2];
 #pragma unroll
     for (int j = 0; j < kHid; ++j) {
-        float a = b1[j];
+        float a = p.mlp[kB1 + j];
 #pragma unroll
-        for (int i = 0; i < kFeat; ++i) a = fmaf(W1[j * kFeat + i], x[i], a);
-        out = fmaf(W2[j], fmaxf(a, 0.0f), out);
+        for (int i = 0; i < kFeat; ++i) a = fmaf(p.mlp[j * kFeat + i], x[i], a);
+        out = fmaf(p.mlp[kW2 + j], fmaxf(a, 0.0f), out);
     }
     float prob = 1.0f / (1.0f + __expf(-out));
     prob = fminf(fmaxf(prob, 1.0f / 16.0f), 15.0f / 16.0f);
@@ -415,14 +417,14 @@ __device__ __forceinline__ uint32_t policy_barrier(const float *wts, const float
 
 // Colour of vertex v for round t: the select barrier, or the policy's.
 template <bool kPolicy>
-__device__ __forceinline__ bool colour_blue(const Params &p, const float *wts, int v, int deg, float role, int t,
+__device__ __forceinline__ bool colour_blue(const Params &p, int v, int deg, float role, float2 wf, int t,
                                             uint32_t seed, uint32_t barrier)
 {
     uint32_t bar = barrier;
     if (kPolicy) {
         float x[kFeat];
-        policy_features(p, v, deg, role, t, x);
-        bar = policy_barrier(wts, x);
+        policy_features(p, wf, deg, role, t, x);
+        bar = policy_barrier(p, x);
         const bool blue = colour_of((uint32_t)(v - base_of(p, v)), seed, bar) == kBlue;
         if (p.trace && t < p.trace_rounds) {
             float *row = p.trace + ((size_t)t * p.n + v) * kTraceCols;
@@ -512,7 +514,8 @@ __device__ void init_phase(const Params &p, Smem &sm)
                 item[k].z = r.y;
                 if (kW) item[k].w = (int)__ldg(p.pwin_off + v);
                 const int deg = degree_of(r);
-                const bool blue = colour_blue<kPolicy>(p, sm.mlp, v, deg, 0.0f, 0, seed, barrier);
+                const float2 wf = kPolicy ? __ldg(p.wfeat + v) : make_float2(0.0f, 0.0f);
+                const bool blue = colour_blue<kPolicy>(p, v, deg, 0.0f, wf, 0, seed, barrier);
                 if (p.last) p.last[v] = 0;
                 p.best[v] = 0ull;
                 if (deg > kWin) {
@@ -559,6 +562,44 @@ __device__ void init_phase(const Params &p, Smem &sm)
 // fallback list.  Each thread walks kPerW vertices at once, two window entries
 // per vertex and step.
 constexpr int kPerW = 2;
+
+// Learned colouring, graphs with symmetric structure: a red vertex of at most
+// kWin entries whose neighbours are all matched leaves in phase A of this
+// round, while the blue vertices scan (the reference waits until it is
+// coloured blue and scans).  Colours do not change during phase A, so the
+// check is exact, and no vertex reads the retired one's colour: every vertex
+// that lists it is its neighbour, hence matched, and matched vertices do not
+// scan.  (Without symmetry an unmatched blue vertex could list it, and its
+// choice would depend on the timing of the retirement.)  Red items are taken from the top of the thread range down, so
+// on small rounds they run on threads that have no blue item.  Each list is
+// read 8 entries at a time, the batch's colour loads in flight together,
+// stopping after the first batch with an unmatched neighbour.
+template <bool kPolicy>
+__device__ __forceinline__ void retire_red(const Params &p, int t, int par)
+{
+    const int n_red = __ldcg(&p.ctl->cnt[par][kRed]);
+    const int4 *list = p.lists[par][kRed];
+    const long long stride = (long long)gridDim.x * kThreads;
+    const long long tid = stride - 1 - ((long long)blockIdx.x * kThreads + threadIdx.x);
+    for (long long i = tid; i < n_red; i += stride) {
+        const int4 it = __ldcg(list + i);
+        if (degree_of(it) > kWin) continue;
+        bool gone = true;
+        for (int j0 = it.y; gone && j0 < it.z; j0 += 8) {
+            int nb[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) nb[u] = j0 + u < it.z ? __ldg(p.nbrs + j0 + u) : -1;
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (nb[u] >= 0 && p.col[nb[u]] != kMatched) gone = false;
+        }
+        if (gone) {
+            p.col[it.x] = kDead;
+            p.ctl->match[it.x] = 2;
+            trace_left<kPolicy>(p, t, it.x);
+        }
+    }
+}
 
 template <bool kW, bool kStats, bool kPolicy>
 __device__ void scan_window(const Params &p, int t, int par)
@@ -665,6 +706,7 @@ __device__ void scan_window(const Params &p, int t, int par)
             }
         }
     }
+    if (kPolicy && p.sym && t >= kRetireFrom) retire_red<kPolicy>(p, t, par);
 }
 
 // ---- phase A2: fallback lists, entry-balanced segments ----
@@ -967,7 +1009,8 @@ __device__ void commit_phase(const Params &p, Smem &sm, int t, bool has_next)
                 ++matched;
                 continue;
             }
-            if (blue[k] && q[k].x == -1) {  // unmatchable (marked in phase A)
+            // unmatchable (marked in phase A; learned colouring: red ones too)
+            if ((blue[k] && q[k].x == -1) || (kPolicy && !blue[k] && __ldcg(p.col + v) == kDead)) {
                 trace_left<kPolicy>(p, t, v);
                 continue;
             }
@@ -976,26 +1019,14 @@ __device__ void commit_phase(const Params &p, Smem &sm, int t, bool has_next)
                 dest[k] = blue[k] ? kBlue : kRed;
                 continue;
             }
-            // learned colouring: a list of at most kWin entries whose
-            // neighbours are all matched leaves now, whatever its colour (the
-            // check stops at the first unmatched neighbour; a neighbour matched
-            // in this phase may still read unmatched, which only delays it)
-            bool gone = false;
-            if (kPolicy && deg <= kWin && t + 1 >= kRetireFrom) {
-                gone = true;
-                for (int j = it[k].y; j < it[k].z; ++j)
-                    if (__ldcg(p.col + __ldg(p.nbrs + j)) != kMatched) {
-                        gone = false;
-                        break;
-                    }
-            }
             const float role = blue[k] ? (q[k].y != 0 ? 1.0f : 0.5f) : 0.0f;
-            const bool nb = colour_blue<kPolicy>(p, sm.mlp, v, deg, role, t + 1, next_seed, barrier);
+            const float2 wf = kPolicy ? __ldg(p.wfeat + v) : make_float2(0.0f, 0.0f);
+            const bool nb = colour_blue<kPolicy>(p, v, deg, role, wf, t + 1, next_seed, barrier);
             if (p.last) p.last[v] = (uint8_t)(t + 1);
             ++act;
             nblue += nb;
             // no neighbours: unmatchable as soon as it is blue
-            if ((nb && deg == 0) || gone) {
+            if (nb && deg == 0) {
                 p.col[v] = kDead;
                 match[v] = 2;
                 ++retired;
@@ -1034,10 +1065,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_rounds(Params p)
 {
     extern __shared__ __align__(16) unsigned char dsmem[];
     Smem &sm = *reinterpret_cast<Smem *>(dsmem);
-    if (kPolicy) {
-        for (int i = threadIdx.x; i < MM_POLICY_FLOATS; i += kThreads) sm.mlp[i] = p.mlp[i];
-        __syncthreads();
-    }
     Ctl *ctl = p.ctl;
     const int cap = ctl->cap;
     const int maximal = ctl->maximal;
@@ -1606,7 +1633,6 @@ struct PushState {
     unsigned long long *tstamp = nullptr;
     unsigned *bar = nullptr;
     int grid[2][3] = {{0, 0, 0}, {0, 0, 0}};  // co-resident blocks of k_rounds by weighting and mode
-    float *mlp = nullptr;                 // learned colouring: policy weights (device)
     float2 *wfeat = nullptr;              // learned colouring: (max, mean) incident weight per vertex
 };
 
@@ -1627,7 +1653,6 @@ void free_state(PushState *s)
     dev_free(s->stats, 0);
     dev_free(s->tstamp, 0);
     dev_free(s->bar, 0);
-    dev_free(s->mlp, 0);
     dev_free(s->wfeat, 0);
     delete s;
 }
@@ -1746,7 +1771,7 @@ Params make_params(mm_graph *g, PushState *s, bool weighted, bool stats, bool ti
     p.seg_first = s->seg_first;
     p.vbase = g->ngraphs > 0 ? g->d_vbase : nullptr;
     p.last = g->ngraphs > 0 ? g->d_last : nullptr;
-    p.mlp = nullptr;
+    std::memset(p.mlp, 0, sizeof(p.mlp));
     p.level = 0.0f;
     p.wfeat = s->wfeat;
     p.trace = nullptr;
@@ -1760,6 +1785,7 @@ Params make_params(mm_graph *g, PushState *s, bool weighted, bool stats, bool ti
 }
 
 struct PolicyArgs {
+    const float *mlp = nullptr;  // host, MM_POLICY_FLOATS
     float level = 0.0f;
     float *trace = nullptr;
     int trace_rounds = 0;
@@ -1770,7 +1796,7 @@ mm_status launch_rounds(mm_graph *g, PushState *s, bool timing, cudaStream_t str
 {
     Params prm = make_params(g, s, kW, kStats, timing);
     if (kPolicy) {
-        prm.mlp = s->mlp;
+        std::memcpy(prm.mlp, pol->mlp, sizeof(prm.mlp));
         prm.level = pol->level;
         prm.trace = pol->trace;
         prm.trace_rounds = pol->trace_rounds;
@@ -2200,9 +2226,8 @@ mm_status push_match_policy(mm_graph *g, int type, uint32_t barrier, const uint3
     PushState *s = nullptr;
     mm_status st = begin_call(g, type, barrier, seeds, nseeds, d_match, stream, &s);
     if (st != MM_OK) return st;
-    if (!s->mlp) {
-        cudaError_t e = dev_alloc((void **)&s->mlp, sizeof(float) * MM_POLICY_FLOATS, stream);
-        if (e == cudaSuccess) e = dev_alloc((void **)&s->wfeat, sizeof(float2) * (size_t)g->n, stream);
+    if (!s->wfeat) {
+        cudaError_t e = dev_alloc((void **)&s->wfeat, sizeof(float2) * (size_t)g->n, stream);
         if (e == cudaSuccess) {
             k_wfeat<<<grid_for((long long)g->n * 32, 256, 148 * 16), 256, 0, stream>>>(g->d_ranges, g->d_w, g->n,
                                                                                     s->wfeat);
@@ -2210,10 +2235,9 @@ mm_status push_match_policy(mm_graph *g, int type, uint32_t barrier, const uint3
         }
         if (e != cudaSuccess) return cuda_fail(e, "policy state");
     }
-    MM_CUDA_TRY(cudaMemcpyAsync(s->mlp, mlp_host, sizeof(float) * MM_POLICY_FLOATS, cudaMemcpyHostToDevice, stream),
-                "policy weights");
     MM_CUDA_TRY(cudaMemsetAsync(s->bar, 0, sizeof(unsigned) * kBarWords, stream), "barrier clear");
     PolicyArgs pol;
+    pol.mlp = mlp_host;
     pol.level = level;
     pol.trace = trace;
     pol.trace_rounds = trace ? trace_rounds : 0;

@@ -56,6 +56,7 @@ def main():
     ap.add_argument("--eval-scale", type=int, default=22)
     ap.add_argument("--seeds", type=int, default=3)
     ap.add_argument("--es-iters", type=int, default=40)
+    ap.add_argument("--eval-only", default="", help="evaluate these weights (a policy_mlp.f32) without training")
     args = ap.parse_args()
     mm = load_package()
     spec = importlib.util.spec_from_file_location("mm_policy", HERE / "policy.py")
@@ -66,6 +67,11 @@ def main():
     torch.cuda.set_device(0)
     type_ = 9
     seed_sets = [mm.rand_seeds(12345 + 1000 * k, 255) for k in range(args.seeds)]
+    if args.eval_only:
+        w2 = pol.load_policy(Path(args.eval_only))
+        lines = [json.dumps({"weights": args.eval_only})]
+        evaluate_all(mm, pol, args, type_, seed_sets, w2, lines)
+        return
     n = 1 << args.train_scale
     train_graphs = pol.hierarchy(mm, mm.Graph.rgg(n, 13.0, seed=101), type_, seed_sets[0])
     train_graphs += pol.hierarchy(mm, mm.Graph.rmat(args.train_scale, 16, seed=103), type_, seed_sets[0])
@@ -127,6 +133,10 @@ def main():
     info = {"training_samples": int(len(X)), "training_graphs": [g.name for g in train_graphs],
             "leave_rate_plain_traces": float(Y.mean()), "held_out_objective": scores, "picked": pick}
     lines = [json.dumps(info)]
+    evaluate_all(mm, pol, args, type_, seed_sets, w2, lines)
+
+
+def evaluate_all(mm, pol, args, type_, seed_sets, w2, lines):
     ne = 1 << args.eval_scale
     for g in (mm.Graph.rgg(ne, 13.0, seed=7), mm.Graph.rmat(args.eval_scale, 16, seed=1)):
         levels = pol.hierarchy(mm, g, type_, seed_sets[0])
