@@ -38,6 +38,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -61,6 +62,7 @@ WORKLOADS = {
     "rgg20_weighted_maximal": dict(kind="rgg", n=1 << 20, deg=13.0, seed=7, type=9),
     "grid512_random_maximal": dict(kind="grid", w=512, h=512, type=7),
     "rmat20_weighted_maximal": dict(kind="rmat", scale=20, ef=16, seed=1, type=9),
+    "rmat22_weighted_maximal": dict(kind="rmat", scale=22, ef=16, seed=1, type=9),
     "batch4096_weighted_maximal": dict(kind="batch", count=4096, seed=3, type=9),
 }
 BATCH_SAMPLE = 48  # graphs of a batch the CPU baseline and the parity check run
@@ -374,10 +376,12 @@ def main():
     # the scans are bound by random single-sector reads: their measured ceiling on this device
     gather_peak = mm.probe_gather_rate(local, max(g.n, 1))
     colour_gathers = float(st[:, mm.ST_WINDOW_ENTRIES].sum() + st[:, mm.ST_STAGED_DEG].sum())
+    # DRAM bytes of one k_rounds launch from an ncu capture of this workload, where one exists
     traffic = None
-    tfile = ROOT / "profiles" / f"traffic_{args.workload}.json"
+    tfile = ROOT / "profiles" / "dram_traffic_k_rounds_rmat_weighted_maximal.md"
     if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get("dram_bytes_per_launch")
+        m = re.search(rf"dram_bytes_per_launch \({re.escape(args.workload)}\): (\d+)", tfile.read_text())
+        traffic = int(m.group(1)) if m else None
 
     # end to end through the C ABI with host buffers (pinned)
     ranges_h = torch.from_numpy(np.ascontiguousarray(g.ranges, dtype=np.int32)).pin_memory()
