@@ -29,9 +29,11 @@ One step = one matching of the whole graph to maximality.
             match[] is also compared with the GPU result ("parity").
 
 --impl reference runs only that CPU matcher, on the same metric.
-Multi-GPU (torchrun): every rank matches its own replica of the graph
-(replicas only: one graph does not shard); value is the sum over ranks divided
-by the slowest rank's time.
+Multi-GPU (torchrun): for a single graph every rank matches its own replica
+(one graph does not shard); for the batch workload every rank matches its own
+shard of a batch of 4096 graphs per GPU, split by estimated adjacency entries
+(independent graphs: no collective).  value is the sum over ranks of edges
+divided by the slowest rank's time.
 """
 from __future__ import annotations
 
@@ -68,16 +70,27 @@ WORKLOADS = {
 BATCH_SAMPLE = 48  # graphs of a batch the CPU baseline and the parity check run
 
 
-def make_batch(mm, count, seed):
+def make_batch(mm, count, seed, rank=0, world=1):
     """Independent graphs, vertex counts log-uniform in [2^10, 2^18], each a 2D grid,
     a random geometric graph (average degree 13) or an Erdos-Renyi graph (average
     degree 8), weights in (0, 1] from a hash of the endpoint pair; their disjoint
-    union, its offsets, and an evenly spaced sample of (index, graph)."""
+    union, its offsets, and an evenly spaced sample of (index, graph).
+
+    On N GPUs the batch has count * N graphs (count per GPU: weak scaling).  Every
+    rank draws all graphs' sizes and kinds, splits them by estimated adjacency
+    entries with shard_batch, and generates and matches only its own range; graph
+    i is the same on any number of GPUs (its own seed), and N = 1 is the single-GPU
+    batch."""
     rng = np.random.default_rng(seed)
-    graphs = []
-    for i in range(count):
+    plan = []
+    for _ in range(count * world):
         n = int(round(np.exp(rng.uniform(np.log(1 << 10), np.log(1 << 18)))))
-        kind = int(rng.integers(3))
+        plan.append((n, int(rng.integers(3))))
+    est = [n * (4, 13, 8)[kind] for n, kind in plan]
+    lo, hi = mm.shard_batch(est, world)[rank]
+    graphs = []
+    for i in range(lo, hi):
+        n, kind = plan[i]
         gs = seed * 100003 + i
         if kind == 0:
             wd = int(np.sqrt(n))
@@ -87,15 +100,16 @@ def make_batch(mm, count, seed):
         else:
             graphs.append(mm.Graph.er(n, 8.0, seed=gs))
     u, off = mm.Graph.union(graphs)
-    pick = np.linspace(0, count - 1, min(BATCH_SAMPLE, count)).astype(int)
-    sample = [(int(i), graphs[int(i)]) for i in pick]
-    return u, {"offsets": off, "sample": sample, "count": count}
+    pick = np.linspace(0, len(graphs) - 1, min(BATCH_SAMPLE, len(graphs))).astype(int)
+    sample = [(int(i) + lo, graphs[int(i)]) for i in pick]
+    return u, {"offsets": off, "sample": sample, "count": len(graphs), "total": count * world, "range": (lo, hi)}
 
 
-def make_graph(mm, spec):
-    """(graph, batch): batch is None, or the offsets and sample of a batch workload."""
+def make_graph(mm, spec, rank=0, world=1):
+    """(graph, batch): batch is None, or the offsets and sample of a batch workload
+    (this rank's shard of it on N GPUs)."""
     if spec["kind"] == "batch":
-        return make_batch(mm, spec["count"], spec["seed"])
+        return make_batch(mm, spec["count"], spec["seed"], rank, world)
     return make_single(mm, spec), None
 
 
@@ -307,7 +321,7 @@ def main():
     mm = load_package()
     t = spec["type"]
     weighted = t in (8, 9)
-    g, batch = make_graph(mm, spec)
+    g, batch = make_graph(mm, spec, rank, world)
     seeds = mm.rand_seeds(MATCH_SEED, 255)
     stream = torch.cuda.Stream()
     sptr = stream.cuda_stream
@@ -331,6 +345,12 @@ def main():
     rounds, st = dg.stats(t, seeds, out.data_ptr(), stream=sptr)
     work = mm.roofline_bytes(st, weighted)
     edges = work["edges"]
+    # all ranks' edges: every rank matches its own replica, or its own shard of a batch
+    edges_all = edges * world
+    if dist and batch is not None:
+        et = torch.tensor([float(edges)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(et, op=dist.ReduceOp.SUM)
+        edges_all = float(et.item())
 
     # L2 is 126 MB; the CSR alone is > 1 GB, and a 512 MB write flushes L2 between steps.
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
@@ -357,7 +377,7 @@ def main():
         tt = torch.tensor([ms], device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
-    value = edges * world / (ms / 1e3)
+    value = edges_all / (ms / 1e3)
     # per-round phase times of the round kernel (barrier timestamps of the same launch shape)
     prof = []
     for _ in range(3):
@@ -412,6 +432,10 @@ def main():
             e2e_ms.append(dt)
             e2e_parts.append(((t1 - t0) * 1e3, (t2 - t1) * 1e3, (t3 - t2) * 1e3))
     e2e = statistics.mean(e2e_ms)
+    if dist:
+        tt = torch.tensor([e2e], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e = float(tt.item())
     e2e_split = [statistics.mean(x[k] for x in e2e_parts) for k in range(3)]
     # where the first call's time goes: reverse-key build (mm_graph_prepare), first and second match
     torch.cuda.synchronize()
@@ -431,7 +455,7 @@ def main():
                   "ms_match_again": (tp[3] - tp[2]) * 1e3}
     h2d = g.n * 8 + g.nnz * 4 + (g.nnz * 4 if weighted else 0) + 255 * 4
     d2h = g.n * 4
-    e2e_value = edges * world / (e2e / 1e3)
+    e2e_value = edges_all / (e2e / 1e3)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -447,10 +471,12 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+int32", "data": "synthetic",
             "config": {"workload": args.workload, "n": g.n, "nnz": g.nnz, "type": t, "barrier": BARRIER,
-                       "graphs": 1 if batch is None else batch["count"],
-                       "srand": MATCH_SEED, "rounds": rounds, "parallelism": f"replicas x{world}",
+                       "graphs": 1 if batch is None else batch["total"],
+                       "srand": MATCH_SEED, "rounds": rounds,
+                       "parallelism": (f"replicas x{world}" if batch is None else
+                                       f"batch shards x{world} (graphs split by estimated entries, no collective)"),
                        "l2": "inputs > L2 (CSR > 1 GB) and a 512 MB L2 flush between steps"},
-            "ms_to_maximal": ms, "edges_per_step": edges,
+            "ms_to_maximal": ms, "edges_per_step": edges_all,
             "e2e": {"value": e2e_value, "unit": "edges/s", "ms_per_step": e2e, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_create": e2e_split[0], "ms_first_match": e2e_split[1],
                     "ms_destroy": e2e_split[2], **e2e_detail},

@@ -422,6 +422,31 @@ class DeviceGraph:
         return rounds.value, ms[:executed], launches.value
 
 
+def shard_batch(sizes, world: int) -> list:
+    """Split a batch of independent graphs 0..len(sizes)-1 over `world` GPUs:
+    contiguous index ranges [lo, hi), one per rank, of about equal total size
+    (sizes: each graph's adjacency entries, or an estimate).  Every rank
+    computes the same split from the same sizes, so no message is exchanged,
+    and the graphs never cross ranks, so matching needs no collective.  Each
+    cut is placed at the graph boundary nearest to its share of the total."""
+    if world < 1:
+        raise ValueError("world must be at least 1")
+    s = np.asarray(sizes, dtype=np.float64).reshape(-1)
+    if (s < 0).any() or not np.isfinite(s).all():
+        raise ValueError("sizes must be finite and non-negative")
+    m = s.size
+    cum = np.concatenate([[0.0], np.cumsum(s)])
+    bounds = [0]
+    for k in range(1, world):
+        target = cum[-1] * k / world
+        b = min(int(np.searchsorted(cum, target, side="left")), m)
+        if b > 0 and target - cum[b - 1] <= cum[b] - target:
+            b -= 1
+        bounds.append(max(b, bounds[-1]))
+    bounds.append(m)
+    return [(bounds[k], bounds[k + 1]) for k in range(world)]
+
+
 def multilevel(g, type_: int, seeds: np.ndarray, target: float = 0.01, device: int = 0,
                barrier: int = DEFAULT_BARRIER, max_levels: int = 64) -> list:
     """Multilevel coarsening: match (type_), contract, repeat until at most
