@@ -58,6 +58,18 @@ def constant_policy(p: float = P0) -> np.ndarray:
     return w
 
 
+def hand_built(feature: int, k: float, centre: float = 0.0) -> np.ndarray:
+    """Weights of the policy p = sigmoid(logit(p0) + k * (x[feature] - centre)) for
+    a non-negative feature (one hidden unit passes it through): e.g. feature 0
+    (log2(1 + degree)) splits neighbours of different degree, feature 4 (the
+    round) makes a schedule.  For probing what the colouring can change."""
+    w = np.zeros(N_FLOATS, dtype=np.float32)
+    w[feature] = 1.0                   # W1[0][feature]: hidden 0 = relu(x[feature])
+    w[N_HID * N_FEAT + N_HID] = k      # W2[0]
+    w[-1] = np.float32(np.log(P0 / (1.0 - P0)) - k * centre)
+    return w
+
+
 def load_policy(path: Path = WEIGHTS) -> np.ndarray:
     w = np.fromfile(path, dtype=np.float32)
     if w.shape != (N_FLOATS,):

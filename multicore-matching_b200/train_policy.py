@@ -57,6 +57,8 @@ def main():
     ap.add_argument("--seeds", type=int, default=3)
     ap.add_argument("--es-iters", type=int, default=40)
     ap.add_argument("--eval-only", default="", help="evaluate these weights (a policy_mlp.f32) without training")
+    ap.add_argument("--hand-built", action="store_true",
+                    help="evaluate hand-built degree-split and round-schedule policies instead of training")
     args = ap.parse_args()
     mm = load_package()
     spec = importlib.util.spec_from_file_location("mm_policy", HERE / "policy.py")
@@ -67,6 +69,9 @@ def main():
     torch.cuda.set_device(0)
     type_ = 9
     seed_sets = [mm.rand_seeds(12345 + 1000 * k, 255) for k in range(args.seeds)]
+    if args.hand_built:
+        probe_hand_built(mm, pol, args, type_, seed_sets)
+        return
     if args.eval_only:
         w2 = pol.load_policy(Path(args.eval_only))
         lines = [json.dumps({"weights": args.eval_only})]
@@ -134,6 +139,53 @@ def main():
             "leave_rate_plain_traces": float(Y.mean()), "held_out_objective": scores, "picked": pick}
     lines = [json.dumps(info)]
     evaluate_all(mm, pol, args, type_, seed_sets, w2, lines)
+
+
+def probe_hand_built(mm, pol, args, type_, seed_sets):
+    """Totals over the evaluation hierarchies for p0 (through the policy kernel)
+    and hand-built policies: p = sigmoid(logit(p0) + k * (log2(1 + degree) - 3.9))
+    and p = sigmoid(logit(p0) + k * round / 32)."""
+    import torch
+
+    cands = {"p0": pol.constant_policy()}
+    for k in (-3.0, -1.5, 1.5, 3.0):
+        cands[f"degree k={k:+.1f}"] = pol.hand_built(0, k, 3.9)
+    for k in (-1.0, 1.0):
+        cands[f"round k={k:+.1f}"] = pol.hand_built(4, k)
+    seeds = mm.rand_seeds(12345, 255)
+    ne = 1 << args.eval_scale
+    lines = []
+    for g in (mm.Graph.rgg(ne, 13.0, seed=7), mm.Graph.rmat(args.eval_scale, 16, seed=1)):
+        levels = pol.hierarchy(mm, g, type_, seed_sets[0])
+        tot = {k: {"rounds": 0, "ms": 0.0, "weight": 0.0, "maximal": True} for k in ("plain", *cands)}
+        for level, lg in enumerate(levels):
+            with mm.DeviceGraph(lg, device=0) as dg:
+                dg.prepare(type_)
+                out = torch.empty(max(lg.n, 1), dtype=torch.int32, device="cuda")
+                for name in tot:
+                    best, r = 1e30, 0
+                    for _ in range(3):
+                        a = torch.cuda.Event(enable_timing=True)
+                        b = torch.cuda.Event(enable_timing=True)
+                        a.record()
+                        if name == "plain":
+                            r = dg.match_device(type_, seeds, out.data_ptr())
+                        else:
+                            r = dg.match_policy(type_, seeds, out.data_ptr(), cands[name], float(level))
+                        b.record()
+                        torch.cuda.synchronize()
+                        best = min(best, a.elapsed_time(b))
+                    chk = dg.check(out.data_ptr())
+                    tot[name]["rounds"] += r
+                    tot[name]["ms"] += best
+                    tot[name]["weight"] += dg.weight(out.data_ptr())[0]
+                    tot[name]["maximal"] &= bool(chk["valid"] and chk["matchable"] == 0)
+        log(f"hand-built policies on {g.name}")
+        lines.append(json.dumps({"graph": g.name, "levels": len(levels), "total": tot}))
+    text = "\n".join(lines)
+    if args.report:
+        Path(args.report).write_text(text + "\n")
+    print(text)
 
 
 def evaluate_all(mm, pol, args, type_, seed_sets, w2, lines):

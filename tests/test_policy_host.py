@@ -84,3 +84,13 @@ def test_es_refine_improves_a_quadratic(pol):
     start = float((target ** 2).sum())
     assert float(((centre - target) ** 2).sum()) < 0.5 * start
     assert float(((best - target) ** 2).sum()) < start
+
+
+def test_hand_built_policy(pol):
+    w = pol.hand_built(0, 2.0, 3.0)
+    X = np.zeros((3, 6), np.float32)
+    X[:, 0] = [3.0, 4.0, 2.0]
+    p = pol.policy_prob(w, X)
+    logit = np.log(pol.P0 / (1 - pol.P0))
+    want = 1 / (1 + np.exp(-(logit + 2.0 * (X[:, 0] - 3.0))))
+    assert np.allclose(p, np.clip(want, pol.P_MIN, pol.P_MAX), atol=1e-6)
