@@ -233,7 +233,9 @@ mm_status mm_match_batch(mm_graph *g, int type, uint32_t barrier, const uint32_t
  * for every vertex coloured in round r < trace_rounds, at [(r * n + v) * 8]:
  * its 6 features, its colour (1 blue, 0 red) and 1 if it left the active set
  * in that round (matched, or retired as unmatchable: match value 2); entries
- * of vertices not coloured keep their contents.
+ * of vertices not coloured keep their contents.  On a graph marked as a batch
+ * (mm_graph_set_batch) every graph's slice is a valid matching of that graph
+ * in its own numbering, and *rounds_out is the rounds of the whole launch.
  */
 #define MM_POLICY_FLOATS 129
 mm_status mm_match_policy(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds,
