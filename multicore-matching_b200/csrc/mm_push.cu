@@ -525,8 +525,10 @@ __device__ void init_phase(const Params &p, Smem &sm)
                 ++act;
                 blue_n += blue;
                 // no neighbours: unmatchable as soon as it is blue (learned
-                // colouring: at once, whatever its colour)
-                if ((blue || kPolicy) && deg == 0) {
+                // colouring on the symmetric path: at once, whatever its colour;
+                // elsewhere another list may still name it, and a blue vertex
+                // there must keep seeing it red)
+                if ((blue || (kPolicy && p.sym)) && deg == 0) {
                     p.col[v] = kDead;
                     p.ctl->match[v] = 2;
                     trace_left<kPolicy>(p, 0, v);

@@ -103,3 +103,47 @@ def test_zero_policy_gives_the_plain_matching(mm, orc, torch_cuda, type_):
             assert np.array_equal(ma[ma >= 4], mb[mb >= 4]), g.name
             if type_ in (7, 9):
                 assert np.array_equal(ma, mb) and r_pol <= r_plain, (g.name, r_pol, r_plain)
+
+
+@pytest.mark.parametrize("type_", [6, 7, 8, 9])
+def test_zero_policy_is_the_plain_matching_off_the_symmetric_path(mm, orc, torch_cuda, type_):
+    """On a CSR that does not take the symmetric path (asymmetric entries,
+    duplicates, self-loops, shuffled and gapped ranges) nothing retires early,
+    so the zero policy (p = 1/2 exactly, barrier 0x80000000) gives exactly the
+    plain result: every match value and the round count."""
+    from graphs_small import random_graph
+
+    seeds = orc.rand_seeds(4242, 256)
+    w = np.zeros(mm.POLICY_FLOATS, np.float32)
+    rng = np.random.default_rng(17)
+    for i in range(6):
+        g = random_graph(rng, int(rng.integers(50, 3000)), avg_deg=float(rng.uniform(1.0, 8.0)),
+                         symmetric=False, shuffle_ranges=i % 2 == 0, gaps=i % 3 == 0)
+        with mm.DeviceGraph(g, device=0) as dg:
+            a = torch_cuda.empty(g.n, dtype=torch_cuda.int32, device="cuda")
+            b = torch_cuda.empty(g.n, dtype=torch_cuda.int32, device="cuda")
+            r_plain = dg.match_device(type_, seeds, a.data_ptr(), 0x80000000)
+            r_pol = dg.match_policy(type_, seeds, b.data_ptr(), w, 0.0, barrier=0x80000000)
+            ma, mb = a.cpu().numpy(), b.cpu().numpy()
+        assert r_pol == r_plain and np.array_equal(ma, mb), (i, g.n)
+        assert orc.check(g, mb)["valid"]
+
+
+def test_policy_on_a_batch_matches_every_graph(mm, orc, torch_cuda):
+    """On a batch every graph's slice is a valid maximal matching of that graph,
+    in its own numbering."""
+    seeds = orc.rand_seeds(99, 256)
+    graphs = [mm.Graph.rgg(2000, 13.0, seed=1), mm.Graph.grid(30, 20), mm.Graph.rmat(11, 16, seed=4),
+              mm.Graph.rgg(500, 6.0, seed=2)]
+    u, off = mm.Graph.union(graphs)
+    rng = np.random.default_rng(5)
+    mlp = (rng.standard_normal(mm.POLICY_FLOATS) * 0.5).astype(np.float32)
+    with mm.DeviceGraph(u, device=0) as dg:
+        dg.set_batch(off)
+        out = torch_cuda.empty(u.n, dtype=torch_cuda.int32, device="cuda")
+        rounds = dg.match_policy(9, seeds, out.data_ptr(), mlp, 1.0)
+        m = out.cpu().numpy()
+    assert rounds <= 255
+    for i, g in enumerate(graphs):
+        chk = orc.check(g, m[off[i]:off[i + 1]])
+        assert chk["valid"] and chk["matchable"] == 0, (i, g.name, chk)
