@@ -574,20 +574,30 @@ constexpr int kPerW = 2;
 // scan.  (Without symmetry an unmatched blue vertex could list it, and its
 // choice would depend on the timing of the retirement.)  Red items are taken from the top of the thread range down, so
 // on small rounds they run on threads that have no blue item.  Each list is
-// read 8 entries at a time, the batch's colour loads in flight together,
-// stopping after the first batch with an unmatched neighbour.
+// read 16 entries, then 8 at a time, each batch's colour loads in flight
+// together, stopping after the first batch with an unmatched neighbour (most
+// lists fit the first batch).  A retired vertex's worklist item is marked with
+// its id complemented, so the commit phase sees the retirement in the item it
+// loads anyway.
 template <bool kPolicy>
-__device__ __forceinline__ void retire_red(const Params &p, int t, int par)
+__device__ __forceinline__ void retire_red(const Params &p, int t, int par, int n_red)
 {
-    const int n_red = __ldcg(&p.ctl->cnt[par][kRed]);
-    const int4 *list = p.lists[par][kRed];
+    int4 *list = p.lists[par][kRed];
     const long long stride = (long long)gridDim.x * kThreads;
     const long long tid = stride - 1 - ((long long)blockIdx.x * kThreads + threadIdx.x);
     for (long long i = tid; i < n_red; i += stride) {
         const int4 it = __ldcg(list + i);
         if (degree_of(it) > kWin) continue;
         bool gone = true;
-        for (int j0 = it.y; gone && j0 < it.z; j0 += 8) {
+        {
+            int nb[16];
+#pragma unroll
+            for (int u = 0; u < 16; ++u) nb[u] = it.y + u < it.z ? __ldg(p.nbrs + it.y + u) : -1;
+#pragma unroll
+            for (int u = 0; u < 16; ++u)
+                if (nb[u] >= 0 && p.col[nb[u]] != kMatched) gone = false;
+        }
+        for (int j0 = it.y + 16; gone && j0 < it.z; j0 += 8) {
             int nb[8];
 #pragma unroll
             for (int u = 0; u < 8; ++u) nb[u] = j0 + u < it.z ? __ldg(p.nbrs + j0 + u) : -1;
@@ -598,6 +608,7 @@ __device__ __forceinline__ void retire_red(const Params &p, int t, int par)
         if (gone) {
             p.col[it.x] = kDead;
             p.ctl->match[it.x] = 2;
+            list[i].x = ~it.x;
             trace_left<kPolicy>(p, t, it.x);
         }
     }
@@ -608,6 +619,7 @@ __device__ void scan_window(const Params &p, int t, int par)
 {
     Ctl *ctl = p.ctl;
     const int n_blue = __ldcg(&ctl->cnt[par][kBlue]);
+    const int n_red = kPolicy ? __ldcg(&ctl->cnt[par][kRed]) : 0;  // read with n_blue: one round trip
     const int4 *list = p.lists[par][kBlue];
     const long long stride = (long long)gridDim.x * kThreads;
     for (long long i0 = (long long)blockIdx.x * kThreads + threadIdx.x; i0 < n_blue; i0 += stride * kPerW) {
@@ -708,7 +720,7 @@ __device__ void scan_window(const Params &p, int t, int par)
             }
         }
     }
-    if (kPolicy && p.sym && t >= kRetireFrom) retire_red<kPolicy>(p, t, par);
+    if (kPolicy && p.sym && t >= kRetireFrom) retire_red<kPolicy>(p, t, par, n_red);
 }
 
 // ---- phase A2: fallback lists, entry-balanced segments ----
@@ -940,7 +952,7 @@ __device__ void commit_phase(const Params &p, Smem &sm, int t, bool has_next)
     int retired = 0;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         int4 it[kPer];
-        bool in[kPer], blue[kPer];
+        bool in[kPer], blue[kPer], gone[kPer];
 #pragma unroll
         for (int k = 0; k < kPer; ++k) {
             const long long i = tile * kTileItems + k * kThreads + threadIdx.x;
@@ -948,6 +960,9 @@ __device__ void commit_phase(const Params &p, Smem &sm, int t, bool has_next)
             blue[k] = i < c0;
             it[k] = make_int4(0, 0, 0, 0);
             if (in[k]) it[k] = blue[k] ? __ldcg(p.lists[par][kBlue] + i) : __ldcg(p.lists[par][kRed] + (i - c0));
+            // learned colouring: a red item retired in phase A carries its id complemented
+            gone[k] = kPolicy && in[k] && !blue[k] && it[k].x < 0;
+            if (gone[k]) it[k].x = ~it[k].x;
         }
         // proposal state: blue -> its request, red -> the best proposal it received
         int2 q[kPer];
@@ -1012,7 +1027,7 @@ __device__ void commit_phase(const Params &p, Smem &sm, int t, bool has_next)
                 continue;
             }
             // unmatchable (marked in phase A; learned colouring: red ones too)
-            if ((blue[k] && q[k].x == -1) || (kPolicy && !blue[k] && __ldcg(p.col + v) == kDead)) {
+            if ((blue[k] && q[k].x == -1) || gone[k]) {
                 trace_left<kPolicy>(p, t, v);
                 continue;
             }
