@@ -54,6 +54,7 @@
 #include <cub/device/device_scan.cuh>
 
 #include <cstddef>
+#include <cmath>
 #include <cstring>
 #include <new>
 
@@ -130,6 +131,10 @@ struct Params {
     // thread reads the same one, so the unrolled MLP takes them straight from
     // the constant bank as operands, with no load instruction per weight.
     float mlp[MM_POLICY_FLOATS];
+    // A policy whose output weights are all zero ignores the features: its
+    // threshold, computed once on the host, is policy_bar (policy_const = 1).
+    int policy_const;
+    uint32_t policy_bar;
 };
 static_assert(sizeof(Params) <= 4096, "launch parameters stay within the classic 4 KB limit");
 
@@ -416,6 +421,13 @@ __device__ __forceinline__ uint32_t policy_barrier(const Params &p, const float 
 }
 
 // Colour of vertex v for round t: the select barrier, or the policy's.
+// Whether colouring round t needs the features: a policy that ignores them
+// needs them only for the trace.
+__device__ __forceinline__ bool policy_needs_features(const Params &p, int t)
+{
+    return !p.policy_const || (p.trace && t < p.trace_rounds);
+}
+
 template <bool kPolicy>
 __device__ __forceinline__ bool colour_blue(const Params &p, int v, int deg, float role, float2 wf, int t,
                                             uint32_t seed, uint32_t barrier)
@@ -423,8 +435,8 @@ __device__ __forceinline__ bool colour_blue(const Params &p, int v, int deg, flo
     uint32_t bar = barrier;
     if (kPolicy) {
         float x[kFeat];
-        policy_features(p, wf, deg, role, t, x);
-        bar = policy_barrier(p, x);
+        if (policy_needs_features(p, t)) policy_features(p, wf, deg, role, t, x);
+        bar = p.policy_const ? p.policy_bar : policy_barrier(p, x);
         const bool blue = colour_of((uint32_t)(v - base_of(p, v)), seed, bar) == kBlue;
         if (p.trace && t < p.trace_rounds) {
             float *row = p.trace + ((size_t)t * p.n + v) * kTraceCols;
@@ -514,7 +526,7 @@ __device__ void init_phase(const Params &p, Smem &sm)
                 item[k].z = r.y;
                 if (kW) item[k].w = (int)__ldg(p.pwin_off + v);
                 const int deg = degree_of(r);
-                const float2 wf = kPolicy ? __ldg(p.wfeat + v) : make_float2(0.0f, 0.0f);
+                const float2 wf = kPolicy && policy_needs_features(p, 0) ? __ldg(p.wfeat + v) : make_float2(0.0f, 0.0f);
                 const bool blue = colour_blue<kPolicy>(p, v, deg, 0.0f, wf, 0, seed, barrier);
                 if (p.last) p.last[v] = 0;
                 p.best[v] = 0ull;
@@ -1037,7 +1049,8 @@ __device__ void commit_phase(const Params &p, Smem &sm, int t, bool has_next)
                 continue;
             }
             const float role = blue[k] ? (q[k].y != 0 ? 1.0f : 0.5f) : 0.0f;
-            const float2 wf = kPolicy ? __ldg(p.wfeat + v) : make_float2(0.0f, 0.0f);
+            const float2 wf =
+                kPolicy && policy_needs_features(p, t + 1) ? __ldg(p.wfeat + v) : make_float2(0.0f, 0.0f);
             const bool nb = colour_blue<kPolicy>(p, v, deg, role, wf, t + 1, next_seed, barrier);
             if (p.last) p.last[v] = (uint8_t)(t + 1);
             ++act;
@@ -1789,6 +1802,8 @@ Params make_params(mm_graph *g, PushState *s, bool weighted, bool stats, bool ti
     p.vbase = g->ngraphs > 0 ? g->d_vbase : nullptr;
     p.last = g->ngraphs > 0 ? g->d_last : nullptr;
     std::memset(p.mlp, 0, sizeof(p.mlp));
+    p.policy_const = 0;
+    p.policy_bar = 0u;
     p.level = 0.0f;
     p.wfeat = s->wfeat;
     p.trace = nullptr;
@@ -1803,6 +1818,8 @@ Params make_params(mm_graph *g, PushState *s, bool weighted, bool stats, bool ti
 
 struct PolicyArgs {
     const float *mlp = nullptr;  // host, MM_POLICY_FLOATS
+    bool constant = false;       // output weights all zero: the threshold is constant_bar
+    uint32_t constant_bar = 0u;
     float level = 0.0f;
     float *trace = nullptr;
     int trace_rounds = 0;
@@ -1814,6 +1831,8 @@ mm_status launch_rounds(mm_graph *g, PushState *s, bool timing, cudaStream_t str
     Params prm = make_params(g, s, kW, kStats, timing);
     if (kPolicy) {
         std::memcpy(prm.mlp, pol->mlp, sizeof(prm.mlp));
+        prm.policy_const = pol->constant ? 1 : 0;
+        prm.policy_bar = pol->constant_bar;
         prm.level = pol->level;
         prm.trace = pol->trace;
         prm.trace_rounds = pol->trace_rounds;
@@ -2255,6 +2274,19 @@ mm_status push_match_policy(mm_graph *g, int type, uint32_t barrier, const uint3
     MM_CUDA_TRY(cudaMemsetAsync(s->bar, 0, sizeof(unsigned) * kBarWords, stream), "barrier clear");
     PolicyArgs pol;
     pol.mlp = mlp_host;
+    // the output layer's weights W2 (after W1 and b1): all zero means every
+    // vertex gets sigmoid(b2), the same clamp and scaling as on the device
+    {
+        constexpr int kW2 = kHid * kFeat + kHid;
+        bool zero = true;
+        for (int j = 0; j < kHid; ++j) zero = zero && mlp_host[kW2 + j] == 0.0f;
+        if (zero) {
+            float prob = 1.0f / (1.0f + std::exp(-mlp_host[kW2 + kHid]));
+            prob = std::fmin(std::fmax(prob, 1.0f / 16.0f), 15.0f / 16.0f);
+            pol.constant = true;
+            pol.constant_bar = (uint32_t)((double)prob * 4294967296.0);
+        }
+    }
     pol.level = level;
     pol.trace = trace;
     pol.trace_rounds = trace ? trace_rounds : 0;

@@ -147,3 +147,19 @@ def test_policy_on_a_batch_matches_every_graph(mm, orc, torch_cuda):
     for i, g in enumerate(graphs):
         chk = orc.check(g, m[off[i]:off[i + 1]])
         assert chk["valid"] and chk["matchable"] == 0, (i, g.name, chk)
+
+
+def test_policy_that_ignores_its_features_is_constant(mm, orc, torch_cuda):
+    """Random hidden weights behind an all-zero output layer give the same
+    probability everywhere, so the same matching as the all-zero policy."""
+    seeds = orc.rand_seeds(31, 256)
+    rng = np.random.default_rng(8)
+    w = (rng.standard_normal(mm.POLICY_FLOATS) * 2.0).astype(np.float32)
+    w[6 * 16 + 16:] = 0.0  # W2 and b2
+    g = mm.Graph.rgg(1 << 13, 13.0, seed=12)
+    with mm.DeviceGraph(g, device=0) as dg:
+        a = torch_cuda.empty(g.n, dtype=torch_cuda.int32, device="cuda")
+        b = torch_cuda.empty(g.n, dtype=torch_cuda.int32, device="cuda")
+        ra = dg.match_policy(9, seeds, a.data_ptr(), w, 0.0)
+        rb = dg.match_policy(9, seeds, b.data_ptr(), np.zeros(mm.POLICY_FLOATS, np.float32), 0.0)
+        assert ra == rb and np.array_equal(a.cpu().numpy(), b.cpu().numpy())
