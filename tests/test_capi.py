@@ -91,3 +91,20 @@ def test_generator_shapes(mm):
     m = mm.Graph.rmat(14, 16, seed=1)
     deg = m.degrees()
     assert deg.max() > 50 * max(1.0, deg.mean())  # power-law skew
+
+
+def test_policy_layout_and_argument_errors(mm):
+    import importlib
+
+    text = (ROOT / "include" / "mm_match.h").read_text()
+    floats = int(re.search(r"#define MM_POLICY_FLOATS (\d+)", text).group(1))
+    pol = importlib.import_module("multicore-matching_b200.policy")
+    assert floats == mm.POLICY_FLOATS == pol.N_FLOATS
+    assert (ROOT / "multicore-matching_b200" / "policy_mlp.f32").stat().st_size == 4 * floats
+    lib = mm.lib()
+    r = ctypes.c_int()
+    seeds = (ctypes.c_uint32 * 4)(1, 2, 3, 4)
+    w = (ctypes.c_float * floats)()
+    # no graph, then no weights: argument errors (MM_ERR_ARG) before any device work
+    assert lib.mm_match_policy(None, 9, 0, seeds, 4, w, ctypes.c_float(0.0), None, ctypes.byref(r), None, 0,
+                               None) == 1
