@@ -224,7 +224,7 @@ mm_status mm_match_batch(mm_graph *g, int type, uint32_t barrier, const uint32_t
  * level / 16 (the caller's coarsening level).  The probability is clamped to
  * [1/16, 15/16], so the maximal types finish inside the round cap whatever
  * the weights.  On graphs that take the symmetric path, from round 3 on, a
- * red vertex of at most 32 entries whose neighbours are all matched leaves in
+ * red vertex of at most 128 entries whose neighbours are all matched leaves in
  * that round (the reference waits until it is coloured blue); the matching is
  * the same as the one the same colours give without that.  mlp: MM_POLICY_FLOATS host
  * floats, W1[16][6], b1[16], W2[16], b2.  The result is a valid matching

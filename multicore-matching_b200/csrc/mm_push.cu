@@ -383,7 +383,8 @@ struct Smem {
 constexpr int kFeat = 6, kHid = 16;
 static_assert(kHid * kFeat + kHid + kHid + 1 == MM_POLICY_FLOATS, "policy layout");
 constexpr int kTraceCols = 8;  // features, colour (1 blue, 0 red), left the active set in that round
-constexpr int kRetireFrom = 3;  // learned colouring: first round in which red vertices retire
+constexpr int kRetireFrom = 3;      // learned colouring: first round in which red vertices retire
+constexpr int kRetireMaxDeg = 128;  // learned colouring: longest list a red vertex checks
 
 // Trace: vertex v left the active set in round t (matched, or blue with no
 // unmatched neighbour and so retired).
@@ -578,19 +579,20 @@ __device__ void init_phase(const Params &p, Smem &sm)
 constexpr int kPerW = 2;
 
 // Learned colouring, graphs with symmetric structure: a red vertex of at most
-// kWin entries whose neighbours are all matched leaves in phase A of this
-// round, while the blue vertices scan (the reference waits until it is
+// kRetireMaxDeg entries whose neighbours are all matched leaves in phase A of
+// this round, while the blue vertices scan (the reference waits until it is
 // coloured blue and scans).  Colours do not change during phase A, so the
 // check is exact, and no vertex reads the retired one's colour: every vertex
 // that lists it is its neighbour, hence matched, and matched vertices do not
 // scan.  (Without symmetry an unmatched blue vertex could list it, and its
-// choice would depend on the timing of the retirement.)  Red items are taken from the top of the thread range down, so
-// on small rounds they run on threads that have no blue item.  Each list is
-// read 16 entries, then 8 at a time, each batch's colour loads in flight
-// together, stopping after the first batch with an unmatched neighbour (most
-// lists fit the first batch).  A retired vertex's worklist item is marked with
-// its id complemented, so the commit phase sees the retirement in the item it
-// loads anyway.
+// choice would depend on the timing of the retirement.)  Red items are taken
+// from the top of the thread range down, so on small rounds they run on
+// threads that have no blue item.  Each list is read 16 entries at a time,
+// each batch's colour loads in flight together, stopping after the first batch
+// with an unmatched neighbour (most lists fit the first batch).  A limit of
+// 128 entries cut R-MAT rounds further than 32 did; 512 cut no more and cost
+// time.  A retired vertex's worklist item is marked with its id complemented,
+// so the commit phase sees the retirement in the item it loads anyway.
 template <bool kPolicy>
 __device__ __forceinline__ void retire_red(const Params &p, int t, int par, int n_red)
 {
@@ -599,7 +601,7 @@ __device__ __forceinline__ void retire_red(const Params &p, int t, int par, int 
     const long long tid = stride - 1 - ((long long)blockIdx.x * kThreads + threadIdx.x);
     for (long long i = tid; i < n_red; i += stride) {
         const int4 it = __ldcg(list + i);
-        if (degree_of(it) > kWin) continue;
+        if (degree_of(it) > kRetireMaxDeg) continue;
         bool gone = true;
         {
             int nb[16];
@@ -609,12 +611,12 @@ __device__ __forceinline__ void retire_red(const Params &p, int t, int par, int 
             for (int u = 0; u < 16; ++u)
                 if (nb[u] >= 0 && p.col[nb[u]] != kMatched) gone = false;
         }
-        for (int j0 = it.y + 16; gone && j0 < it.z; j0 += 8) {
-            int nb[8];
+        for (int j0 = it.y + 16; gone && j0 < it.z; j0 += 16) {
+            int nb[16];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) nb[u] = j0 + u < it.z ? __ldg(p.nbrs + j0 + u) : -1;
+            for (int u = 0; u < 16; ++u) nb[u] = j0 + u < it.z ? __ldg(p.nbrs + j0 + u) : -1;
 #pragma unroll
-            for (int u = 0; u < 8; ++u)
+            for (int u = 0; u < 16; ++u)
                 if (nb[u] >= 0 && p.col[nb[u]] != kMatched) gone = false;
         }
         if (gone) {

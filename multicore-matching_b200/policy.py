@@ -4,7 +4,7 @@ The reference colours every vertex blue with one probability, the select
 barrier (0x88B81733 / 2^32 = 0.534, bin/match.cpp:183).  mm_match_policy lets a
 per-vertex MLP (6 -> 16 -> 1) choose that probability from local features
 (FEATURES below), and on graphs with symmetric structure retires, from round 3
-on, a red vertex of at most 32 entries as soon as none of its neighbours is
+on, a red vertex of at most 128 entries as soon as none of its neighbours is
 unmatched, instead of waiting until it is coloured blue.
 
 Training has two stages.
