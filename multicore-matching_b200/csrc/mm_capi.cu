@@ -520,27 +520,36 @@ mm_status check_match_args(mm_graph *g, int type, const uint32_t *seeds, int nse
 // ---- batches of independent graphs ----
 // vbase[v] = first vertex of v's graph (a warp per graph), then every entry
 // must stay inside its vertex's graph: the union is disjoint.
-__global__ void k_batch_vbase(const int *goff, int ngraphs, int *vbase)
+// vbase[v]: the first vertex of v's graph; vend[v]: one past its last.
+__global__ void k_batch_vbase(const int *goff, int ngraphs, int *vbase, int *vend)
 {
     const int lane = threadIdx.x & 31;
     const long long gwarp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long gi = gwarp; gi < ngraphs; gi += nwarps)
-        for (int v = goff[gi] + lane; v < goff[gi + 1]; v += 32) vbase[v] = goff[gi];
+    for (long long gi = gwarp; gi < ngraphs; gi += nwarps) {
+        const int lo = goff[gi], hi = goff[gi + 1];
+        for (int v = lo + lane; v < hi; v += 32) {
+            vbase[v] = lo;
+            vend[v] = hi;
+        }
+    }
 }
 
-__global__ void k_batch_edges(const int2 *ranges, const int *nbrs, const int *vbase, int n, int *bad)
+// Every entry of vertex v must name a vertex of v's own graph [vbase[v],
+// vend[v]): a comparison per entry, a thread per vertex (neighbouring vertices'
+// lists are neighbours in memory, so the pass streams), with no gather.
+__global__ void k_batch_edges(const int2 *ranges, const int *nbrs, const int *vbase, const int *vend, int n, int *bad)
 {
-    const int lane = threadIdx.x & 31;
-    const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long v = warp0; v < n; v += nwarps) {
+    int cross = 0;
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
         const int2 r = ranges[v];
-        const int b = vbase[v];
-        int cross = 0;
-        for (int j = r.x + lane; j < r.y; j += 32) cross |= vbase[nbrs[j]] != b;
-        if (__any_sync(0xffffffffu, cross) && lane == 0) atomicOr(bad, 1);
+        const int lo = vbase[v], hi = vend[v];
+        for (int j = r.x; j < r.y; ++j) {
+            const int u = __ldg(nbrs + j);
+            cross |= u < lo || u >= hi;
+        }
     }
+    if (__any_sync(0xffffffffu, cross) && (threadIdx.x & 31) == 0) atomicOr(bad, 1);
 }
 
 // ---- measurement: random-gather ceiling ----
@@ -750,25 +759,27 @@ MM_API mm_status mm_graph_set_batch(mm_graph *g, int ngraphs, const int *offsets
             return MM_ERR_ARG;
         }
     DeviceGuard guard(g->device);
-    int *goff = nullptr, *vbase = nullptr, *bad = nullptr;
+    int *goff = nullptr, *vbase = nullptr, *vend = nullptr, *bad = nullptr;
     uint8_t *last = nullptr;
     const size_t nv = (size_t)(g->n > 0 ? g->n : 1);
     cudaError_t e = dev_alloc((void **)&goff, sizeof(int) * ((size_t)ngraphs + 1), 0);
     if (e == cudaSuccess) e = dev_alloc((void **)&vbase, sizeof(int) * nv, 0);
+    if (e == cudaSuccess) e = dev_alloc((void **)&vend, sizeof(int) * nv, 0);  // for the check only
     if (e == cudaSuccess) e = dev_alloc((void **)&last, nv, 0);
     if (e == cudaSuccess) e = dev_alloc((void **)&bad, sizeof(int), 0);
     if (e == cudaSuccess) e = cudaMemsetAsync(bad, 0, sizeof(int), 0);
     if (e == cudaSuccess) e = cudaMemcpyAsync(goff, offsets, sizeof(int) * ((size_t)ngraphs + 1), cudaMemcpyHostToDevice, 0);
     if (e == cudaSuccess) {
-        k_batch_vbase<<<grid_for((long long)ngraphs * 32, 256, 148 * 8), 256>>>(goff, ngraphs, vbase);
+        k_batch_vbase<<<grid_for((long long)ngraphs * 32, 256, 148 * 8), 256>>>(goff, ngraphs, vbase, vend);
         if (g->n > 0)
-            k_batch_edges<<<grid_for((long long)g->n * 32, 256, 148 * 16), 256>>>(g->d_ranges, g->d_nbrs, vbase, g->n,
-                                                                                bad);
+            k_batch_edges<<<grid_for((long long)g->n, 256, 148 * 16), 256>>>(g->d_ranges, g->d_nbrs, vbase, vend,
+                                                                           g->n, bad);
         e = cudaGetLastError();
     }
     int hbad = 0;
     if (e == cudaSuccess) e = cudaMemcpy(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost);
     dev_free(bad, 0);
+    dev_free(vend, 0);
     if (e != cudaSuccess || hbad) {
         dev_free(goff, 0);
         dev_free(vbase, 0);
