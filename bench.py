@@ -437,21 +437,28 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e = float(tt.item())
     e2e_split = [statistics.mean(x[k] for x in e2e_parts) for k in range(3)]
-    # where the first call's time goes: reverse-key build (mm_graph_prepare), first and second match
-    torch.cuda.synchronize()
+    # where one step's time goes, each call followed by a device synchronisation: upload,
+    # batch set-up, reverse-key build (mm_graph_prepare), first and second match
+    def synced():
+        torch.cuda.synchronize()
+        return time.perf_counter()
+
     h = ctypes.c_void_p()
+    ts = [synced()]
     mm._check(lib.mm_graph_create(g.n, ranges_h.data_ptr(), g.nnz, nbrs_h.data_ptr(),
                                   None if w_h is None else w_h.data_ptr(), local, ctypes.byref(h)))
+    ts.append(synced())
     if batch is not None:
         mm._check(lib.mm_graph_set_batch(h, len(batch["offsets"]) - 1, batch["offsets"].ctypes.data))
-    tp = [time.perf_counter()]
+    tp = [synced()]
     mm._check(lib.mm_graph_prepare(h, t))
-    tp.append(time.perf_counter())
+    tp.append(synced())
     for _ in range(2):
         mm._check(lib.mm_match(h, t, BARRIER, sd.ctypes.data, len(sd), match_h.data_ptr(), ctypes.byref(rr), None))
-        tp.append(time.perf_counter())
+        tp.append(synced())
     lib.mm_graph_destroy(h)
-    e2e_detail = {"ms_prepare": (tp[1] - tp[0]) * 1e3, "ms_match_first": (tp[2] - tp[1]) * 1e3,
+    e2e_detail = {"ms_create_synced": (ts[1] - ts[0]) * 1e3, "ms_set_batch_synced": (tp[0] - ts[1]) * 1e3,
+                  "ms_prepare": (tp[1] - tp[0]) * 1e3, "ms_match_first": (tp[2] - tp[1]) * 1e3,
                   "ms_match_again": (tp[3] - tp[2]) * 1e3}
     h2d = g.n * 8 + g.nnz * 4 + (g.nnz * 4 if weighted else 0) + 255 * 4
     d2h = g.n * 4
