@@ -142,6 +142,8 @@ class ClockSampler:
         self.dev = device_index
         self.proc = None
         self.lines = []
+        self.started = threading.Event()
+        self.t0 = None  # samples that arrive from here on are inside the timed region
 
     def __enter__(self):
         try:
@@ -150,13 +152,20 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # nvidia-smi takes a moment to start: wait for its first line, so the
+            # timed region is sampled from its first step
+            self.started.wait(timeout=2.0)
         except (OSError, FileNotFoundError):
             self.proc = None
+        self.t0 = time.perf_counter()
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            now = time.perf_counter()
+            if self.t0 is not None and now >= self.t0:
+                self.lines.append(line.strip())
+            self.started.set()
 
     def __exit__(self, *exc):
         if self.proc:
@@ -293,7 +302,8 @@ def cpu_baseline(mm, g, t, gpu_match, workload, batch=None):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 400; 20 for --impl reference, whose steps are CPU matchings)")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -302,6 +312,8 @@ def main():
     ap.add_argument("--ncu-case", action="store_true",
                     help="build + prepare, then one host-stepped matching only (for ncu captures of the kernels)")
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 20 if args.impl == "reference" else 400
     args.warmup = max(args.warmup, 3)
     spec = WORKLOADS[args.workload]
     if args.impl == "reference":
