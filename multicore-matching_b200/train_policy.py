@@ -9,8 +9,11 @@ sequences.  Stage 1 fits the policy to traces of the plain colouring (every
 vertex blue with p0) by inverse propensity weighting inside a trust region
 around p0; stage 2 refines it on-policy by evolution strategies on the total
 rounds over the training hierarchies, penalising a matching weight more than
-0.5% below the plain method's.  The weights go to --out (policy_mlp.f32 next
-to this file by default).
+0.5% below the plain method's.  The pick among the candidates is made on
+held-out seeds; a pick other than the constant plain probability p0 must also
+beat p0 in device time on larger held-out hierarchies (--confirm-scale), since
+it evaluates the MLP at every colouring.  The weights go to --out
+(policy_mlp.f32 next to this file by default).
 
 Evaluation graphs (held out): RGG and R-MAT with 2^22 vertices and their plain
 hierarchies; per level, rounds, device time and matching weight of the plain
@@ -56,6 +59,8 @@ def main():
     ap.add_argument("--eval-scale", type=int, default=22)
     ap.add_argument("--seeds", type=int, default=3)
     ap.add_argument("--es-iters", type=int, default=40)
+    ap.add_argument("--confirm-scale", type=int, default=20,
+                    help="a pick other than p0 must also beat p0 in device time on hierarchies of this scale")
     ap.add_argument("--eval-only", default="", help="evaluate these weights (a policy_mlp.f32) without training")
     ap.add_argument("--hand-built", action="store_true",
                     help="evaluate hand-built degree-split and round-schedule policies instead of training")
@@ -130,13 +135,30 @@ def main():
         scores = {k: val_obj(w) for k, w in cands.items()}
         log(f"held-out objective (plain = -1): {scores}")
         pick = max(scores, key=scores.get)
-        w2 = cands[pick]
     finally:
         for dg in dgs:
             dg.close()
+    confirm = None
+    if pick != "retire_only":
+        # fewer rounds at the training scale is not enough: a policy that uses its
+        # features evaluates the MLP at every colouring, so it must also win on
+        # device time on larger held-out hierarchies, or p0 stays
+        nc = 1 << args.confirm_scale
+        ms = {"p0": 0.0, pick: 0.0}
+        for g in (mm.Graph.rgg(nc, 13.0, seed=7), mm.Graph.rmat(args.confirm_scale, 16, seed=1)):
+            rows = pol.evaluate(mm, pol.hierarchy(mm, g, type_, seed_sets[0]), type_, mm.rand_seeds(12345, 255),
+                                cands[pick])
+            ms["p0"] += sum(r["retire"]["ms"] for r in rows)
+            ms[pick] += sum(r["learned"]["ms"] for r in rows)
+        confirm = {"scale": args.confirm_scale, "ms": ms}
+        log(f"confirmation at 2^{args.confirm_scale}: {ms}")
+        if ms[pick] >= ms["p0"]:
+            pick = "retire_only"
+    w2 = cands[pick]
     w2.tofile(args.out)
     info = {"training_samples": int(len(X)), "training_graphs": [g.name for g in train_graphs],
-            "leave_rate_plain_traces": float(Y.mean()), "held_out_objective": scores, "picked": pick}
+            "leave_rate_plain_traces": float(Y.mean()), "held_out_objective": scores, "confirmation": confirm,
+            "picked": pick}
     lines = [json.dumps(info)]
     evaluate_all(mm, pol, args, type_, seed_sets, w2, lines)
 
