@@ -65,7 +65,7 @@ enum {
 };
 
 /* Number of int64 counters per round written by mm_match_stats. */
-#define MM_STATS_COLS 11
+#define MM_STATS_COLS 13
 enum {
     MM_ST_ACTIVE = 0,     /* vertices that could still be matched at the round's colouring */
     MM_ST_BLUE = 1,       /* of those, coloured blue */
@@ -77,7 +77,9 @@ enum {
     MM_ST_MATCHED = 7,    /* vertices matched in the round */
     MM_ST_STAGED_DEG = 8,   /* push path: entries its fallback (full-list) scan read */
     MM_ST_STAGED_ITEMS = 9, /* push path: list pieces that scan handled */
-    MM_ST_WINDOW_ENTRIES = 10 /* push path: preference-window entries the blue scans read */
+    MM_ST_WINDOW_ENTRIES = 10, /* push path: preference-window entries the blue scans read */
+    MM_ST_FINISH_ITEMS = 11,  /* push path: active vertices its finish phase classified (round it ran in) */
+    MM_ST_FINISH_ENTRIES = 12 /* push path: adjacency entries the finish phase's list scans read */
 };
 
 typedef struct mm_graph mm_graph;

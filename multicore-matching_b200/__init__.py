@@ -36,11 +36,11 @@ PATH_AUTO, PATH_PULL, PATH_PUSH = 0, 1, 2
 # Default select barrier of the reference CLI (bin/match.cpp:183): p(blue) ~ 0.534.
 DEFAULT_BARRIER = 0x88B81733
 
-STATS_COLS = 11
+STATS_COLS = 13
 POLICY_FLOATS = 129  # MM_POLICY_FLOATS: W1[16][6], b1[16], W2[16], b2
 PROFILE_KERNELS = 4  # window scan, fallback scan, commit/recolour, their sum
 (ST_ACTIVE, ST_BLUE, ST_RED, ST_REQ_ENTRIES, ST_RESP_ENTRIES, ST_BLUE_DEG, ST_RED_DEG, ST_MATCHED,
- ST_STAGED_DEG, ST_STAGED_ITEMS, ST_WINDOW_ENTRIES) = range(11)
+ ST_STAGED_DEG, ST_STAGED_ITEMS, ST_WINDOW_ENTRIES, ST_FINISH_ITEMS, ST_FINISH_ENTRIES) = range(13)
 
 STATUS = {0: "MM_OK", 1: "MM_ERR_ARG", 2: "MM_ERR_GRAPH", 3: "MM_ERR_CUDA", 4: "MM_ERR_NOMEM",
           5: "MM_ERR_UNSUPPORTED", 6: "MM_ERR_SEEDS", 7: "MM_ERR_DEVICE"}

@@ -86,6 +86,8 @@ struct Ctl {
     int cnt[2][kParityLists];      // worklist lengths by round parity
     unsigned long long staged_pack;  // fallback list of the round: (items << 32) | entries
     int retired[2];        // vertices of the round that were unmatchable as soon as coloured
+    int fin_abort;         // finish phase: t + 1 if the attempt in round t was called off
+    int fin_last;          // finish phase: last round in which any of its vertices was active
 };
 
 struct Params {
@@ -1085,6 +1087,437 @@ __device__ void commit_phase(const Params &p, Smem &sm, int t, bool has_next)
     if ((threadIdx.x & 31) == 0 && retired) atomicAdd(&ctl->retired[par ^ 1], retired);
 }
 
+// ---- finish phase ----
+//
+// After the first rounds the vertices that can still be matched form a sparse
+// subgraph: on R-MAT 2^23 at round 5, 334 k active vertices share 40 k entries
+// that point at another active vertex, and its connected components have at
+// most 7 members (grids, random geometric and Erdos-Renyi graphs reach the same
+// state by round 3).  A vertex's future depends only on the colours and choices
+// of the active vertices it can reach: matched neighbours never change, and on
+// the symmetric path no active vertex has an unmatchable neighbour (a vertex
+// became unmatchable because every neighbour was matched).  So each component
+// can play all its remaining rounds on its own, with the same seeds, and the
+// grid needs no further barrier.
+//
+// The phase runs at the start of round t in two passes over the round's
+// worklist items, each ended by a grid barrier:
+//   classify  every item scans its own list: no active neighbour (a singleton),
+//             an active neighbour with a smaller id (a member: another vertex
+//             speaks for its component), or else a root candidate, which
+//             searches its component with its warp (breadth first, at most
+//             kFinMembers members and kFinEntries entries between members).
+//             A larger component, a list longer than kFinMaxDeg or an
+//             unmatchable neighbour calls the attempt off (ctl->fin_abort),
+//             and round t runs as usual.
+//   resolve   a singleton walks its own hash sequence: it leaves (match value
+//             2) in the first round it is blue, or keeps red to the round cap.
+//             A root whose search finds no smaller member plays its component
+//             in its warp, lane l holding member l: colour, request (the best
+//             red neighbour by the same keys as the scans), respond (an
+//             atomic max of the proposal keys in shared memory), commit.
+// Every vertex's match value is then final, and the matching executed
+// max(last active round) + 2 rounds, the reference's closing round included
+// (at most the cap).
+constexpr int kFinMembers = 32;    // members of a component played by one warp (one per lane)
+constexpr int kFinEntries = 128;   // entries between members of one component
+constexpr int kFinShort = 32;      // lists a thread scans on its own; longer ones its warp scans
+constexpr int kFinMaxDeg = 2048;   // longest list the finish phase accepts
+constexpr int kFinDiv = 12;        // first attempt once the active set is at most 1/kFinDiv of round 0's
+enum : int { kFinSingle = 1, kFinMember = 2, kFinRootCand = 3 };
+enum : int { kFinNotRoot = 0, kFinRoot = 1, kFinTooBig = 2 };
+
+// One warp's component: members' first entry, list start and degree, the
+// entries between members (preference key and the target's member slot), the
+// members' colours of the round being played and the best proposal each
+// received.
+struct FinWarp {
+    unsigned long long pref[kFinEntries];
+    unsigned long long best[kFinMembers];
+    int eoff[kFinMembers + 1];
+    int mbeg[kFinMembers];
+    int mdeg[kFinMembers];
+    uint8_t tgt[kFinEntries];
+    uint8_t st[kFinMembers];
+};
+static_assert(sizeof(FinWarp) * kWarps <= sizeof(Smem), "the finish phase reuses the scan phases' shared memory");
+
+// Item i of round parity `par` (blue list first, then red).
+__device__ __forceinline__ int4 item_at(const Params &p, int par, int c0, long long i)
+{
+    return i < c0 ? __ldcg(p.lists[par][kBlue] + i) : __ldcg(p.lists[par][kRed] + (i - c0));
+}
+
+// Own-list scan of vertex v, entries [b, e): active neighbours (blue or red),
+// whether one has a smaller id, whether a neighbour is unmatchable.
+__device__ __forceinline__ void fin_scan_thread(const Params &p, int v, int b, int e, int &nint, bool &lower,
+                                                bool &bad)
+{
+    for (int j0 = b; j0 < e; j0 += 8) {
+        int u[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) u[k] = j0 + k < e ? __ldg(p.nbrs + j0 + k) : -1;
+        uint8_t c[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) c[k] = u[k] >= 0 ? p.col[u[k]] : (uint8_t)kMatched;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (c[k] <= kRed) {
+                ++nint;
+                lower |= u[k] < v;
+            }
+            bad |= c[k] == kDead;
+        }
+    }
+}
+
+// The same scan by a whole warp (lane-strided), for a list longer than kFinShort.
+__device__ __forceinline__ void fin_scan_warp(const Params &p, int v, int b, int e, int &nint, bool &lower,
+                                              bool &bad)
+{
+    const int lane = threadIdx.x & 31;
+    int cnt = 0;
+    bool lo = false, bd = false;
+    for (int j0 = b + lane; j0 < e; j0 += 32 * 4) {
+        int u[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) u[k] = j0 + 32 * k < e ? __ldg(p.nbrs + j0 + 32 * k) : -1;
+        uint8_t c[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) c[k] = u[k] >= 0 ? p.col[u[k]] : (uint8_t)kMatched;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (c[k] <= kRed) {
+                ++cnt;
+                lo |= u[k] < v;
+            }
+            bd |= c[k] == kDead;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(kFull, cnt, o);
+    nint = cnt;
+    lower = __any_sync(kFull, lo);
+    bad = __any_sync(kFull, bd);
+}
+
+// Component search for root candidate v by its warp.  Members are numbered in
+// discovery order (member 0 is v; lane l's `mem` holds member l); each
+// member's entries that point at a member are stored in order, from
+// fw.eoff[member].  Returns kFinNotRoot as soon as a member has a smaller id
+// than v, kFinTooBig if the component does not fit, else kFinRoot with *k
+// members.
+template <bool kW>
+__device__ __forceinline__ int fin_search(const Params &p, FinWarp &fw, int v, int *mem_out, int *k_out,
+                                          unsigned long long *scanned)
+{
+    const int lane = threadIdx.x & 31;
+    int mem = lane == 0 ? v : -1;
+    int k = 1, ne = 0;
+    unsigned long long seen = 0;
+    for (int f = 0; f < k; ++f) {
+        const int x = __shfl_sync(kFull, mem, f);
+        const int2 r = __ldg(p.ranges + x);
+        const int b = r.x, e = r.y > r.x ? r.y : r.x;
+        if (e - b > kFinMaxDeg) return kFinTooBig;
+        if (lane == 0) {
+            fw.eoff[f] = ne;
+            fw.mbeg[f] = b;
+            fw.mdeg[f] = e - b;
+        }
+        seen += (unsigned long long)(e - b);
+        for (int j0 = b; j0 < e; j0 += 32) {
+            const int j = j0 + lane;
+            int u = -1;
+            uint8_t c = kMatched;
+            if (j < e) {
+                u = __ldg(p.nbrs + j);
+                c = p.col[u];
+            }
+            const bool in = c <= kRed;
+            if (__any_sync(kFull, c == kDead)) return kFinTooBig;
+            if (__any_sync(kFull, in && u < v)) return kFinNotRoot;
+            unsigned m = __ballot_sync(kFull, in);
+            unsigned long long pref = 0;
+            if (in) pref = kW ? cand_key<true>(j, __ldg(p.w + j)) : (unsigned long long)(uint32_t)~j;
+            while (m) {
+                const int s = __ffs(m) - 1;
+                m &= m - 1;
+                const int us = __shfl_sync(kFull, u, s);
+                const unsigned hit = __ballot_sync(kFull, lane < k && mem == us);
+                int slot;
+                if (hit) {
+                    slot = __ffs(hit) - 1;
+                } else {
+                    if (k == kFinMembers) return kFinTooBig;
+                    slot = k;
+                    if (lane == k) mem = us;
+                    ++k;
+                }
+                if (ne == kFinEntries) return kFinTooBig;
+                if (lane == s) {
+                    fw.pref[ne] = pref;
+                    fw.tgt[ne] = (uint8_t)slot;
+                }
+                ++ne;
+            }
+        }
+    }
+    if (lane == 0) fw.eoff[k] = ne;
+    __syncwarp();
+    *mem_out = mem;
+    *k_out = k;
+    if (scanned) *scanned = seen;
+    return kFinRoot;
+}
+
+// Adjacency entries the reference's respond loop inspects for red vertex v
+// (entries [b, b + deg)) whose best proposal key is kb: in random mode it
+// stops at its first proposer in list order, here the proposer with the
+// smallest id (kb's low half complemented), found in the sorted list.
+template <bool kW>
+__device__ __forceinline__ unsigned long long respond_seen(const Params &p, int b, int deg, unsigned long long kb)
+{
+    if (kW || !kb) return (unsigned long long)deg;
+    const int first = (int)~(uint32_t)kb;
+    int lo = b, hi = b + deg;
+    while (lo < hi) {
+        const int mid = (int)(((long long)lo + hi) >> 1);
+        if (__ldg(p.nbrs + mid) < first) lo = mid + 1;
+        else hi = mid;
+    }
+    return (unsigned long long)(lo - b + 1);
+}
+
+// Play a component found by fin_search (k members, lane l = member l) from
+// round t0 until none of its members can be matched or the cap is reached;
+// writes every member's match value (and batch round marks).  Returns, in
+// every lane, the last round in which a member was active.
+template <bool kW, bool kStats>
+__device__ __forceinline__ int fin_play(const Params &p, FinWarp &fw, int t0, int cap, int mem, int k)
+{
+    const int lane = threadIdx.x & 31;
+    const bool own = lane < k;
+    const int g = own ? mem : 0;
+    const int base = own ? base_of(p, g) : 0;
+    const uint32_t hid = (uint32_t)(g - base);
+    const uint32_t bar = p.ctl->barrier;
+    int eb = 0, ee = 0, deg = 0, beg = 0;
+    if (own) {
+        eb = fw.eoff[lane];
+        ee = fw.eoff[lane + 1];
+        deg = fw.mdeg[lane];
+        beg = fw.mbeg[lane];
+        fw.best[lane] = 0ull;
+    }
+    bool act = own, blue = false;
+    int val = 0, lastr = -1;
+    __syncwarp();
+    for (int t = t0; t < cap && __any_sync(kFull, act); ++t) {
+        if (act) {
+            blue = colour_of(hid, p.seeds[t], bar) == kBlue;
+            lastr = t;
+        }
+        if (own) fw.st[lane] = act ? (blue ? kBlue : kRed) : (val == 2 ? kDead : kMatched);
+        __syncwarp();
+        // request: the best red neighbour among the members (matched ones
+        // outside the component neither attract nor keep a vertex alive)
+        unsigned long long best = 0ull;
+        int choice = 0;
+        if (act && blue) {
+            for (int e = eb; e < ee; ++e) {
+                const int tg = fw.tgt[e];
+                const uint8_t c = fw.st[tg];
+                const unsigned long long key = c == kRed ? fw.pref[e] : (c == kMatched ? 0ull : 1ull);
+                if (key > best) {
+                    best = key;
+                    choice = tg;
+                }
+            }
+        }
+        unsigned long long crk = 0ull;
+        if (act && blue && best >= 2) {
+            // the target's entry for this vertex has the same weight (symmetric path)
+            crk = kW ? (((best >> 32) << 32) | (unsigned long long)(uint32_t)~(uint32_t)g)
+                     : (unsigned long long)(uint32_t)~(uint32_t)g;
+            atomicMax(&fw.best[choice], crk);
+        }
+        __syncwarp();
+        const int gp = __shfl_sync(kFull, g, choice);
+        bool matched = false, dead = false;
+        unsigned long long kb = 0ull;
+        if (act) {
+            if (blue) {
+                if (best >= 2 && (uint32_t)fw.best[choice] == (uint32_t)crk) {
+                    val = 4 + min(g, gp) - base;
+                    matched = true;
+                } else if (best == 0) {
+                    val = 2;
+                    dead = true;
+                }
+            } else {
+                kb = fw.best[lane];
+                if (kb) {
+                    val = 4 + min(g, (int)~(uint32_t)kb) - base;
+                    matched = true;
+                }
+            }
+        }
+        if (kStats) {
+            const bool b = act && blue, r = act && !blue;
+            if (t > t0) {  // round t0's colouring was counted by the commit that made it
+                stat_add(p, t, MM_ST_ACTIVE, act ? 1ull : 0ull);
+                stat_add(p, t, MM_ST_BLUE, b ? 1ull : 0ull);
+                stat_add(p, t, MM_ST_RED, r ? 1ull : 0ull);
+            }
+            stat_add(p, t, MM_ST_BLUE_DEG, b ? (unsigned long long)deg : 0ull);
+            stat_add(p, t, MM_ST_RED_DEG, r ? (unsigned long long)deg : 0ull);
+            stat_add(p, t, MM_ST_REQ_ENTRIES,
+                     b ? request_seen<kW>(beg, deg, best >= 2 ? (int)~(uint32_t)best : -1) : 0ull);
+            stat_add(p, t, MM_ST_RESP_ENTRIES, r ? respond_seen<kW>(p, beg, deg, kb) : 0ull);
+            stat_add(p, t, MM_ST_MATCHED, matched ? 1ull : 0ull);
+        }
+        __syncwarp();
+        if (own) fw.best[lane] = 0ull;
+        if (matched || dead) act = false;
+    }
+    if (own) {
+        // members still unmatched at the cap keep their last colour
+        p.ctl->match[g] = act ? (blue ? 0 : 1) : val;
+        if (p.last) p.last[g] = (uint8_t)lastr;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lastr = max(lastr, __shfl_xor_sync(kFull, lastr, o));
+    return lastr;
+}
+
+// Pass 1: classify round t's items (cls[i]) and search the root candidates'
+// components; calls the attempt off (ctl->fin_abort = t + 1) if one cannot be
+// finished here.
+template <bool kW, bool kStats>
+__device__ __forceinline__ void finish_classify(const Params &p, Smem &sm, int t, int par, int c0, int c1, int *cls)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    FinWarp &fw = reinterpret_cast<FinWarp *>(&sm)[warp];
+    const long long A = (long long)c0 + c1;
+    const long long gw = (long long)blockIdx.x * kWarps + warp, nw = (long long)gridDim.x * kWarps;
+    bool abort = false;
+    for (long long base = gw * 32; base < A; base += nw * 32) {
+        const long long i = base + lane;
+        const int4 it = i < A ? item_at(p, par, c0, i) : make_int4(-1, 0, 0, 0);
+        const int deg = it.x >= 0 ? degree_of(it) : 0;
+        int nint = 0;
+        bool lower = false, bad = false;
+        if (it.x >= 0 && deg <= kFinShort) fin_scan_thread(p, it.x, it.y, it.y + deg, nint, lower, bad);
+        unsigned longs = __ballot_sync(kFull, it.x >= 0 && deg > kFinShort);
+        while (longs) {
+            const int s = __ffs(longs) - 1;
+            longs &= longs - 1;
+            const int vs = __shfl_sync(kFull, it.x, s), bs = __shfl_sync(kFull, it.y, s);
+            const int ds = __shfl_sync(kFull, deg, s);
+            if (ds > kFinMaxDeg) {
+                if (lane == s) bad = true;
+                continue;
+            }
+            int n2;
+            bool l2, b2;
+            fin_scan_warp(p, vs, bs, bs + ds, n2, l2, b2);
+            if (lane == s) {
+                nint = n2;
+                lower = l2;
+                bad = b2;
+            }
+        }
+        const int c = it.x < 0 ? 0 : (nint == 0 ? kFinSingle : (lower ? kFinMember : kFinRootCand));
+        if (i < A) cls[i] = c;
+        abort |= bad;
+        if (kStats) {
+            stat_add(p, t, MM_ST_FINISH_ITEMS, it.x >= 0 ? 1ull : 0ull);
+            stat_add(p, t, MM_ST_FINISH_ENTRIES, (unsigned long long)deg);
+        }
+        unsigned roots = __ballot_sync(kFull, c == kFinRootCand);
+        if (__any_sync(kFull, abort)) roots = 0;  // the attempt is off already
+        while (roots) {
+            const int s = __ffs(roots) - 1;
+            roots &= roots - 1;
+            int mem, k;
+            unsigned long long seen = 0;
+            const int r = fin_search<kW>(p, fw, __shfl_sync(kFull, it.x, s), &mem, &k, kStats ? &seen : nullptr);
+            if (kStats && lane == 0) atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_FINISH_ENTRIES], seen);
+            if (r == kFinTooBig) {
+                abort = true;
+                break;
+            }
+        }
+        if (__any_sync(kFull, abort)) break;
+    }
+    if (abort && lane == 0) atomicExch(&p.ctl->fin_abort, t + 1);
+}
+
+// Pass 2: resolve singletons and play the components of the roots.
+template <bool kW, bool kStats>
+__device__ __forceinline__ void finish_resolve(const Params &p, Smem &sm, int t, int par, int c0, int c1, int cap,
+                                               const int *cls)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    FinWarp &fw = reinterpret_cast<FinWarp *>(&sm)[warp];
+    const long long A = (long long)c0 + c1;
+    const long long gw = (long long)blockIdx.x * kWarps + warp, nw = (long long)gridDim.x * kWarps;
+    const uint32_t bar = p.ctl->barrier;
+    int last_all = -1;
+    for (long long base = gw * 32; base < A; base += nw * 32) {
+        const long long i = base + lane;
+        const int c = i < A ? __ldcg(cls + i) : 0;
+        const int4 it = c == kFinSingle || c == kFinRootCand ? item_at(p, par, c0, i) : make_int4(-1, 0, 0, 0);
+        // singletons: the first round in which they are blue ends them
+        {
+            const bool mine = c == kFinSingle;
+            const int v = it.x, deg = mine ? degree_of(it) : 0;
+            const uint32_t hid = mine ? (uint32_t)(v - base_of(p, v)) : 0u;
+            bool act = mine, blue = i < c0;
+            int lastr = -1;
+            for (int r = t; r < cap && __any_sync(kFull, act); ++r) {
+                if (act) {
+                    if (r > t) blue = colour_of(hid, p.seeds[r], bar) == kBlue;
+                    lastr = r;
+                }
+                if (kStats) {
+                    const bool b = act && blue, rd = act && !blue;
+                    if (r > t) {  // round t's colouring was counted by the commit that made it
+                        stat_add(p, r, MM_ST_ACTIVE, act ? 1ull : 0ull);
+                        stat_add(p, r, MM_ST_BLUE, b ? 1ull : 0ull);
+                        stat_add(p, r, MM_ST_RED, rd ? 1ull : 0ull);
+                    }
+                    stat_add(p, r, MM_ST_BLUE_DEG, b ? (unsigned long long)deg : 0ull);
+                    stat_add(p, r, MM_ST_RED_DEG, rd ? (unsigned long long)deg : 0ull);
+                    stat_add(p, r, MM_ST_REQ_ENTRIES, b ? (unsigned long long)deg : 0ull);
+                    stat_add(p, r, MM_ST_RESP_ENTRIES, rd ? (unsigned long long)deg : 0ull);
+                }
+                if (act && blue) act = false;
+            }
+            if (mine) {
+                // still red at the cap: it keeps that colour
+                p.ctl->match[v] = act ? 1 : 2;
+                if (p.last) p.last[v] = (uint8_t)lastr;
+                last_all = max(last_all, lastr);
+            }
+        }
+        // roots: play their components
+        unsigned roots = __ballot_sync(kFull, c == kFinRootCand);
+        while (roots) {
+            const int s = __ffs(roots) - 1;
+            roots &= roots - 1;
+            int mem, k;
+            const int r = fin_search<kW>(p, fw, __shfl_sync(kFull, it.x, s), &mem, &k, nullptr);
+            if (r == kFinRoot) last_all = max(last_all, fin_play<kW, kStats>(p, fw, t, cap, mem, k));
+            __syncwarp();  // fw is reused by the next root
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) last_all = max(last_all, __shfl_xor_sync(kFull, last_all, o));
+    if (lane == 0 && last_all >= 0) atomicMax(&p.ctl->fin_last, last_all);
+}
+
 // The whole matching in one cooperative launch: set-up, then per round the
 // window scan (A1), the fallback scan (A2, only in rounds that have fallback
 // lists) and the commit phase (B), separated by grid barriers.  Every block
@@ -1106,9 +1539,37 @@ __global__ void __launch_bounds__(kThreads, 2) k_rounds(Params p)
 
     init_phase<kW, kStats, kPolicy>(p, sm);
     if (!grid_sync(p.bar, p.ctl, p.tstamp, 0)) return;
+    // active vertices at round 0; round 1 clears these counters only after two
+    // more grid barriers
+    const long long active0 = (long long)__ldcg(&ctl->cnt[0][kBlue]) + __ldcg(&ctl->cnt[0][kRed]);
+    long long fin_next = active0;  // finish phase: next attempt once the active set is this small
     int t = 0;
     for (;; ++t) {
         const int par = t & 1;
+        // finish phase (the symmetric path of the reference's colouring only):
+        // every block reads the same counters and takes the same branch
+        if (!kPolicy && p.sym && t > 0) {
+            const int c0 = __ldcg(&ctl->cnt[par][kBlue]), c1 = __ldcg(&ctl->cnt[par][kRed]);
+            const long long act = (long long)c0 + c1;
+            if (act > 0 && act * kFinDiv <= active0 && act <= fin_next) {
+                int *cls = reinterpret_cast<int *>(p.req);  // per item; req is rewritten before it is read
+                finish_classify<kW, kStats>(p, sm, t, par, c0, c1, cls);
+                // profile: a finished round reports the classify pass as its window
+                // scan and the resolve pass as its fallback scan
+                if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 1)) return;
+                if (__ldcg(&ctl->fin_abort) != t + 1) {
+                    finish_resolve<kW, kStats>(p, sm, t, par, c0, c1, cap, cls);
+                    if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 2)) return;
+                    if (blockIdx.x == 0 && threadIdx.x == 0) {
+                        const int last = __ldcg(&ctl->fin_last);
+                        ctl->rounds = maximal ? min(last + 2, cap) : cap;
+                        if (p.tstamp) p.tstamp[3 * t + 3] = p.tstamp[3 * t + 2];
+                    }
+                    return;  // every vertex's match value is final
+                }
+                fin_next = act / 2;  // called off: try again once the active set has halved
+            }
+        }
         // phase A1; the next round's counters were last read in round t - 1
         if (blockIdx.x == 0 && threadIdx.x < kParityLists) {
             ctl->cnt[par ^ 1][threadIdx.x] = 0;

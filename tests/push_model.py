@@ -131,7 +131,157 @@ def reverse_keys_sorted(n, ranges, nbrs, w, weighted, chunk=2048):
     return None if bad else rk
 
 
-def push_match(g, type_, seeds, barrier, colour_hash):
+def is_symmetric(n, ranges, nbrs, w, weighted):
+    """The upload test of the symmetric path: contiguous ranges in vertex order,
+    strictly increasing lists, and the entries (v, u[, w]) are those (u, v[, w])
+    transposed."""
+    if n == 0 or ranges[0, 0] != 0 or ranges[-1, 1] != len(nbrs):
+        return False
+    if np.any(ranges[:, 1] < ranges[:, 0]) or np.any(ranges[1:, 0] != ranges[:-1, 1]):
+        return False
+    ent = {}
+    for v in range(n):
+        lst = [int(x) for x in nbrs[ranges[v, 0]:ranges[v, 1]]]
+        if any(b <= a for a, b in zip(lst, lst[1:])):
+            return False
+        for j in range(int(ranges[v, 0]), int(ranges[v, 1])):
+            key = (v, int(nbrs[j]))
+            ent[key] = np.float32(w[j]).tobytes() if weighted else b""
+    return all(ent.get((u, v)) == x for (v, u), x in ent.items())
+
+
+FIN_SINGLE, FIN_MEMBER, FIN_ROOT = 1, 2, 3
+
+
+def finish_model(n, ranges, nbrs, w, weighted, maximal, cap, seeds, barrier, colour_hash, col, match, active, t,
+                 lim):
+    """The finish phase of the round kernel (mm_push.cu: finish_classify,
+    fin_search, finish_resolve, fin_play) at the start of round t, vertex by
+    vertex.  col holds the colours of round t; match the final values of the
+    vertices no longer active.  Returns the rounds executed, with match filled
+    in for every active vertex, or None if the attempt is called off (then
+    nothing has changed)."""
+    BLUE, RED, DEAD, MATCHED = 0, 1, 2, 3
+
+    def lst(x):
+        return range(int(ranges[x, 0]), max(int(ranges[x, 1]), int(ranges[x, 0])))
+
+    def search(v):
+        mem, ents = [v], []  # ents: (owner slot, target slot, preference key)
+        f = 0
+        while f < len(mem):
+            x = mem[f]
+            js = lst(x)
+            if len(js) > lim["maxdeg"]:
+                return "big", None
+            rows = [list(js)[i:i + 32] for i in range(0, len(js), 32)]
+            for row in rows:
+                cs = [col[int(nbrs[j])] for j in row]
+                if any(c == DEAD for c in cs):
+                    return "big", None
+                if any(c <= RED and int(nbrs[j]) < v for j, c in zip(row, cs)):
+                    return "notroot", None
+                for j, c in zip(row, cs):
+                    if c > RED:
+                        continue
+                    u = int(nbrs[j])
+                    if u in mem:
+                        slot = mem.index(u)
+                    else:
+                        if len(mem) == lim["members"]:
+                            return "big", None
+                        slot = len(mem)
+                        mem.append(u)
+                    if len(ents) == lim["entries"]:
+                        return "big", None
+                    # a weight that can never be picked still marks an unmatched neighbour (key 1)
+                    ents.append((f, slot, (cand_key(j, float(w[j]), weighted) or 1) if weighted else (~j & M32)))
+            f += 1
+        return "root", (mem, ents)
+
+    # pass 1: classify, search the root candidates' components
+    cls = {}
+    for v in active:
+        js = lst(v)
+        if len(js) > lim["maxdeg"]:
+            return None
+        cs = [col[int(nbrs[j])] for j in js]
+        if any(c == DEAD for c in cs):
+            return None
+        inner = [int(nbrs[j]) for j, c in zip(js, cs) if c <= RED]
+        cls[v] = FIN_SINGLE if not inner else (FIN_MEMBER if min(inner) < v else FIN_ROOT)
+    for v in active:
+        if cls[v] == FIN_ROOT and search(v)[0] == "big":
+            return None
+    # pass 2: resolve
+    last_all = -1
+    for v in active:
+        if cls[v] == FIN_SINGLE:
+            blue, r, last = col[v] == BLUE, t, t
+            while True:
+                last = r
+                if blue:
+                    match[v] = 2
+                    break
+                r += 1
+                if r >= cap:
+                    match[v] = 1
+                    break
+                blue = colour_hash(v, int(seeds[r])) < barrier
+            last_all = max(last_all, last)
+        elif cls[v] == FIN_ROOT:
+            res, comp = search(v)
+            if res != "root":
+                continue
+            mem, ents = comp
+            k = len(mem)
+            act, val, blue, last = [True] * k, [0] * k, [False] * k, [-1] * k
+            r = t
+            while r < cap and any(act):
+                for l in range(k):
+                    if act[l]:
+                        blue[l] = colour_hash(mem[l], int(seeds[r])) < barrier
+                        last[l] = r
+                st = [(BLUE if blue[l] else RED) if act[l] else (DEAD if val[l] == 2 else MATCHED) for l in range(k)]
+                best, choice, crk, got = [0] * k, [0] * k, [0] * k, [0] * k
+                for l in range(k):
+                    if not (act[l] and blue[l]):
+                        continue
+                    for (o, tg, pref) in ents:
+                        if o != l:
+                            continue
+                        key = pref if st[tg] == RED else (0 if st[tg] == MATCHED else 1)
+                        if key > best[l]:
+                            best[l], choice[l] = key, tg
+                    if best[l] >= 2:
+                        crk[l] = (((best[l] >> 32) << 32) | (~mem[l] & M32)) if weighted else (~mem[l] & M32)
+                        got[choice[l]] = max(got[choice[l]], crk[l])
+                done = [False] * k
+                for l in range(k):
+                    if not act[l]:
+                        continue
+                    if blue[l]:
+                        if best[l] >= 2 and (got[choice[l]] & M32) == (crk[l] & M32):
+                            val[l] = 4 + min(mem[l], mem[choice[l]])
+                            done[l] = True
+                        elif best[l] == 0:
+                            val[l] = 2
+                            done[l] = True
+                    elif got[l]:
+                        val[l] = 4 + min(mem[l], ~got[l] & M32)
+                        done[l] = True
+                for l in range(k):
+                    if done[l]:
+                        act[l] = False
+                r += 1
+            for l in range(k):
+                match[mem[l]] = (0 if blue[l] else 1) if act[l] else val[l]
+            last_all = max(last_all, max(last))
+    return min(last_all + 2, cap) if maximal else cap
+
+
+def push_match(g, type_, seeds, barrier, colour_hash, finish=None):
+    """finish: None, or the finish phase's limits {div, members, entries, maxdeg}."""
     n = g.n
     ranges = np.asarray(g.ranges)
     nbrs = np.asarray(g.nbrs)
@@ -147,7 +297,19 @@ def push_match(g, type_, seeds, barrier, colour_hash):
     best = [0] * n
     rounds = None
     t = 0
+    sym = finish is not None and is_symmetric(n, ranges, nbrs, w, weighted)
+    act0 = len(active)
+    fin_next = act0
     while True:
+        if sym and t > 0 and active and len(active) * finish["div"] <= act0 and len(active) <= fin_next:
+            r = finish_model(n, ranges, nbrs, w, weighted, maximal, cap, seeds, barrier, colour_hash, col, match,
+                             active, t, finish)
+            if r is not None:
+                out = np.zeros(n, np.int32)
+                for v in range(n):
+                    out[v] = match[v] if match[v] is not None else col[v]
+                return out, r
+            fin_next = len(active) // 2
         # phase A: blue vertices scan and propose
         req = {}
         dead = set()

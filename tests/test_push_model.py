@@ -53,3 +53,68 @@ def test_sorted_reverse_key_build_equals_pair_definition():
                 assert got is None
                 seen_unsorted += 1
     assert seen_unsorted > 0
+
+
+def symmetric_graph(rng, n, avg_deg, loops=0.05, special=True):
+    """A CSR that takes the symmetric path: contiguous, strictly increasing lists,
+    every entry's transpose present with the same weight (self-loops once)."""
+    from graphs_small import SPECIAL_WEIGHTS, SmallGraph
+
+    pairs = {}
+    for _ in range(int(n * avg_deg / 2)):
+        u, v = int(rng.integers(n)), int(rng.integers(n))
+        if u == v and rng.random() > loops:
+            continue
+        a, b = min(u, v), max(u, v)
+        if (a, b) in pairs:
+            continue
+        pairs[(a, b)] = (SPECIAL_WEIGHTS[rng.integers(len(SPECIAL_WEIGHTS))] if special and rng.random() < 0.3
+                         else np.float32(rng.integers(1, 8) / 4))
+    lists = [[] for _ in range(n)]
+    for (a, b), wt in pairs.items():
+        lists[a].append((b, wt))
+        if a != b:
+            lists[b].append((a, wt))
+    nbrs, wts, ranges = [], [], np.zeros((n, 2), np.int64)
+    for v in range(n):
+        ranges[v, 0] = len(nbrs)
+        for u, wt in sorted(lists[v], key=lambda e: e[0]):
+            nbrs.append(u)
+            wts.append(wt)
+        ranges[v, 1] = len(nbrs)
+    return SmallGraph(n, ranges, np.array(nbrs, np.int32), np.array(wts, np.float32))
+
+
+def test_finish_phase_model_equals_oracle(orc):
+    """The finish phase (components played on their own from the round the
+    active set is small enough) gives the oracle's matching and round count,
+    whether it completes or is called off (small limits force both)."""
+    import push_model
+
+    outcomes = {"done": 0, "off": 0}
+    model = push_model.finish_model
+
+    def counted(*a, **k):
+        r = model(*a, **k)
+        outcomes["done" if r is not None else "off"] += 1
+        return r
+
+    push_model.finish_model = counted
+    try:
+        rng = np.random.default_rng(5)
+        for it in range(60):
+            n = int(rng.integers(2, 90))
+            g = symmetric_graph(rng, n, float(rng.uniform(0.5, 5)))
+            assert push_model.is_symmetric(g.n, g.ranges, g.nbrs, g.weights, True)
+            seeds = orc.rand_seeds(int(rng.integers(1, 1000)))
+            lim = [dict(div=1, members=32, entries=128, maxdeg=2048), dict(div=2, members=3, entries=4, maxdeg=4),
+                   dict(div=12, members=32, entries=128, maxdeg=2048)][it % 3]
+            for barrier in (0x88B81733, 0x40000000):
+                for t in (6, 7, 8, 9):
+                    want, rounds, _ = orc.match(g, t, seeds, barrier)
+                    got, got_rounds = push_match(g, t, seeds, barrier, orc.colour_hash, finish=lim)
+                    assert got_rounds == rounds, (it, t, hex(barrier))
+                    assert np.array_equal(got, want), (it, t, hex(barrier))
+    finally:
+        push_model.finish_model = model
+    assert outcomes["done"] > 100 and outcomes["off"] > 100, outcomes
