@@ -368,6 +368,7 @@ struct Smem {
     LongStage stage[kWarps];
     int tile_warp[kWarps][2];             // compaction: per-warp counts, then offsets
     int tile_base[2];                     // compaction: tile bases
+    uint32_t seeds[256];                  // the call's colouring seeds (finish phase)
 };
 
 // ---- learned colouring ----
@@ -1140,7 +1141,8 @@ struct FinWarp {
     uint8_t tgt[kFinEntries];
     uint8_t st[kFinMembers];
 };
-static_assert(sizeof(FinWarp) * kWarps <= sizeof(Smem), "the finish phase reuses the scan phases' shared memory");
+static_assert(sizeof(FinWarp) * kWarps <= offsetof(Smem, tile_warp),
+              "the finish phase reuses the fallback scan's shared memory");
 
 // Item i of round parity `par` (blue list first, then red).
 __device__ __forceinline__ int4 item_at(const Params &p, int par, int c0, long long i)
@@ -1229,9 +1231,11 @@ __device__ __forceinline__ int fin_search(const Params &p, FinWarp &fw, int v, i
         for (int j0 = b; j0 < e; j0 += 32) {
             const int j = j0 + lane;
             int u = -1;
+            float wj = 0.0f;
             uint8_t c = kMatched;
             if (j < e) {
                 u = __ldg(p.nbrs + j);
+                if (kW) wj = __ldg(p.w + j);  // with the id: no dependent load once the colour is known
                 c = p.col[u];
             }
             const bool in = c <= kRed;
@@ -1239,7 +1243,7 @@ __device__ __forceinline__ int fin_search(const Params &p, FinWarp &fw, int v, i
             if (__any_sync(kFull, in && u < v)) return kFinNotRoot;
             unsigned m = __ballot_sync(kFull, in);
             unsigned long long pref = 0;
-            if (in) pref = kW ? cand_key<true>(j, __ldg(p.w + j)) : (unsigned long long)(uint32_t)~j;
+            if (in) pref = kW ? cand_key<true>(j, wj) : (unsigned long long)(uint32_t)~j;
             while (m) {
                 const int s = __ffs(m) - 1;
                 m &= m - 1;
@@ -1294,7 +1298,8 @@ __device__ __forceinline__ unsigned long long respond_seen(const Params &p, int 
 // writes every member's match value (and batch round marks).  Returns, in
 // every lane, the last round in which a member was active.
 template <bool kW, bool kStats>
-__device__ __forceinline__ int fin_play(const Params &p, FinWarp &fw, int t0, int cap, int mem, int k)
+__device__ __forceinline__ int fin_play(const Params &p, FinWarp &fw, const uint32_t *seeds, int t0, int cap, int mem,
+                                       int k)
 {
     const int lane = threadIdx.x & 31;
     const bool own = lane < k;
@@ -1315,7 +1320,7 @@ __device__ __forceinline__ int fin_play(const Params &p, FinWarp &fw, int t0, in
     __syncwarp();
     for (int t = t0; t < cap && __any_sync(kFull, act); ++t) {
         if (act) {
-            blue = colour_of(hid, p.seeds[t], bar) == kBlue;
+            blue = colour_of(hid, seeds[t], bar) == kBlue;
             lastr = t;
         }
         if (own) fw.st[lane] = act ? (blue ? kBlue : kRed) : (val == 2 ? kDead : kMatched);
@@ -1391,86 +1396,75 @@ __device__ __forceinline__ int fin_play(const Params &p, FinWarp &fw, int t0, in
     return lastr;
 }
 
-// Pass 1: classify round t's items (cls[i]) and search the root candidates'
-// components; calls the attempt off (ctl->fin_abort = t + 1) if one cannot be
-// finished here.
-template <bool kW, bool kStats>
-__device__ __forceinline__ void finish_classify(const Params &p, Smem &sm, int t, int par, int c0, int c1, int *cls)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    FinWarp &fw = reinterpret_cast<FinWarp *>(&sm)[warp];
-    const long long A = (long long)c0 + c1;
-    const long long gw = (long long)blockIdx.x * kWarps + warp, nw = (long long)gridDim.x * kWarps;
-    bool abort = false;
-    for (long long base = gw * 32; base < A; base += nw * 32) {
-        const long long i = base + lane;
-        const int4 it = i < A ? item_at(p, par, c0, i) : make_int4(-1, 0, 0, 0);
-        const int deg = it.x >= 0 ? degree_of(it) : 0;
-        int nint = 0;
-        bool lower = false, bad = false;
-        if (it.x >= 0 && deg <= kFinShort) fin_scan_thread(p, it.x, it.y, it.y + deg, nint, lower, bad);
-        unsigned longs = __ballot_sync(kFull, it.x >= 0 && deg > kFinShort);
-        while (longs) {
-            const int s = __ffs(longs) - 1;
-            longs &= longs - 1;
-            const int vs = __shfl_sync(kFull, it.x, s), bs = __shfl_sync(kFull, it.y, s);
-            const int ds = __shfl_sync(kFull, deg, s);
-            if (ds > kFinMaxDeg) {
-                if (lane == s) bad = true;
-                continue;
-            }
-            int n2;
-            bool l2, b2;
-            fin_scan_warp(p, vs, bs, bs + ds, n2, l2, b2);
-            if (lane == s) {
-                nint = n2;
-                lower = l2;
-                bad = b2;
-            }
-        }
-        const int c = it.x < 0 ? 0 : (nint == 0 ? kFinSingle : (lower ? kFinMember : kFinRootCand));
-        if (i < A) cls[i] = c;
-        abort |= bad;
-        if (kStats) {
-            stat_add(p, t, MM_ST_FINISH_ITEMS, it.x >= 0 ? 1ull : 0ull);
-            stat_add(p, t, MM_ST_FINISH_ENTRIES, (unsigned long long)deg);
-        }
-        unsigned roots = __ballot_sync(kFull, c == kFinRootCand);
-        if (__any_sync(kFull, abort)) roots = 0;  // the attempt is off already
-        while (roots) {
-            const int s = __ffs(roots) - 1;
-            roots &= roots - 1;
-            int mem, k;
-            unsigned long long seen = 0;
-            const int r = fin_search<kW>(p, fw, __shfl_sync(kFull, it.x, s), &mem, &k, kStats ? &seen : nullptr);
-            if (kStats && lane == 0) atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_FINISH_ENTRIES], seen);
-            if (r == kFinTooBig) {
-                abort = true;
-                break;
-            }
-        }
-        if (__any_sync(kFull, abort)) break;
-    }
-    if (abort && lane == 0) atomicExch(&p.ctl->fin_abort, t + 1);
-}
+// One pass of the finish phase over round t's items.  kMode:
+//   kFinPassClassify  classify every item (cls[i]) and search the root
+//                     candidates' components; call the attempt off
+//                     (ctl->fin_abort = t + 1) if one cannot be finished here;
+//   kFinPassResolve   resolve the singletons and play the roots' components,
+//                     from that classification;
+//   kFinPassBoth      both at once, speculatively: an item is classified and
+//                     resolved in one go, each root searched once.  If the
+//                     attempt is called off, the values already written are
+//                     the ones the following rounds write again.
+// The instrumented kernel runs the first two (its counters must not count a
+// called-off attempt's rounds); the others run the third.
+enum : int { kFinPassClassify = 0, kFinPassResolve = 1, kFinPassBoth = 2 };
 
-// Pass 2: resolve singletons and play the components of the roots.
-template <bool kW, bool kStats>
-__device__ __forceinline__ void finish_resolve(const Params &p, Smem &sm, int t, int par, int c0, int c1, int cap,
-                                               const int *cls)
+template <bool kW, bool kStats, int kMode>
+__device__ __forceinline__ void finish_pass(const Params &p, Smem &sm, int t, int par, int c0, int c1, int cap,
+                                            int *cls)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     FinWarp &fw = reinterpret_cast<FinWarp *>(&sm)[warp];
+    const uint32_t *seeds = sm.seeds;
     const long long A = (long long)c0 + c1;
     const long long gw = (long long)blockIdx.x * kWarps + warp, nw = (long long)gridDim.x * kWarps;
     const uint32_t bar = p.ctl->barrier;
+    bool abort = false;
     int last_all = -1;
     for (long long base = gw * 32; base < A; base += nw * 32) {
         const long long i = base + lane;
-        const int c = i < A ? __ldcg(cls + i) : 0;
-        const int4 it = c == kFinSingle || c == kFinRootCand ? item_at(p, par, c0, i) : make_int4(-1, 0, 0, 0);
+        int c = 0;
+        int4 it = make_int4(-1, 0, 0, 0);
+        if (kMode == kFinPassResolve) {
+            c = i < A ? __ldcg(cls + i) : 0;
+            if (c == kFinSingle || c == kFinRootCand) it = item_at(p, par, c0, i);
+        } else {
+            if (i < A) it = item_at(p, par, c0, i);
+            const int deg = it.x >= 0 ? degree_of(it) : 0;
+            int nint = 0;
+            bool lower = false, bad = false;
+            if (it.x >= 0 && deg <= kFinShort) fin_scan_thread(p, it.x, it.y, it.y + deg, nint, lower, bad);
+            unsigned longs = __ballot_sync(kFull, it.x >= 0 && deg > kFinShort);
+            while (longs) {
+                const int s = __ffs(longs) - 1;
+                longs &= longs - 1;
+                const int vs = __shfl_sync(kFull, it.x, s), bs = __shfl_sync(kFull, it.y, s);
+                const int ds = __shfl_sync(kFull, deg, s);
+                if (ds > kFinMaxDeg) {
+                    if (lane == s) bad = true;
+                    continue;
+                }
+                int n2;
+                bool l2, b2;
+                fin_scan_warp(p, vs, bs, bs + ds, n2, l2, b2);
+                if (lane == s) {
+                    nint = n2;
+                    lower = l2;
+                    bad = b2;
+                }
+            }
+            c = it.x < 0 ? 0 : (nint == 0 ? kFinSingle : (lower ? kFinMember : kFinRootCand));
+            if (kMode == kFinPassClassify && i < A) cls[i] = c;
+            abort |= bad;
+            if (kStats) {
+                stat_add(p, t, MM_ST_FINISH_ITEMS, it.x >= 0 ? 1ull : 0ull);
+                stat_add(p, t, MM_ST_FINISH_ENTRIES, (unsigned long long)deg);
+            }
+            if (__any_sync(kFull, abort)) break;  // the attempt is off
+        }
         // singletons: the first round in which they are blue ends them
-        {
+        if (kMode != kFinPassClassify) {
             const bool mine = c == kFinSingle;
             const int v = it.x, deg = mine ? degree_of(it) : 0;
             const uint32_t hid = mine ? (uint32_t)(v - base_of(p, v)) : 0u;
@@ -1478,7 +1472,7 @@ __device__ __forceinline__ void finish_resolve(const Params &p, Smem &sm, int t,
             int lastr = -1;
             for (int r = t; r < cap && __any_sync(kFull, act); ++r) {
                 if (act) {
-                    if (r > t) blue = colour_of(hid, p.seeds[r], bar) == kBlue;
+                    if (r > t) blue = colour_of(hid, seeds[r], bar) == kBlue;
                     lastr = r;
                 }
                 if (kStats) {
@@ -1502,20 +1496,33 @@ __device__ __forceinline__ void finish_resolve(const Params &p, Smem &sm, int t,
                 last_all = max(last_all, lastr);
             }
         }
-        // roots: play their components
+        // root candidates: search, then (unless only classifying) play
         unsigned roots = __ballot_sync(kFull, c == kFinRootCand);
         while (roots) {
             const int s = __ffs(roots) - 1;
             roots &= roots - 1;
             int mem, k;
-            const int r = fin_search<kW>(p, fw, __shfl_sync(kFull, it.x, s), &mem, &k, nullptr);
-            if (r == kFinRoot) last_all = max(last_all, fin_play<kW, kStats>(p, fw, t, cap, mem, k));
+            unsigned long long seen = 0;
+            const int r = fin_search<kW>(p, fw, __shfl_sync(kFull, it.x, s), &mem, &k,
+                                         kStats && kMode == kFinPassClassify ? &seen : nullptr);
+            if (kStats && kMode == kFinPassClassify && lane == 0)
+                atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_FINISH_ENTRIES], seen);
+            if (r == kFinTooBig) {
+                abort = true;
+                break;
+            }
+            if (kMode != kFinPassClassify && r == kFinRoot)
+                last_all = max(last_all, fin_play<kW, kStats>(p, fw, seeds, t, cap, mem, k));
             __syncwarp();  // fw is reused by the next root
         }
+        if (kMode != kFinPassResolve && __any_sync(kFull, abort)) break;
     }
+    if (kMode != kFinPassResolve && abort && lane == 0) atomicExch(&p.ctl->fin_abort, t + 1);
+    if (kMode != kFinPassClassify) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) last_all = max(last_all, __shfl_xor_sync(kFull, last_all, o));
-    if (lane == 0 && last_all >= 0) atomicMax(&p.ctl->fin_last, last_all);
+        for (int o = 16; o > 0; o >>= 1) last_all = max(last_all, __shfl_xor_sync(kFull, last_all, o));
+        if (lane == 0 && last_all >= 0) atomicMax(&p.ctl->fin_last, last_all);
+    }
 }
 
 // The whole matching in one cooperative launch: set-up, then per round the
@@ -1537,6 +1544,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_rounds(Params p)
     const int gwarp = blockIdx.x * kWarps + (threadIdx.x >> 5);
     const int nwarps = gridDim.x * kWarps;
 
+    // the seed buffer holds 256 words (only the call's seeds are meaningful)
+    for (int i = threadIdx.x; i < 256; i += kThreads) sm.seeds[i] = p.seeds[i];
     init_phase<kW, kStats, kPolicy>(p, sm);
     if (!grid_sync(p.bar, p.ctl, p.tstamp, 0)) return;
     // active vertices at round 0; round 1 clears these counters only after two
@@ -1553,13 +1562,24 @@ __global__ void __launch_bounds__(kThreads, 2) k_rounds(Params p)
             const long long act = (long long)c0 + c1;
             if (act > 0 && act * kFinDiv <= active0 && act <= fin_next) {
                 int *cls = reinterpret_cast<int *>(p.req);  // per item; req is rewritten before it is read
-                finish_classify<kW, kStats>(p, sm, t, par, c0, c1, cls);
-                // profile: a finished round reports the classify pass as its window
-                // scan and the resolve pass as its fallback scan
-                if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 1)) return;
-                if (__ldcg(&ctl->fin_abort) != t + 1) {
-                    finish_resolve<kW, kStats>(p, sm, t, par, c0, c1, cap, cls);
-                    if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 2)) return;
+                // profile: a finished round reports its first pass as the window
+                // scan and the second (instrumented kernel) as the fallback scan
+                bool done;
+                if (kStats) {
+                    finish_pass<kW, kStats, kFinPassClassify>(p, sm, t, par, c0, c1, cap, cls);
+                    if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 1)) return;
+                    done = __ldcg(&ctl->fin_abort) != t + 1;
+                    if (done) {
+                        finish_pass<kW, kStats, kFinPassResolve>(p, sm, t, par, c0, c1, cap, cls);
+                        if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 2)) return;
+                    }
+                } else {
+                    finish_pass<kW, kStats, kFinPassBoth>(p, sm, t, par, c0, c1, cap, cls);
+                    if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 1)) return;
+                    done = __ldcg(&ctl->fin_abort) != t + 1;
+                    if (done && blockIdx.x == 0 && threadIdx.x == 0 && p.tstamp) p.tstamp[3 * t + 2] = p.tstamp[3 * t + 1];
+                }
+                if (done) {
                     if (blockIdx.x == 0 && threadIdx.x == 0) {
                         const int last = __ldcg(&ctl->fin_last);
                         ctl->rounds = maximal ? min(last + 2, cap) : cap;
