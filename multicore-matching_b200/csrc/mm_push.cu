@@ -1396,6 +1396,194 @@ __device__ __forceinline__ int fin_play(const Params &p, FinWarp &fw, const uint
     return lastr;
 }
 
+// Lane-level components.  Most components of the finish round are pairs and
+// short paths, and a warp that searched and played its lanes' roots one after
+// another made each warp's roots a chain of dependent loads (about 5 roots a
+// tile on a 512 x 512 grid at round 3, 15 us each).  So each lane first
+// searches and plays its own root's component on its own, in per-thread
+// storage; a component with more than kFinTMembers members, more than
+// kFinTEntries entries between them or a member list longer than kFinTMaxDeg
+// goes to the warp-level search above.
+constexpr int kFinTMembers = 8;
+constexpr int kFinTEntries = 16;
+constexpr int kFinTMaxDeg = 64;
+enum : int { kFinOverflow = 3 };
+
+struct FinComp {
+    unsigned long long pref[kFinTEntries];
+    int mem[kFinTMembers];
+    int mbeg[kFinTMembers];
+    int mdeg[kFinTMembers];
+    uint8_t tgt[kFinTEntries];
+    uint8_t eoff[kFinTMembers + 1];
+    int k;
+};
+
+// As fin_search, by one thread for root candidate v (own list [b0, e0)); or
+// kFinOverflow when the component does not fit FinComp.
+template <bool kW>
+__device__ __forceinline__ int fin_search_thread(const Params &p, int v, int b0, int e0, FinComp &cp,
+                                                 unsigned long long *scanned)
+{
+    int k = 1, ne = 0;
+    cp.mem[0] = v;
+    unsigned long long seen = 0;
+    for (int f = 0; f < k; ++f) {
+        const int x = cp.mem[f];
+        int b = b0, e = e0;
+        if (f > 0) {
+            const int2 r = __ldg(p.ranges + x);
+            b = r.x;
+            e = r.y > r.x ? r.y : r.x;
+        }
+        if (e - b > kFinTMaxDeg) return kFinOverflow;
+        cp.eoff[f] = (uint8_t)ne;
+        cp.mbeg[f] = b;
+        cp.mdeg[f] = e - b;
+        seen += (unsigned long long)(e - b);
+        for (int j0 = b; j0 < e; j0 += 8) {
+            int u[8];
+            float wv[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                u[q] = j0 + q < e ? __ldg(p.nbrs + j0 + q) : -1;
+                wv[q] = kW && j0 + q < e ? __ldg(p.w + j0 + q) : 0.0f;
+            }
+            uint8_t c[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) c[q] = u[q] >= 0 ? p.col[u[q]] : (uint8_t)kMatched;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                if (c[q] == kDead) return kFinTooBig;  // not on the symmetric path
+                if (c[q] > kRed) continue;
+                if (u[q] < v) return kFinNotRoot;
+                int slot = -1;
+                for (int m = 0; m < k; ++m)
+                    if (cp.mem[m] == u[q]) slot = m;
+                if (slot < 0) {
+                    if (k == kFinTMembers) return kFinOverflow;
+                    slot = k;
+                    cp.mem[k++] = u[q];
+                }
+                if (ne == kFinTEntries) return kFinOverflow;
+                cp.pref[ne] = kW ? cand_key<true>(j0 + q, wv[q]) : (unsigned long long)(uint32_t)~(j0 + q);
+                cp.tgt[ne] = (uint8_t)slot;
+                ++ne;
+            }
+        }
+    }
+    cp.eoff[k] = (uint8_t)ne;
+    cp.k = k;
+    if (scanned) *scanned = seen;
+    return kFinRoot;
+}
+
+__device__ __forceinline__ void stat_add_one(const Params &p, int round, int col, unsigned long long v)
+{
+    if (v) atomicAdd(&p.stats[(size_t)round * MM_STATS_COLS + col], v);
+}
+
+// As fin_play, by one thread for a component found by fin_search_thread.
+template <bool kW, bool kStats>
+__device__ __forceinline__ int fin_play_thread(const Params &p, const FinComp &cp, const uint32_t *seeds, int t0,
+                                               int cap)
+{
+    const int k = cp.k;
+    const uint32_t bar = p.ctl->barrier;
+    uint8_t st[kFinTMembers], ch[kFinTMembers];
+    int val[kFinTMembers], lastm[kFinTMembers];
+    unsigned long long recv[kFinTMembers], bkey[kFinTMembers];
+    for (int l = 0; l < k; ++l) {
+        st[l] = kBlue;  // active; coloured at the top of each round
+        val[l] = 0;
+        lastm[l] = -1;
+    }
+    int lastr = -1;
+    for (int t = t0; t < cap; ++t) {
+        bool any = false;
+        for (int l = 0; l < k; ++l) {
+            if (st[l] > kRed) continue;
+            const int g = cp.mem[l];
+            st[l] = colour_of((uint32_t)(g - base_of(p, g)), seeds[t], bar);
+            lastm[l] = t;
+            any = true;
+            if (kStats && t > t0) {  // round t0's colouring was counted by the commit that made it
+                stat_add_one(p, t, MM_ST_ACTIVE, 1ull);
+                stat_add_one(p, t, st[l] == kBlue ? MM_ST_BLUE : MM_ST_RED, 1ull);
+            }
+        }
+        if (!any) break;
+        lastr = t;
+        // request: the best red neighbour among the members
+        for (int l = 0; l < k; ++l) {
+            recv[l] = 0ull;
+            bkey[l] = 0ull;
+            ch[l] = 0;
+        }
+        for (int l = 0; l < k; ++l) {
+            if (st[l] != kBlue) continue;
+            unsigned long long best = 0ull;
+            int choice = 0;
+            for (int e = cp.eoff[l]; e < cp.eoff[l + 1]; ++e) {
+                const int tg = cp.tgt[e];
+                const uint8_t c = st[tg];
+                const unsigned long long key = c == kRed ? cp.pref[e] : (c == kMatched ? 0ull : 1ull);
+                if (key > best) {
+                    best = key;
+                    choice = tg;
+                }
+            }
+            bkey[l] = best;
+            ch[l] = (uint8_t)choice;
+        }
+        // respond: each red keeps the largest proposal key
+        for (int l = 0; l < k; ++l) {
+            if (st[l] != kBlue || bkey[l] < 2) continue;
+            const unsigned long long g = (unsigned long long)(uint32_t)~(uint32_t)cp.mem[l];
+            const unsigned long long crk = kW ? (((bkey[l] >> 32) << 32) | g) : g;
+            if (crk > recv[ch[l]]) recv[ch[l]] = crk;
+        }
+        // commit (decisions read only recv and bkey, so states update in place)
+        for (int l = 0; l < k; ++l) {
+            const int g = cp.mem[l];
+            if (st[l] == kBlue) {
+                const unsigned long long gl = (unsigned long long)(uint32_t)~(uint32_t)g;
+                const unsigned long long crk = kW ? (((bkey[l] >> 32) << 32) | gl) : gl;
+                if (kStats) {
+                    stat_add_one(p, t, MM_ST_BLUE_DEG, (unsigned long long)cp.mdeg[l]);
+                    stat_add_one(p, t, MM_ST_REQ_ENTRIES,
+                                 request_seen<kW>(cp.mbeg[l], cp.mdeg[l], bkey[l] >= 2 ? (int)~(uint32_t)bkey[l] : -1));
+                }
+                if (bkey[l] >= 2 && (uint32_t)recv[ch[l]] == (uint32_t)crk) {
+                    val[l] = 4 + min(g, cp.mem[ch[l]]) - base_of(p, g);
+                    st[l] = kMatched;
+                    if (kStats) stat_add_one(p, t, MM_ST_MATCHED, 1ull);
+                } else if (bkey[l] == 0) {
+                    val[l] = 2;
+                    st[l] = kDead;
+                }
+            } else if (st[l] == kRed) {
+                if (kStats) {
+                    stat_add_one(p, t, MM_ST_RED_DEG, (unsigned long long)cp.mdeg[l]);
+                    stat_add_one(p, t, MM_ST_RESP_ENTRIES, respond_seen<kW>(p, cp.mbeg[l], cp.mdeg[l], recv[l]));
+                }
+                if (recv[l]) {
+                    val[l] = 4 + min(g, (int)~(uint32_t)recv[l]) - base_of(p, g);
+                    st[l] = kMatched;
+                    if (kStats) stat_add_one(p, t, MM_ST_MATCHED, 1ull);
+                }
+            }
+        }
+    }
+    for (int l = 0; l < k; ++l) {
+        const int g = cp.mem[l];
+        // members still unmatched at the cap keep their last colour
+        p.ctl->match[g] = st[l] <= kRed ? (int)st[l] : val[l];
+        if (p.last) p.last[g] = (uint8_t)lastm[l];
+    }
+    return lastr;
+}
+
 // One pass of the finish phase over round t's items.  kMode:
 //   kFinPassClassify  classify every item (cls[i]) and search the root
 //                     candidates' components; call the attempt off
@@ -1496,8 +1684,21 @@ __device__ __forceinline__ void finish_pass(const Params &p, Smem &sm, int t, in
                 last_all = max(last_all, lastr);
             }
         }
-        // root candidates: search, then (unless only classifying) play
-        unsigned roots = __ballot_sync(kFull, c == kFinRootCand);
+        // root candidates: each lane searches (and, unless only classifying,
+        // plays) its own; components too large for a lane go to the warp
+        int rres = kFinNotRoot;
+        if (c == kFinRootCand) {
+            FinComp cp;
+            unsigned long long seen = 0;
+            rres = fin_search_thread<kW>(p, it.x, it.y, it.y + degree_of(it), cp,
+                                         kStats && kMode == kFinPassClassify ? &seen : nullptr);
+            if (kStats && kMode == kFinPassClassify) stat_add_one(p, t, MM_ST_FINISH_ENTRIES, seen);
+            if (rres == kFinTooBig) abort = true;
+            else if (rres == kFinRoot && kMode != kFinPassClassify)
+                last_all = max(last_all, fin_play_thread<kW, kStats>(p, cp, seeds, t, cap));
+        }
+        unsigned roots = __ballot_sync(kFull, rres == kFinOverflow);
+        if (kMode != kFinPassResolve && __any_sync(kFull, abort)) roots = 0;
         while (roots) {
             const int s = __ffs(roots) - 1;
             roots &= roots - 1;
