@@ -1103,20 +1103,24 @@ __device__ void commit_phase(const Params &p, Smem &sm, int t, bool has_next)
 //
 // The phase runs at the start of round t in two passes over the round's
 // worklist items, each ended by a grid barrier:
-//   classify  every item scans its own list: no active neighbour (a singleton),
-//             an active neighbour with a smaller id (a member: another vertex
-//             speaks for its component), or else a root candidate, which
-//             searches its component with its warp (breadth first, at most
-//             kFinMembers members and kFinEntries entries between members).
-//             A larger component, a list longer than kFinMaxDeg or an
-//             unmatchable neighbour calls the attempt off (ctl->fin_abort),
-//             and round t runs as usual.
-//   resolve   a singleton walks its own hash sequence: it leaves (match value
-//             2) in the first round it is blue, or keeps red to the round cap.
-//             A root whose search finds no smaller member plays its component
-//             in its warp, lane l holding member l: colour, request (the best
-//             red neighbour by the same keys as the scans), respond (an
-//             atomic max of the proposal keys in shared memory), commit.
+//   scan   every item scans its own list: no active neighbour (a singleton),
+//          an active neighbour with a smaller id (a member: another vertex
+//          speaks for its component), or else a root candidate.  It records
+//          its first two active neighbours with their preference keys.  A
+//          singleton walks its own hash sequence at once: it leaves (match
+//          value 2) in the first round it is blue, or keeps red to the cap.
+//   roots  each root candidate's lane follows the records breadth first to
+//          its component and, if no member has a smaller id, plays it: per
+//          round colour, request (the best red neighbour by the same keys as
+//          the scans), respond (the largest proposal key), commit.  A
+//          component that a lane cannot hold (records incomplete, more than
+//          kFinTMembers members) is searched and played by the warp, lane l
+//          holding member l (up to kFinMembers members, kFinEntries entries).
+// A larger component, a list longer than kFinMaxDeg or an unmatchable
+// neighbour calls the attempt off (ctl->fin_abort), and round t runs as
+// usual; values already written are the ones the rounds write again.  The
+// instrumented kernel checks first and resolves in a third pass, so that its
+// counters never include a called-off attempt.
 // Every vertex's match value is then final, and the matching executed
 // max(last active round) + 2 rounds, the reference's closing round included
 // (at most the cap).
@@ -1151,9 +1155,10 @@ __device__ __forceinline__ int4 item_at(const Params &p, int par, int c0, long l
 }
 
 // Own-list scan of vertex v, entries [b, e): active neighbours (blue or red),
-// whether one has a smaller id, whether a neighbour is unmatchable.
+// whether one has a smaller id, whether a neighbour is unmatchable, and the
+// positions and ids of the first two active neighbours (j0 / u0, j1 / u1).
 __device__ __forceinline__ void fin_scan_thread(const Params &p, int v, int b, int e, int &nint, bool &lower,
-                                                bool &bad)
+                                                bool &bad, int &j0r, int &u0r, int &j1r, int &u1r)
 {
     for (int j0 = b; j0 < e; j0 += 8) {
         int u[8];
@@ -1165,6 +1170,13 @@ __device__ __forceinline__ void fin_scan_thread(const Params &p, int v, int b, i
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             if (c[k] <= kRed) {
+                if (nint == 0) {
+                    j0r = j0 + k;
+                    u0r = u[k];
+                } else if (nint == 1) {
+                    j1r = j0 + k;
+                    u1r = u[k];
+                }
                 ++nint;
                 lower |= u[k] < v;
             }
@@ -1397,16 +1409,13 @@ __device__ __forceinline__ int fin_play(const Params &p, FinWarp &fw, const uint
 }
 
 // Lane-level components.  Most components of the finish round are pairs and
-// short paths, and a warp that searched and played its lanes' roots one after
-// another made each warp's roots a chain of dependent loads (about 5 roots a
-// tile on a 512 x 512 grid at round 3, 15 us each).  So each lane first
-// searches and plays its own root's component on its own, in per-thread
-// storage; a component with more than kFinTMembers members, more than
-// kFinTEntries entries between them or a member list longer than kFinTMaxDeg
-// goes to the warp-level search above.
+// short paths.  A warp that searched its lanes' roots one after another, each
+// rescanning its members' lists, made every warp a chain of dependent loads
+// (on RGG 2^20 at round 3, 9 root candidates a tile and 52 us a warp).  So each
+// lane searches its own root's component through the records and plays it in
+// per-thread storage.
 constexpr int kFinTMembers = 8;
 constexpr int kFinTEntries = 16;
-constexpr int kFinTMaxDeg = 64;
 enum : int { kFinOverflow = 3 };
 
 struct FinComp {
@@ -1419,62 +1428,62 @@ struct FinComp {
     int k;
 };
 
-// As fin_search, by one thread for root candidate v (own list [b0, e0)); or
-// kFinOverflow when the component does not fit FinComp.
-template <bool kW>
-__device__ __forceinline__ int fin_search_thread(const Params &p, int v, int b0, int e0, FinComp &cp,
-                                                 unsigned long long *scanned)
+// The finish phase's record of item i (two int4 slots in the worklist
+// memory of the other parity, which the round has not written yet):
+// rec[2i] = {u0, pref0 low, pref0 high, meta}, rec[2i + 1] = {u1, pref1 low,
+// pref1 high, 0}: its first two entries that point at an active vertex, with
+// their preference keys; meta = class | active-neighbour count << 8 (a count
+// above 2 means the record is incomplete, as for lists its warp scanned).
+constexpr int kFinRecFull = 255;  // meta count of a list whose entries are not all recorded
+
+__device__ __forceinline__ int fin_meta_class(int meta) { return meta & 0xff; }
+__device__ __forceinline__ int fin_meta_count(int meta) { return (meta >> 8) & 0xff; }
+
+// As fin_search, by one thread for root candidate v (item i), following the
+// records instead of the lists: each member costs two loads from L2 (its
+// item index, its record).  kFinOverflow when a member's record is incomplete
+// or the component does not fit FinComp.  The lists' bounds are read only
+// for the instrumented kernel's counters.
+template <bool kW, bool kStats>
+__device__ __forceinline__ int fin_search_thread(const Params &p, const int4 *rec, int v, long long i, FinComp &cp)
 {
+    long long ix[kFinTMembers];
     int k = 1, ne = 0;
     cp.mem[0] = v;
-    unsigned long long seen = 0;
+    ix[0] = i;
     for (int f = 0; f < k; ++f) {
-        const int x = cp.mem[f];
-        int b = b0, e = e0;
-        if (f > 0) {
-            const int2 r = __ldg(p.ranges + x);
-            b = r.x;
-            e = r.y > r.x ? r.y : r.x;
-        }
-        if (e - b > kFinTMaxDeg) return kFinOverflow;
+        const int4 r0 = __ldcg(rec + 2 * ix[f]);
+        const int cnt = fin_meta_count(r0.w);
+        if (cnt > 2) return kFinOverflow;
         cp.eoff[f] = (uint8_t)ne;
-        cp.mbeg[f] = b;
-        cp.mdeg[f] = e - b;
-        seen += (unsigned long long)(e - b);
-        for (int j0 = b; j0 < e; j0 += 8) {
-            int u[8];
-            float wv[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                u[q] = j0 + q < e ? __ldg(p.nbrs + j0 + q) : -1;
-                wv[q] = kW && j0 + q < e ? __ldg(p.w + j0 + q) : 0.0f;
+        if (kStats) {
+            const int2 r = __ldg(p.ranges + cp.mem[f]);
+            cp.mbeg[f] = r.x;
+            cp.mdeg[f] = r.y > r.x ? r.y - r.x : 0;
+        }
+        const int4 r1 = cnt > 1 ? __ldcg(rec + 2 * ix[f] + 1) : make_int4(0, 0, 0, 0);
+        for (int q = 0; q < cnt; ++q) {
+            const int4 rq = q == 0 ? r0 : r1;
+            const int u = rq.x;
+            if (u < v) return kFinNotRoot;
+            int slot = -1;
+            for (int m = 0; m < k; ++m)
+                if (cp.mem[m] == u) slot = m;
+            if (slot < 0) {
+                if (k == kFinTMembers) return kFinOverflow;
+                slot = k;
+                cp.mem[k] = u;
+                ix[k] = __ldcg(p.req + u).x;  // its item (written by the scan pass)
+                ++k;
             }
-            uint8_t c[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) c[q] = u[q] >= 0 ? p.col[u[q]] : (uint8_t)kMatched;
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                if (c[q] == kDead) return kFinTooBig;  // not on the symmetric path
-                if (c[q] > kRed) continue;
-                if (u[q] < v) return kFinNotRoot;
-                int slot = -1;
-                for (int m = 0; m < k; ++m)
-                    if (cp.mem[m] == u[q]) slot = m;
-                if (slot < 0) {
-                    if (k == kFinTMembers) return kFinOverflow;
-                    slot = k;
-                    cp.mem[k++] = u[q];
-                }
-                if (ne == kFinTEntries) return kFinOverflow;
-                cp.pref[ne] = kW ? cand_key<true>(j0 + q, wv[q]) : (unsigned long long)(uint32_t)~(j0 + q);
-                cp.tgt[ne] = (uint8_t)slot;
-                ++ne;
-            }
+            if (ne == kFinTEntries) return kFinOverflow;
+            cp.pref[ne] = ((unsigned long long)(uint32_t)rq.z << 32) | (uint32_t)rq.y;
+            cp.tgt[ne] = (uint8_t)slot;
+            ++ne;
         }
     }
     cp.eoff[k] = (uint8_t)ne;
     cp.k = k;
-    if (scanned) *scanned = seen;
     return kFinRoot;
 }
 
@@ -1584,142 +1593,171 @@ __device__ __forceinline__ int fin_play_thread(const Params &p, const FinComp &c
     return lastr;
 }
 
-// One pass of the finish phase over round t's items.  kMode:
-//   kFinPassClassify  classify every item (cls[i]) and search the root
-//                     candidates' components; call the attempt off
-//                     (ctl->fin_abort = t + 1) if one cannot be finished here;
-//   kFinPassResolve   resolve the singletons and play the roots' components,
-//                     from that classification;
-//   kFinPassBoth      both at once, speculatively: an item is classified and
-//                     resolved in one go, each root searched once.  If the
-//                     attempt is called off, the values already written are
-//                     the ones the following rounds write again.
-// The instrumented kernel runs the first two (its counters must not count a
-// called-off attempt's rounds); the others run the third.
-enum : int { kFinPassClassify = 0, kFinPassResolve = 1, kFinPassBoth = 2 };
+// Singletons of a tile (mine): each leaves in the first round from t on in
+// which it is blue (blue0: its colour in round t), or keeps red to the cap.
+template <bool kStats>
+__device__ __forceinline__ void fin_singles(const Params &p, const uint32_t *seeds, int t, int cap, bool mine, int v,
+                                            int deg, bool blue0, int &last_all)
+{
+    const uint32_t bar = p.ctl->barrier;
+    const uint32_t hid = mine ? (uint32_t)(v - base_of(p, v)) : 0u;
+    bool act = mine, blue = blue0;
+    int lastr = -1;
+    for (int r = t; r < cap && __any_sync(kFull, act); ++r) {
+        if (act) {
+            if (r > t) blue = colour_of(hid, seeds[r], bar) == kBlue;
+            lastr = r;
+        }
+        if (kStats) {
+            const bool b = act && blue, rd = act && !blue;
+            if (r > t) {  // round t's colouring was counted by the commit that made it
+                stat_add(p, r, MM_ST_ACTIVE, act ? 1ull : 0ull);
+                stat_add(p, r, MM_ST_BLUE, b ? 1ull : 0ull);
+                stat_add(p, r, MM_ST_RED, rd ? 1ull : 0ull);
+            }
+            stat_add(p, r, MM_ST_BLUE_DEG, b ? (unsigned long long)deg : 0ull);
+            stat_add(p, r, MM_ST_RED_DEG, rd ? (unsigned long long)deg : 0ull);
+            stat_add(p, r, MM_ST_REQ_ENTRIES, b ? (unsigned long long)deg : 0ull);
+            stat_add(p, r, MM_ST_RESP_ENTRIES, rd ? (unsigned long long)deg : 0ull);
+        }
+        if (act && blue) act = false;
+    }
+    if (mine) {
+        // still red at the cap: it keeps that colour
+        p.ctl->match[v] = act ? 1 : 2;
+        if (p.last) p.last[v] = (uint8_t)lastr;
+        last_all = max(last_all, lastr);
+    }
+}
 
-template <bool kW, bool kStats, int kMode>
-__device__ __forceinline__ void finish_pass(const Params &p, Smem &sm, int t, int par, int c0, int c1, int cap,
-                                            int *cls)
+// Finish pass 1 over round t's items: scan each item's own list (a thread
+// each, its warp for lists longer than kFinShort), classify it, record its
+// first two active neighbours (non-singletons also record their item index
+// in req[v].x), and, with kSingles, resolve the singletons at once.  Calls
+// the attempt off for a list longer than kFinMaxDeg or an unmatchable
+// neighbour.
+template <bool kW, bool kStats, bool kSingles>
+__device__ __forceinline__ void finish_scan(const Params &p, Smem &sm, int t, int par, int c0, int c1, int cap,
+                                            int4 *rec)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    FinWarp &fw = reinterpret_cast<FinWarp *>(&sm)[warp];
-    const uint32_t *seeds = sm.seeds;
     const long long A = (long long)c0 + c1;
     const long long gw = (long long)blockIdx.x * kWarps + warp, nw = (long long)gridDim.x * kWarps;
-    const uint32_t bar = p.ctl->barrier;
     bool abort = false;
     int last_all = -1;
     for (long long base = gw * 32; base < A; base += nw * 32) {
         const long long i = base + lane;
-        int c = 0;
-        int4 it = make_int4(-1, 0, 0, 0);
-        if (kMode == kFinPassResolve) {
-            c = i < A ? __ldcg(cls + i) : 0;
-            if (c == kFinSingle || c == kFinRootCand) it = item_at(p, par, c0, i);
-        } else {
-            if (i < A) it = item_at(p, par, c0, i);
-            const int deg = it.x >= 0 ? degree_of(it) : 0;
-            int nint = 0;
-            bool lower = false, bad = false;
-            if (it.x >= 0 && deg <= kFinShort) fin_scan_thread(p, it.x, it.y, it.y + deg, nint, lower, bad);
-            unsigned longs = __ballot_sync(kFull, it.x >= 0 && deg > kFinShort);
-            while (longs) {
-                const int s = __ffs(longs) - 1;
-                longs &= longs - 1;
-                const int vs = __shfl_sync(kFull, it.x, s), bs = __shfl_sync(kFull, it.y, s);
-                const int ds = __shfl_sync(kFull, deg, s);
-                if (ds > kFinMaxDeg) {
-                    if (lane == s) bad = true;
-                    continue;
-                }
-                int n2;
-                bool l2, b2;
-                fin_scan_warp(p, vs, bs, bs + ds, n2, l2, b2);
-                if (lane == s) {
-                    nint = n2;
-                    lower = l2;
-                    bad = b2;
-                }
+        const int4 it = i < A ? item_at(p, par, c0, i) : make_int4(-1, 0, 0, 0);
+        const int deg = it.x >= 0 ? degree_of(it) : 0;
+        int nint = 0, j0 = 0, u0 = 0, j1 = 0, u1 = 0;
+        bool lower = false, bad = false, complete = true;
+        if (it.x >= 0 && deg <= kFinShort) fin_scan_thread(p, it.x, it.y, it.y + deg, nint, lower, bad, j0, u0, j1, u1);
+        unsigned longs = __ballot_sync(kFull, it.x >= 0 && deg > kFinShort);
+        while (longs) {
+            const int s = __ffs(longs) - 1;
+            longs &= longs - 1;
+            const int vs = __shfl_sync(kFull, it.x, s), bs = __shfl_sync(kFull, it.y, s);
+            const int ds = __shfl_sync(kFull, deg, s);
+            if (ds > kFinMaxDeg) {
+                if (lane == s) bad = true;
+                continue;
             }
-            c = it.x < 0 ? 0 : (nint == 0 ? kFinSingle : (lower ? kFinMember : kFinRootCand));
-            if (kMode == kFinPassClassify && i < A) cls[i] = c;
-            abort |= bad;
-            if (kStats) {
-                stat_add(p, t, MM_ST_FINISH_ITEMS, it.x >= 0 ? 1ull : 0ull);
-                stat_add(p, t, MM_ST_FINISH_ENTRIES, (unsigned long long)deg);
-            }
-            if (__any_sync(kFull, abort)) break;  // the attempt is off
-        }
-        // singletons: the first round in which they are blue ends them
-        if (kMode != kFinPassClassify) {
-            const bool mine = c == kFinSingle;
-            const int v = it.x, deg = mine ? degree_of(it) : 0;
-            const uint32_t hid = mine ? (uint32_t)(v - base_of(p, v)) : 0u;
-            bool act = mine, blue = i < c0;
-            int lastr = -1;
-            for (int r = t; r < cap && __any_sync(kFull, act); ++r) {
-                if (act) {
-                    if (r > t) blue = colour_of(hid, seeds[r], bar) == kBlue;
-                    lastr = r;
-                }
-                if (kStats) {
-                    const bool b = act && blue, rd = act && !blue;
-                    if (r > t) {  // round t's colouring was counted by the commit that made it
-                        stat_add(p, r, MM_ST_ACTIVE, act ? 1ull : 0ull);
-                        stat_add(p, r, MM_ST_BLUE, b ? 1ull : 0ull);
-                        stat_add(p, r, MM_ST_RED, rd ? 1ull : 0ull);
-                    }
-                    stat_add(p, r, MM_ST_BLUE_DEG, b ? (unsigned long long)deg : 0ull);
-                    stat_add(p, r, MM_ST_RED_DEG, rd ? (unsigned long long)deg : 0ull);
-                    stat_add(p, r, MM_ST_REQ_ENTRIES, b ? (unsigned long long)deg : 0ull);
-                    stat_add(p, r, MM_ST_RESP_ENTRIES, rd ? (unsigned long long)deg : 0ull);
-                }
-                if (act && blue) act = false;
-            }
-            if (mine) {
-                // still red at the cap: it keeps that colour
-                p.ctl->match[v] = act ? 1 : 2;
-                if (p.last) p.last[v] = (uint8_t)lastr;
-                last_all = max(last_all, lastr);
+            int n2;
+            bool l2, b2;
+            fin_scan_warp(p, vs, bs, bs + ds, n2, l2, b2);
+            if (lane == s) {
+                nint = n2;
+                lower = l2;
+                bad = b2;
+                complete = false;  // its entries are not recorded
             }
         }
-        // root candidates: each lane searches (and, unless only classifying,
-        // plays) its own; components too large for a lane go to the warp
+        const int c = it.x < 0 ? 0 : (nint == 0 ? kFinSingle : (lower ? kFinMember : kFinRootCand));
+        abort |= bad;
+        if (it.x >= 0) {
+            const int cnt = nint == 0 ? 0 : (!complete ? kFinRecFull : min(nint, 3));
+            const int meta = c | (cnt << 8);
+            if (nint > 0) {
+                unsigned long long q0, q1 = 0ull;
+                if (kW) {
+                    q0 = cand_key<true>(j0, __ldg(p.w + j0));
+                    if (nint > 1 && complete) q1 = cand_key<true>(j1, __ldg(p.w + j1));
+                } else {
+                    q0 = (unsigned long long)(uint32_t)~j0;
+                    q1 = (unsigned long long)(uint32_t)~j1;
+                }
+                rec[2 * i] = make_int4(u0, (int)(uint32_t)q0, (int)(uint32_t)(q0 >> 32), meta);
+                rec[2 * i + 1] = make_int4(u1, (int)(uint32_t)q1, (int)(uint32_t)(q1 >> 32), it.x);
+                p.req[it.x].x = (int)i;
+            } else {
+                rec[2 * i] = make_int4(0, 0, 0, meta);
+            }
+        }
+        if (kStats) {
+            stat_add(p, t, MM_ST_FINISH_ITEMS, it.x >= 0 ? 1ull : 0ull);
+            stat_add(p, t, MM_ST_FINISH_ENTRIES, (unsigned long long)deg);
+        }
+        if (__any_sync(kFull, abort)) break;  // the attempt is off
+        if (kSingles) fin_singles<kStats>(p, sm.seeds, t, cap, c == kFinSingle, it.x, deg, i < c0, last_all);
+    }
+    if (abort && lane == 0) atomicExch(&p.ctl->fin_abort, t + 1);
+    if (kSingles) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) last_all = max(last_all, __shfl_xor_sync(kFull, last_all, o));
+        if (lane == 0 && last_all >= 0) atomicMax(&p.ctl->fin_last, last_all);
+    }
+}
+
+// Finish pass 2 over round t's items: each root candidate's lane searches its
+// component through the records and, with kPlay, plays it; a component that
+// a lane cannot hold goes to the warp (list scans, up to kFinMembers members),
+// and one larger than that calls the attempt off.  With kSingles (the
+// instrumented kernel's last pass) the singletons are resolved here too.
+template <bool kW, bool kStats, bool kPlay, bool kSingles>
+__device__ __forceinline__ void finish_roots(const Params &p, Smem &sm, int t, int par, int c0, int c1, int cap,
+                                             const int4 *rec)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    FinWarp &fw = reinterpret_cast<FinWarp *>(&sm)[warp];
+    const long long A = (long long)c0 + c1;
+    const long long gw = (long long)blockIdx.x * kWarps + warp, nw = (long long)gridDim.x * kWarps;
+    bool abort = false;
+    int last_all = -1;
+    for (long long base = gw * 32; base < A; base += nw * 32) {
+        const long long i = base + lane;
+        const int meta = i < A ? __ldcg(&rec[2 * i].w) : 0;
+        const int c = fin_meta_class(meta);
+        if (kSingles) {
+            const int4 it = c == kFinSingle ? item_at(p, par, c0, i) : make_int4(-1, 0, 0, 0);
+            fin_singles<kStats>(p, sm.seeds, t, cap, c == kFinSingle, it.x, c == kFinSingle ? degree_of(it) : 0,
+                                i < c0, last_all);
+        }
+        const int v = c == kFinRootCand ? __ldcg(&rec[2 * i + 1].w) : -1;
         int rres = kFinNotRoot;
         if (c == kFinRootCand) {
             FinComp cp;
-            unsigned long long seen = 0;
-            rres = fin_search_thread<kW>(p, it.x, it.y, it.y + degree_of(it), cp,
-                                         kStats && kMode == kFinPassClassify ? &seen : nullptr);
-            if (kStats && kMode == kFinPassClassify) stat_add_one(p, t, MM_ST_FINISH_ENTRIES, seen);
-            if (rres == kFinTooBig) abort = true;
-            else if (rres == kFinRoot && kMode != kFinPassClassify)
-                last_all = max(last_all, fin_play_thread<kW, kStats>(p, cp, seeds, t, cap));
+            rres = fin_search_thread<kW, kStats>(p, rec, v, i, cp);
+            if (kPlay && rres == kFinRoot) last_all = max(last_all, fin_play_thread<kW, kStats>(p, cp, sm.seeds, t, cap));
         }
         unsigned roots = __ballot_sync(kFull, rres == kFinOverflow);
-        if (kMode != kFinPassResolve && __any_sync(kFull, abort)) roots = 0;
         while (roots) {
             const int s = __ffs(roots) - 1;
             roots &= roots - 1;
             int mem, k;
             unsigned long long seen = 0;
-            const int r = fin_search<kW>(p, fw, __shfl_sync(kFull, it.x, s), &mem, &k,
-                                         kStats && kMode == kFinPassClassify ? &seen : nullptr);
-            if (kStats && kMode == kFinPassClassify && lane == 0)
-                atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_FINISH_ENTRIES], seen);
+            const int r = fin_search<kW>(p, fw, __shfl_sync(kFull, v, s), &mem, &k, kStats && !kPlay ? &seen : nullptr);
+            if (kStats && !kPlay && lane == 0) atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_FINISH_ENTRIES], seen);
             if (r == kFinTooBig) {
                 abort = true;
                 break;
             }
-            if (kMode != kFinPassClassify && r == kFinRoot)
-                last_all = max(last_all, fin_play<kW, kStats>(p, fw, seeds, t, cap, mem, k));
+            if (kPlay && r == kFinRoot) last_all = max(last_all, fin_play<kW, kStats>(p, fw, sm.seeds, t, cap, mem, k));
             __syncwarp();  // fw is reused by the next root
         }
-        if (kMode != kFinPassResolve && __any_sync(kFull, abort)) break;
+        if (__any_sync(kFull, abort)) break;
     }
-    if (kMode != kFinPassResolve && abort && lane == 0) atomicExch(&p.ctl->fin_abort, t + 1);
-    if (kMode != kFinPassClassify) {
+    if (abort && lane == 0) atomicExch(&p.ctl->fin_abort, t + 1);
+    if (kPlay) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) last_all = max(last_all, __shfl_xor_sync(kFull, last_all, o));
         if (lane == 0 && last_all >= 0) atomicMax(&p.ctl->fin_last, last_all);
@@ -1762,23 +1800,37 @@ __global__ void __launch_bounds__(kThreads, 2) k_rounds(Params p)
             const int c0 = __ldcg(&ctl->cnt[par][kBlue]), c1 = __ldcg(&ctl->cnt[par][kRed]);
             const long long act = (long long)c0 + c1;
             if (act > 0 && act * kFinDiv <= active0 && act <= fin_next) {
-                int *cls = reinterpret_cast<int *>(p.req);  // per item; req is rewritten before it is read
-                // profile: a finished round reports its first pass as the window
-                // scan and the second (instrumented kernel) as the fallback scan
+                // records: the worklist memory of the other parity (2n items, written
+                // by this round's commit only, after the phase)
+                int4 *rec = p.lists[par ^ 1][kBlue];
+                // profile: a finished round reports its first pass as the window scan,
+                // the rest as the fallback scan
                 bool done;
                 if (kStats) {
-                    finish_pass<kW, kStats, kFinPassClassify>(p, sm, t, par, c0, c1, cap, cls);
+                    // counters must not count a called-off attempt: check, then resolve
+                    finish_scan<kW, kStats, false>(p, sm, t, par, c0, c1, cap, rec);
                     if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 1)) return;
                     done = __ldcg(&ctl->fin_abort) != t + 1;
                     if (done) {
-                        finish_pass<kW, kStats, kFinPassResolve>(p, sm, t, par, c0, c1, cap, cls);
+                        finish_roots<kW, kStats, false, false>(p, sm, t, par, c0, c1, cap, rec);
+                        if (!grid_sync(p.bar, p.ctl, p.tstamp, -1)) return;
+                        done = __ldcg(&ctl->fin_abort) != t + 1;
+                    }
+                    if (done) {
+                        finish_roots<kW, kStats, true, true>(p, sm, t, par, c0, c1, cap, rec);
                         if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 2)) return;
                     }
                 } else {
-                    finish_pass<kW, kStats, kFinPassBoth>(p, sm, t, par, c0, c1, cap, cls);
+                    // speculative: a called-off attempt leaves only values that the
+                    // following rounds write again
+                    finish_scan<kW, kStats, true>(p, sm, t, par, c0, c1, cap, rec);
                     if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 1)) return;
                     done = __ldcg(&ctl->fin_abort) != t + 1;
-                    if (done && blockIdx.x == 0 && threadIdx.x == 0 && p.tstamp) p.tstamp[3 * t + 2] = p.tstamp[3 * t + 1];
+                    if (done) {
+                        finish_roots<kW, kStats, true, false>(p, sm, t, par, c0, c1, cap, rec);
+                        if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 2)) return;
+                        done = __ldcg(&ctl->fin_abort) != t + 1;
+                    }
                 }
                 if (done) {
                     if (blockIdx.x == 0 && threadIdx.x == 0) {
