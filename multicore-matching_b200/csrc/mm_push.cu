@@ -1139,6 +1139,7 @@ enum : int { kFinNotRoot = 0, kFinRoot = 1, kFinTooBig = 2 };
 struct FinWarp {
     unsigned long long pref[kFinEntries];
     unsigned long long best[kFinMembers];
+    int mem[kFinMembers];
     int eoff[kFinMembers + 1];
     int mbeg[kFinMembers];
     int mdeg[kFinMembers];
@@ -1156,9 +1157,10 @@ __device__ __forceinline__ int4 item_at(const Params &p, int par, int c0, long l
 
 // Own-list scan of vertex v, entries [b, e): active neighbours (blue or red),
 // whether one has a smaller id, whether a neighbour is unmatchable, and the
-// positions and ids of the first two active neighbours (j0 / u0, j1 / u1).
+// positions and ids of the first kFinRec active neighbours.
+constexpr int kFinRec = 4;  // active neighbours a record holds
 __device__ __forceinline__ void fin_scan_thread(const Params &p, int v, int b, int e, int &nint, bool &lower,
-                                                bool &bad, int &j0r, int &u0r, int &j1r, int &u1r)
+                                                bool &bad, int (&jr)[kFinRec], int (&ur)[kFinRec])
 {
     for (int j0 = b; j0 < e; j0 += 8) {
         int u[8];
@@ -1170,12 +1172,12 @@ __device__ __forceinline__ void fin_scan_thread(const Params &p, int v, int b, i
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             if (c[k] <= kRed) {
-                if (nint == 0) {
-                    j0r = j0 + k;
-                    u0r = u[k];
-                } else if (nint == 1) {
-                    j1r = j0 + k;
-                    u1r = u[k];
+#pragma unroll
+                for (int q = 0; q < kFinRec; ++q) {
+                    if (nint == q) {
+                        jr[q] = j0 + k;
+                        ur[q] = u[k];
+                    }
                 }
                 ++nint;
                 lower |= u[k] < v;
@@ -1428,14 +1430,14 @@ struct FinComp {
     int k;
 };
 
-// The finish phase's record of item i (two int4 slots in the worklist
-// memory of the other parity, which the round has not written yet):
-// rec[2i] = {u0, pref0 low, pref0 high, meta}, rec[2i + 1] = {u1, pref1 low,
-// pref1 high, 0}: its first two entries that point at an active vertex, with
-// their preference keys; meta = class | active-neighbour count << 8 (a count
-// above 2 means the record is incomplete, as for lists its warp scanned).
-constexpr int kFinRecFull = 255;  // meta count of a list whose entries are not all recorded
-
+// The finish phase's record of item i: four int4 slots, rec[4i .. 4i + 3], in
+// the worklist memory of the other parity (2n slots, which the round has not
+// written yet; an attempt has at most n / kFinDiv items): {meta, v, 0, 0},
+// then the ids, preference-key low halves and high halves of its first
+// kFinRec entries that point at an active vertex.  meta = class | count << 8,
+// count = its active neighbours, kFinRec + 1 if more than a record holds,
+// kFinRecFull if its warp scanned the list (not recorded).
+constexpr int kFinRecFull = 255;
 __device__ __forceinline__ int fin_meta_class(int meta) { return meta & 0xff; }
 __device__ __forceinline__ int fin_meta_count(int meta) { return (meta >> 8) & 0xff; }
 
@@ -1452,19 +1454,24 @@ __device__ __forceinline__ int fin_search_thread(const Params &p, const int4 *re
     cp.mem[0] = v;
     ix[0] = i;
     for (int f = 0; f < k; ++f) {
-        const int4 r0 = __ldcg(rec + 2 * ix[f]);
-        const int cnt = fin_meta_count(r0.w);
-        if (cnt > 2) return kFinOverflow;
+        const int4 r0 = __ldcg(rec + 4 * ix[f]);
+        const int cnt = fin_meta_count(r0.x);
+        if (cnt > kFinRec) return kFinOverflow;
         cp.eoff[f] = (uint8_t)ne;
         if (kStats) {
             const int2 r = __ldg(p.ranges + cp.mem[f]);
             cp.mbeg[f] = r.x;
             cp.mdeg[f] = r.y > r.x ? r.y - r.x : 0;
         }
-        const int4 r1 = cnt > 1 ? __ldcg(rec + 2 * ix[f] + 1) : make_int4(0, 0, 0, 0);
-        for (int q = 0; q < cnt; ++q) {
-            const int4 rq = q == 0 ? r0 : r1;
-            const int u = rq.x;
+        if (cnt == 0) continue;
+        const int4 ru = __ldcg(rec + 4 * ix[f] + 1), rl = __ldcg(rec + 4 * ix[f] + 2), rh = __ldcg(rec + 4 * ix[f] + 3);
+        const int uu[kFinRec] = {ru.x, ru.y, ru.z, ru.w};
+        const int lo[kFinRec] = {rl.x, rl.y, rl.z, rl.w};
+        const int hi[kFinRec] = {rh.x, rh.y, rh.z, rh.w};
+#pragma unroll
+        for (int q = 0; q < kFinRec; ++q) {
+            if (q >= cnt) break;
+            const int u = uu[q];
             if (u < v) return kFinNotRoot;
             int slot = -1;
             for (int m = 0; m < k; ++m)
@@ -1477,7 +1484,7 @@ __device__ __forceinline__ int fin_search_thread(const Params &p, const int4 *re
                 ++k;
             }
             if (ne == kFinTEntries) return kFinOverflow;
-            cp.pref[ne] = ((unsigned long long)(uint32_t)rq.z << 32) | (uint32_t)rq.y;
+            cp.pref[ne] = ((unsigned long long)(uint32_t)hi[q] << 32) | (uint32_t)lo[q];
             cp.tgt[ne] = (uint8_t)slot;
             ++ne;
         }
@@ -1485,112 +1492,6 @@ __device__ __forceinline__ int fin_search_thread(const Params &p, const int4 *re
     cp.eoff[k] = (uint8_t)ne;
     cp.k = k;
     return kFinRoot;
-}
-
-__device__ __forceinline__ void stat_add_one(const Params &p, int round, int col, unsigned long long v)
-{
-    if (v) atomicAdd(&p.stats[(size_t)round * MM_STATS_COLS + col], v);
-}
-
-// As fin_play, by one thread for a component found by fin_search_thread.
-template <bool kW, bool kStats>
-__device__ __forceinline__ int fin_play_thread(const Params &p, const FinComp &cp, const uint32_t *seeds, int t0,
-                                               int cap)
-{
-    const int k = cp.k;
-    const uint32_t bar = p.ctl->barrier;
-    uint8_t st[kFinTMembers], ch[kFinTMembers];
-    int val[kFinTMembers], lastm[kFinTMembers];
-    unsigned long long recv[kFinTMembers], bkey[kFinTMembers];
-    for (int l = 0; l < k; ++l) {
-        st[l] = kBlue;  // active; coloured at the top of each round
-        val[l] = 0;
-        lastm[l] = -1;
-    }
-    int lastr = -1;
-    for (int t = t0; t < cap; ++t) {
-        bool any = false;
-        for (int l = 0; l < k; ++l) {
-            if (st[l] > kRed) continue;
-            const int g = cp.mem[l];
-            st[l] = colour_of((uint32_t)(g - base_of(p, g)), seeds[t], bar);
-            lastm[l] = t;
-            any = true;
-            if (kStats && t > t0) {  // round t0's colouring was counted by the commit that made it
-                stat_add_one(p, t, MM_ST_ACTIVE, 1ull);
-                stat_add_one(p, t, st[l] == kBlue ? MM_ST_BLUE : MM_ST_RED, 1ull);
-            }
-        }
-        if (!any) break;
-        lastr = t;
-        // request: the best red neighbour among the members
-        for (int l = 0; l < k; ++l) {
-            recv[l] = 0ull;
-            bkey[l] = 0ull;
-            ch[l] = 0;
-        }
-        for (int l = 0; l < k; ++l) {
-            if (st[l] != kBlue) continue;
-            unsigned long long best = 0ull;
-            int choice = 0;
-            for (int e = cp.eoff[l]; e < cp.eoff[l + 1]; ++e) {
-                const int tg = cp.tgt[e];
-                const uint8_t c = st[tg];
-                const unsigned long long key = c == kRed ? cp.pref[e] : (c == kMatched ? 0ull : 1ull);
-                if (key > best) {
-                    best = key;
-                    choice = tg;
-                }
-            }
-            bkey[l] = best;
-            ch[l] = (uint8_t)choice;
-        }
-        // respond: each red keeps the largest proposal key
-        for (int l = 0; l < k; ++l) {
-            if (st[l] != kBlue || bkey[l] < 2) continue;
-            const unsigned long long g = (unsigned long long)(uint32_t)~(uint32_t)cp.mem[l];
-            const unsigned long long crk = kW ? (((bkey[l] >> 32) << 32) | g) : g;
-            if (crk > recv[ch[l]]) recv[ch[l]] = crk;
-        }
-        // commit (decisions read only recv and bkey, so states update in place)
-        for (int l = 0; l < k; ++l) {
-            const int g = cp.mem[l];
-            if (st[l] == kBlue) {
-                const unsigned long long gl = (unsigned long long)(uint32_t)~(uint32_t)g;
-                const unsigned long long crk = kW ? (((bkey[l] >> 32) << 32) | gl) : gl;
-                if (kStats) {
-                    stat_add_one(p, t, MM_ST_BLUE_DEG, (unsigned long long)cp.mdeg[l]);
-                    stat_add_one(p, t, MM_ST_REQ_ENTRIES,
-                                 request_seen<kW>(cp.mbeg[l], cp.mdeg[l], bkey[l] >= 2 ? (int)~(uint32_t)bkey[l] : -1));
-                }
-                if (bkey[l] >= 2 && (uint32_t)recv[ch[l]] == (uint32_t)crk) {
-                    val[l] = 4 + min(g, cp.mem[ch[l]]) - base_of(p, g);
-                    st[l] = kMatched;
-                    if (kStats) stat_add_one(p, t, MM_ST_MATCHED, 1ull);
-                } else if (bkey[l] == 0) {
-                    val[l] = 2;
-                    st[l] = kDead;
-                }
-            } else if (st[l] == kRed) {
-                if (kStats) {
-                    stat_add_one(p, t, MM_ST_RED_DEG, (unsigned long long)cp.mdeg[l]);
-                    stat_add_one(p, t, MM_ST_RESP_ENTRIES, respond_seen<kW>(p, cp.mbeg[l], cp.mdeg[l], recv[l]));
-                }
-                if (recv[l]) {
-                    val[l] = 4 + min(g, (int)~(uint32_t)recv[l]) - base_of(p, g);
-                    st[l] = kMatched;
-                    if (kStats) stat_add_one(p, t, MM_ST_MATCHED, 1ull);
-                }
-            }
-        }
-    }
-    for (int l = 0; l < k; ++l) {
-        const int g = cp.mem[l];
-        // members still unmatched at the cap keep their last colour
-        p.ctl->match[g] = st[l] <= kRed ? (int)st[l] : val[l];
-        if (p.last) p.last[g] = (uint8_t)lastm[l];
-    }
-    return lastr;
 }
 
 // Singletons of a tile (mine): each leaves in the first round from t on in
@@ -1649,9 +1550,9 @@ __device__ __forceinline__ void finish_scan(const Params &p, Smem &sm, int t, in
         const long long i = base + lane;
         const int4 it = i < A ? item_at(p, par, c0, i) : make_int4(-1, 0, 0, 0);
         const int deg = it.x >= 0 ? degree_of(it) : 0;
-        int nint = 0, j0 = 0, u0 = 0, j1 = 0, u1 = 0;
+        int nint = 0, jr[kFinRec] = {0, 0, 0, 0}, ur[kFinRec] = {0, 0, 0, 0};
         bool lower = false, bad = false, complete = true;
-        if (it.x >= 0 && deg <= kFinShort) fin_scan_thread(p, it.x, it.y, it.y + deg, nint, lower, bad, j0, u0, j1, u1);
+        if (it.x >= 0 && deg <= kFinShort) fin_scan_thread(p, it.x, it.y, it.y + deg, nint, lower, bad, jr, ur);
         unsigned longs = __ballot_sync(kFull, it.x >= 0 && deg > kFinShort);
         while (longs) {
             const int s = __ffs(longs) - 1;
@@ -1675,22 +1576,23 @@ __device__ __forceinline__ void finish_scan(const Params &p, Smem &sm, int t, in
         const int c = it.x < 0 ? 0 : (nint == 0 ? kFinSingle : (lower ? kFinMember : kFinRootCand));
         abort |= bad;
         if (it.x >= 0) {
-            const int cnt = nint == 0 ? 0 : (!complete ? kFinRecFull : min(nint, 3));
-            const int meta = c | (cnt << 8);
+            const int cnt = nint == 0 ? 0 : (!complete ? kFinRecFull : min(nint, kFinRec + 1));
+            rec[4 * i] = make_int4(c | (cnt << 8), it.x, 0, 0);
             if (nint > 0) {
-                unsigned long long q0, q1 = 0ull;
-                if (kW) {
-                    q0 = cand_key<true>(j0, __ldg(p.w + j0));
-                    if (nint > 1 && complete) q1 = cand_key<true>(j1, __ldg(p.w + j1));
-                } else {
-                    q0 = (unsigned long long)(uint32_t)~j0;
-                    q1 = (unsigned long long)(uint32_t)~j1;
-                }
-                rec[2 * i] = make_int4(u0, (int)(uint32_t)q0, (int)(uint32_t)(q0 >> 32), meta);
-                rec[2 * i + 1] = make_int4(u1, (int)(uint32_t)q1, (int)(uint32_t)(q1 >> 32), it.x);
                 p.req[it.x].x = (int)i;
-            } else {
-                rec[2 * i] = make_int4(0, 0, 0, meta);
+                if (cnt <= kFinRec) {
+                    uint32_t lo[kFinRec], hi[kFinRec];
+#pragma unroll
+                    for (int q = 0; q < kFinRec; ++q) {
+                        unsigned long long key = 0ull;
+                        if (q < cnt) key = kW ? cand_key<true>(jr[q], __ldg(p.w + jr[q])) : (unsigned long long)(uint32_t)~jr[q];
+                        lo[q] = (uint32_t)key;
+                        hi[q] = (uint32_t)(key >> 32);
+                    }
+                    rec[4 * i + 1] = make_int4(ur[0], ur[1], ur[2], ur[3]);
+                    rec[4 * i + 2] = make_int4((int)lo[0], (int)lo[1], (int)lo[2], (int)lo[3]);
+                    rec[4 * i + 3] = make_int4((int)hi[0], (int)hi[1], (int)hi[2], (int)hi[3]);
+                }
             }
         }
         if (kStats) {
@@ -1725,19 +1627,57 @@ __device__ __forceinline__ void finish_roots(const Params &p, Smem &sm, int t, i
     int last_all = -1;
     for (long long base = gw * 32; base < A; base += nw * 32) {
         const long long i = base + lane;
-        const int meta = i < A ? __ldcg(&rec[2 * i].w) : 0;
+        const int4 r0 = i < A ? __ldcg(rec + 4 * i) : make_int4(0, -1, 0, 0);
+        const int meta = r0.x;
         const int c = fin_meta_class(meta);
         if (kSingles) {
             const int4 it = c == kFinSingle ? item_at(p, par, c0, i) : make_int4(-1, 0, 0, 0);
             fin_singles<kStats>(p, sm.seeds, t, cap, c == kFinSingle, it.x, c == kFinSingle ? degree_of(it) : 0,
                                 i < c0, last_all);
         }
-        const int v = c == kFinRootCand ? __ldcg(&rec[2 * i + 1].w) : -1;
+        const int v = c == kFinRootCand ? r0.y : -1;
         int rres = kFinNotRoot;
-        if (c == kFinRootCand) {
-            FinComp cp;
-            rres = fin_search_thread<kW, kStats>(p, rec, v, i, cp);
-            if (kPlay && rres == kFinRoot) last_all = max(last_all, fin_play_thread<kW, kStats>(p, cp, sm.seeds, t, cap));
+        FinComp cp;
+        if (c == kFinRootCand) rres = fin_search_thread<kW, kStats>(p, rec, v, i, cp);
+        // the lanes' components, packed into the warp and played together, a lane
+        // per member (a lane playing its component alone would colour its
+        // members one after another)
+        unsigned pend = __ballot_sync(kFull, kPlay && rres == kFinRoot);
+        while (pend) {
+            const bool mine = (pend >> lane) & 1u;
+            const int km = mine ? cp.k : 0, nem = mine ? (int)cp.eoff[cp.k] : 0;
+            int pk = km, pe = nem;  // inclusive prefix sums in lane order
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(kFull, pk, o), z = __shfl_up_sync(kFull, pe, o);
+                if (lane >= o) {
+                    pk += y;
+                    pe += z;
+                }
+            }
+            const bool take = mine && pk <= kFinMembers && pe <= kFinEntries;
+            const unsigned batch = __ballot_sync(kFull, take);  // a prefix of pend
+            const int lastl = 31 - __clz(batch);
+            const int ktot = __shfl_sync(kFull, pk, lastl), etot = __shfl_sync(kFull, pe, lastl);
+            if (take) {
+                const int mo = pk - km, eo = pe - nem;
+                for (int l = 0; l < km; ++l) {
+                    fw.mem[mo + l] = cp.mem[l];
+                    fw.eoff[mo + l] = eo + cp.eoff[l];
+                    fw.mdeg[mo + l] = cp.mdeg[l];
+                    fw.mbeg[mo + l] = cp.mbeg[l];
+                }
+                for (int e = 0; e < nem; ++e) {
+                    fw.pref[eo + e] = cp.pref[e];
+                    fw.tgt[eo + e] = (uint8_t)(mo + cp.tgt[e]);
+                }
+            }
+            if (lane == 0) fw.eoff[ktot] = etot;
+            __syncwarp();
+            const int ml = lane < ktot ? fw.mem[lane] : 0;
+            last_all = max(last_all, fin_play<kW, kStats>(p, fw, sm.seeds, t, cap, ml, ktot));
+            __syncwarp();  // fw is refilled by the next batch
+            pend &= ~batch;
         }
         unsigned roots = __ballot_sync(kFull, rres == kFinOverflow);
         while (roots) {
@@ -2475,6 +2415,7 @@ mm_status alloc_state(mm_graph *g, PushState **out)
         set_error(std::string("push: device allocation failed: ") + cudaGetErrorString(e));
         return MM_ERR_NOMEM;
     }
+    // a parity's two lists are adjacent: the finish phase uses both as one array of 2n
     for (int par = 0; par < 2; ++par)
         for (int l = 0; l < kParityLists; ++l) s->lists[par][l] = s->list_mem + (2 * par + l) * n;
     int sms = 0, dev = 0, coop = 0;
