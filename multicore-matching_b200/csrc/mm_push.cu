@@ -1187,31 +1187,44 @@ __device__ __forceinline__ void fin_scan_thread(const Params &p, int v, int b, i
     }
 }
 
-// The same scan by a whole warp (lane-strided), for a list longer than kFinShort.
+// The same scan by a whole warp, rows of 32 entries, for a list longer than
+// kFinShort; every lane gets the results (the first kFinRec active
+// neighbours in list order too).
 __device__ __forceinline__ void fin_scan_warp(const Params &p, int v, int b, int e, int &nint, bool &lower,
-                                              bool &bad)
+                                              bool &bad, int (&jr)[kFinRec], int (&ur)[kFinRec])
 {
     const int lane = threadIdx.x & 31;
     int cnt = 0;
     bool lo = false, bd = false;
-    for (int j0 = b + lane; j0 < e; j0 += 32 * 4) {
+    for (int r0 = b; r0 < e; r0 += 32 * 4) {
         int u[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) u[k] = j0 + 32 * k < e ? __ldg(p.nbrs + j0 + 32 * k) : -1;
+        for (int k = 0; k < 4; ++k) u[k] = r0 + 32 * k + lane < e ? __ldg(p.nbrs + r0 + 32 * k + lane) : -1;
         uint8_t c[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) c[k] = u[k] >= 0 ? p.col[u[k]] : (uint8_t)kMatched;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            if (c[k] <= kRed) {
-                ++cnt;
-                lo |= u[k] < v;
-            }
+            const bool in = c[k] <= kRed;
+            lo |= in && u[k] < v;
             bd |= c[k] == kDead;
+            unsigned m = __ballot_sync(kFull, in);
+            while (m && cnt < kFinRec) {
+                const int sb = __ffs(m) - 1;
+                m &= m - 1;
+                const int us = __shfl_sync(kFull, u[k], sb);
+#pragma unroll
+                for (int q = 0; q < kFinRec; ++q) {
+                    if (cnt == q) {
+                        jr[q] = r0 + 32 * k + sb;
+                        ur[q] = us;
+                    }
+                }
+                ++cnt;
+            }
+            cnt += __popc(m);
         }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(kFull, cnt, o);
     nint = cnt;
     lower = __any_sync(kFull, lo);
     bad = __any_sync(kFull, bd);
@@ -1416,8 +1429,8 @@ __device__ __forceinline__ int fin_play(const Params &p, FinWarp &fw, const uint
 // (on RGG 2^20 at round 3, 9 root candidates a tile and 52 us a warp).  So each
 // lane searches its own root's component through the records and plays it in
 // per-thread storage.
-constexpr int kFinTMembers = 8;
-constexpr int kFinTEntries = 16;
+constexpr int kFinTMembers = 16;
+constexpr int kFinTEntries = 32;
 enum : int { kFinOverflow = 3 };
 
 struct FinComp {
@@ -1435,9 +1448,7 @@ struct FinComp {
 // written yet; an attempt has at most n / kFinDiv items): {meta, v, 0, 0},
 // then the ids, preference-key low halves and high halves of its first
 // kFinRec entries that point at an active vertex.  meta = class | count << 8,
-// count = its active neighbours, kFinRec + 1 if more than a record holds,
-// kFinRecFull if its warp scanned the list (not recorded).
-constexpr int kFinRecFull = 255;
+// count = its active neighbours, kFinRec + 1 if more than a record holds.
 __device__ __forceinline__ int fin_meta_class(int meta) { return meta & 0xff; }
 __device__ __forceinline__ int fin_meta_count(int meta) { return (meta >> 8) & 0xff; }
 
@@ -1551,7 +1562,7 @@ __device__ __forceinline__ void finish_scan(const Params &p, Smem &sm, int t, in
         const int4 it = i < A ? item_at(p, par, c0, i) : make_int4(-1, 0, 0, 0);
         const int deg = it.x >= 0 ? degree_of(it) : 0;
         int nint = 0, jr[kFinRec] = {0, 0, 0, 0}, ur[kFinRec] = {0, 0, 0, 0};
-        bool lower = false, bad = false, complete = true;
+        bool lower = false, bad = false;
         if (it.x >= 0 && deg <= kFinShort) fin_scan_thread(p, it.x, it.y, it.y + deg, nint, lower, bad, jr, ur);
         unsigned longs = __ballot_sync(kFull, it.x >= 0 && deg > kFinShort);
         while (longs) {
@@ -1563,20 +1574,24 @@ __device__ __forceinline__ void finish_scan(const Params &p, Smem &sm, int t, in
                 if (lane == s) bad = true;
                 continue;
             }
-            int n2;
+            int n2, j2[kFinRec], u2[kFinRec];
             bool l2, b2;
-            fin_scan_warp(p, vs, bs, bs + ds, n2, l2, b2);
+            fin_scan_warp(p, vs, bs, bs + ds, n2, l2, b2, j2, u2);
             if (lane == s) {
                 nint = n2;
                 lower = l2;
                 bad = b2;
-                complete = false;  // its entries are not recorded
+#pragma unroll
+                for (int q = 0; q < kFinRec; ++q) {
+                    jr[q] = j2[q];
+                    ur[q] = u2[q];
+                }
             }
         }
         const int c = it.x < 0 ? 0 : (nint == 0 ? kFinSingle : (lower ? kFinMember : kFinRootCand));
         abort |= bad;
         if (it.x >= 0) {
-            const int cnt = nint == 0 ? 0 : (!complete ? kFinRecFull : min(nint, kFinRec + 1));
+            const int cnt = min(nint, kFinRec + 1);
             rec[4 * i] = make_int4(c | (cnt << 8), it.x, 0, 0);
             if (nint > 0) {
                 p.req[it.x].x = (int)i;
