@@ -88,7 +88,13 @@ struct Ctl {
     int retired[2];        // vertices of the round that were unmatchable as soon as coloured
     int fin_abort;         // finish phase: t + 1 if the attempt in round t was called off
     int fin_last;          // finish phase: last round in which any of its vertices was active
+    int fin_round;         // finish phase: the round it starts at (set by k_rounds)
+    int fin_state;         // finish phase: kFinState*
+    long long active0;     // vertices active at round 0 (for a resumed round kernel)
 };
+
+// Finish-phase hand-over between the launches of one matching.
+enum : int { kFinStateNone = 0, kFinStatePending = 1, kFinStateDone = 2, kFinStateResume = 3 };
 
 struct Params {
     int n;
@@ -114,6 +120,7 @@ struct Params {
     unsigned long long *stats;      // [kMaxRounds][MM_STATS_COLS] or null
     unsigned long long *tstamp;     // [3 * kMaxRounds + 1] barrier times (ns) or null
     unsigned *bar;                  // [kBarWords] grid barrier words, zero at launch
+    int resume;                     // round kernel: continue from ctl->fin_round (finish called off)
     // A batch of independent graphs (a disjoint union, edges never cross): each
     // vertex's graph starts at vbase[v], and the graph's own numbering (v -
     // vbase[v]) drives the colouring and the match values, so every graph gets
@@ -140,7 +147,8 @@ struct Params {
 };
 static_assert(sizeof(Params) <= 4096, "launch parameters stay within the classic 4 KB limit");
 
-__device__ __forceinline__ int base_of(const Params &p, int v) { return p.vbase ? __ldg(p.vbase + v) : 0; }
+template <class P>
+__device__ __forceinline__ int base_of(const P &p, int v) { return p.vbase ? __ldg(p.vbase + v) : 0; }
 
 __device__ __forceinline__ int degree_of(int2 r) { return r.y > r.x ? r.y - r.x : 0; }
 __device__ __forceinline__ int degree_of(int4 it) { return it.z > it.y ? it.z - it.y : 0; }
@@ -157,7 +165,8 @@ __device__ __forceinline__ int warp_incl_scan(int v)
     return v;
 }
 
-__device__ __forceinline__ void stat_add(const Params &p, int round, int col, unsigned long long v)
+template <class P>
+__device__ __forceinline__ void stat_add(const P &p, int round, int col, unsigned long long v)
 {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFull, v, o);
@@ -1738,64 +1747,38 @@ __global__ void __launch_bounds__(kThreads, 2) k_rounds(Params p)
     const int gwarp = blockIdx.x * kWarps + (threadIdx.x >> 5);
     const int nwarps = gridDim.x * kWarps;
 
-    // the seed buffer holds 256 words (only the call's seeds are meaningful)
-    for (int i = threadIdx.x; i < 256; i += kThreads) sm.seeds[i] = p.seeds[i];
-    init_phase<kW, kStats, kPolicy>(p, sm);
-    if (!grid_sync(p.bar, p.ctl, p.tstamp, 0)) return;
-    // active vertices at round 0; round 1 clears these counters only after two
-    // more grid barriers
-    const long long active0 = (long long)__ldcg(&ctl->cnt[0][kBlue]) + __ldcg(&ctl->cnt[0][kRed]);
-    long long fin_next = active0;  // finish phase: next attempt once the active set is this small
-    int t = 0;
+    long long active0, fin_next;
+    int t;
+    if (p.resume) {
+        // the finish kernel called its attempt off: carry on from its round,
+        // without another attempt
+        if (ctl->fin_state != kFinStateResume) return;
+        t = ctl->fin_round;
+        active0 = ctl->active0;
+        fin_next = -1;
+    } else {
+        init_phase<kW, kStats, kPolicy>(p, sm);
+        if (!grid_sync(p.bar, p.ctl, p.tstamp, 0)) return;
+        // active vertices at round 0; round 1 clears these counters only after
+        // two more grid barriers
+        active0 = (long long)__ldcg(&ctl->cnt[0][kBlue]) + __ldcg(&ctl->cnt[0][kRed]);
+        if (blockIdx.x == 0 && threadIdx.x == 0) ctl->active0 = active0;
+        fin_next = active0;  // finish phase: attempt once the active set is this small
+        t = 0;
+    }
     for (;; ++t) {
         const int par = t & 1;
-        // finish phase (the symmetric path of the reference's colouring only):
-        // every block reads the same counters and takes the same branch
+        // Hand the rest to the finish kernel (the symmetric path of the
+        // reference's colouring only).  Every block reads the same counters and
+        // leaves here; round t's worklists and colours are complete.
         if (!kPolicy && p.sym && t > 0) {
-            const int c0 = __ldcg(&ctl->cnt[par][kBlue]), c1 = __ldcg(&ctl->cnt[par][kRed]);
-            const long long act = (long long)c0 + c1;
+            const long long act = (long long)__ldcg(&ctl->cnt[par][kBlue]) + __ldcg(&ctl->cnt[par][kRed]);
             if (act > 0 && act * kFinDiv <= active0 && act <= fin_next) {
-                // records: the worklist memory of the other parity (2n items, written
-                // by this round's commit only, after the phase)
-                int4 *rec = p.lists[par ^ 1][kBlue];
-                // profile: a finished round reports its first pass as the window scan,
-                // the rest as the fallback scan
-                bool done;
-                if (kStats) {
-                    // counters must not count a called-off attempt: check, then resolve
-                    finish_scan<kW, kStats, false>(p, sm, t, par, c0, c1, cap, rec);
-                    if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 1)) return;
-                    done = __ldcg(&ctl->fin_abort) != t + 1;
-                    if (done) {
-                        finish_roots<kW, kStats, false, false>(p, sm, t, par, c0, c1, cap, rec);
-                        if (!grid_sync(p.bar, p.ctl, p.tstamp, -1)) return;
-                        done = __ldcg(&ctl->fin_abort) != t + 1;
-                    }
-                    if (done) {
-                        finish_roots<kW, kStats, true, true>(p, sm, t, par, c0, c1, cap, rec);
-                        if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 2)) return;
-                    }
-                } else {
-                    // speculative: a called-off attempt leaves only values that the
-                    // following rounds write again
-                    finish_scan<kW, kStats, true>(p, sm, t, par, c0, c1, cap, rec);
-                    if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 1)) return;
-                    done = __ldcg(&ctl->fin_abort) != t + 1;
-                    if (done) {
-                        finish_roots<kW, kStats, true, false>(p, sm, t, par, c0, c1, cap, rec);
-                        if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 2)) return;
-                        done = __ldcg(&ctl->fin_abort) != t + 1;
-                    }
+                if (blockIdx.x == 0 && threadIdx.x == 0) {
+                    ctl->fin_round = t;
+                    ctl->fin_state = kFinStatePending;
                 }
-                if (done) {
-                    if (blockIdx.x == 0 && threadIdx.x == 0) {
-                        const int last = __ldcg(&ctl->fin_last);
-                        ctl->rounds = maximal ? min(last + 2, cap) : cap;
-                        if (p.tstamp) p.tstamp[3 * t + 3] = p.tstamp[3 * t + 2];
-                    }
-                    return;  // every vertex's match value is final
-                }
-                fin_next = act / 2;  // called off: try again once the active set has halved
+                return;
             }
         }
         // phase A1; the next round's counters were last read in round t - 1
@@ -1842,6 +1825,68 @@ __global__ void __launch_bounds__(kThreads, 2) k_rounds(Params p)
     for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < total; i += (long long)gridDim.x * kThreads) {
         const int v = i < cb ? __ldcg(p.lists[par][kBlue] + i).x : __ldcg(p.lists[par][kRed] + (i - cb)).x;
         match[v] = __ldcg(p.col + v);
+    }
+}
+
+// The finish phase as its own cooperative launch, after k_rounds has stopped
+// at round ctl->fin_round (its code inside the round kernel cost that kernel's
+// scan and commit loops registers: its rounds 0-4 ran 7% slower on R-MAT 2^23).
+// It returns at once if the round kernel finished the matching itself.  If the
+// attempt is called off, the resumed round kernel carries on from that round.
+template <bool kW, bool kStats>
+__global__ void __launch_bounds__(kThreads, 2) k_finish(Params p)
+{
+    extern __shared__ __align__(16) unsigned char dsmem[];
+    Smem &sm = *reinterpret_cast<Smem *>(dsmem);
+    Ctl *ctl = p.ctl;
+    if (ctl->fin_state != kFinStatePending) return;
+    const int cap = ctl->cap, maximal = ctl->maximal;
+    const int t = ctl->fin_round, par = t & 1;
+    const int c0 = ctl->cnt[par][kBlue], c1 = ctl->cnt[par][kRed];
+    // the seed buffer holds 256 words (only the call's seeds are meaningful)
+    for (int i = threadIdx.x; i < 256; i += kThreads) sm.seeds[i] = p.seeds[i];
+    __syncthreads();
+    // records: the worklist memory of the other parity (2n items, written by
+    // round t's commit only, which runs after this kernel if at all)
+    int4 *rec = p.lists[par ^ 1][kBlue];
+    // profile: the first pass is reported as round t's window scan, the rest
+    // as its fallback scan
+    bool done;
+    if (kStats) {
+        // counters must not count a called-off attempt: check, then resolve
+        finish_scan<kW, kStats, false>(p, sm, t, par, c0, c1, cap, rec);
+        if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 1)) return;
+        done = __ldcg(&ctl->fin_abort) != t + 1;
+        if (done) {
+            finish_roots<kW, kStats, false, false>(p, sm, t, par, c0, c1, cap, rec);
+            if (!grid_sync(p.bar, p.ctl, p.tstamp, -1)) return;
+            done = __ldcg(&ctl->fin_abort) != t + 1;
+        }
+        if (done) {
+            finish_roots<kW, kStats, true, true>(p, sm, t, par, c0, c1, cap, rec);
+            if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 2)) return;
+        }
+    } else {
+        // speculative: a called-off attempt leaves only values that the
+        // resumed rounds write again
+        finish_scan<kW, kStats, true>(p, sm, t, par, c0, c1, cap, rec);
+        if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 1)) return;
+        done = __ldcg(&ctl->fin_abort) != t + 1;
+        if (done) {
+            finish_roots<kW, kStats, true, false>(p, sm, t, par, c0, c1, cap, rec);
+            if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 2)) return;
+            done = __ldcg(&ctl->fin_abort) != t + 1;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (done) {
+            const int last = __ldcg(&ctl->fin_last);
+            ctl->rounds = maximal ? min(last + 2, cap) : cap;
+            ctl->fin_state = kFinStateDone;
+            if (p.tstamp) p.tstamp[3 * t + 3] = p.tstamp[3 * t + 2];
+        } else {
+            ctl->fin_state = kFinStateResume;
+        }
     }
 }
 
@@ -2354,6 +2399,7 @@ struct PushState {
     unsigned long long *tstamp = nullptr;
     unsigned *bar = nullptr;
     int grid[2][3] = {{0, 0, 0}, {0, 0, 0}};  // co-resident blocks of k_rounds by weighting and mode
+    int fgrid[2][2] = {{0, 0}, {0, 0}};       // co-resident blocks of k_finish by weighting and stats
     float2 *wfeat = nullptr;              // learned colouring: (max, mean) incident weight per vertex
 };
 
@@ -2376,6 +2422,18 @@ void free_state(PushState *s)
     dev_free(s->bar, 0);
     dev_free(s->wfeat, 0);
     delete s;
+}
+
+template <bool kW, bool kStats>
+int coresident_finish_blocks(int sms)
+{
+    int occ = 0;
+    if (cudaFuncSetAttribute(k_finish<kW, kStats>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem)) !=
+        cudaSuccess)
+        return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_finish<kW, kStats>, kThreads, sizeof(Smem)) != cudaSuccess)
+        return 0;
+    return occ * sms;
 }
 
 template <bool kW, bool kStats, bool kPolicy>
@@ -2420,8 +2478,9 @@ mm_status alloc_state(mm_graph *g, PushState **out)
     if (e == cudaSuccess)
         e = dev_alloc((void **)&s->stats, sizeof(unsigned long long) * kMaxRounds * MM_STATS_COLS, 0);
     if (e == cudaSuccess) e = dev_alloc((void **)&s->tstamp, sizeof(unsigned long long) * kStampCount, 0);
-    if (e == cudaSuccess) e = dev_alloc((void **)&s->bar, sizeof(unsigned) * kBarWords, 0);
-    if (e == cudaSuccess) e = cudaMemsetAsync(s->bar, 0, sizeof(unsigned) * kBarWords, 0);
+    // two sets of barrier words: the round kernel's and the finish kernel's
+    if (e == cudaSuccess) e = dev_alloc((void **)&s->bar, sizeof(unsigned) * 2 * kBarWords, 0);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->bar, 0, sizeof(unsigned) * 2 * kBarWords, 0);
     if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) {
         cudaDeviceSynchronize();
@@ -2443,6 +2502,10 @@ mm_status alloc_state(mm_graph *g, PushState **out)
     s->grid[1][0] = coresident_blocks<true, false, false>(sms);
     s->grid[1][1] = coresident_blocks<true, true, false>(sms);
     s->grid[1][2] = coresident_blocks<true, false, true>(sms);
+    s->fgrid[0][0] = coresident_finish_blocks<false, false>(sms);
+    s->fgrid[0][1] = coresident_finish_blocks<false, true>(sms);
+    s->fgrid[1][0] = coresident_finish_blocks<true, false>(sms);
+    s->fgrid[1][1] = coresident_finish_blocks<true, true>(sms);
     cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) {
         free_state(s);
@@ -2450,11 +2513,16 @@ mm_status alloc_state(mm_graph *g, PushState **out)
     }
     const int most = kBarMaxGroups * kBarGroup;
     bool over = false, under = false;
-    for (int a = 0; a < 2; ++a)
+    for (int a = 0; a < 2; ++a) {
         for (int b = 0; b < 3; ++b) {
             over |= s->grid[a][b] > most;
             under |= s->grid[a][b] < 1;
         }
+        for (int b = 0; b < 2; ++b) {
+            over |= s->fgrid[a][b] > most;
+            under |= s->fgrid[a][b] < 1;
+        }
+    }
     if (over) {
         free_state(s);
         set_error("push: more co-resident blocks than the grid barrier supports");
@@ -2505,6 +2573,7 @@ Params make_params(mm_graph *g, PushState *s, bool weighted, bool stats, bool ti
     p.stats = stats ? s->stats : nullptr;
     p.tstamp = timing ? s->tstamp : nullptr;
     p.bar = s->bar;
+    p.resume = 0;
     return p;
 }
 
@@ -2534,6 +2603,23 @@ mm_status launch_rounds(mm_graph *g, PushState *s, bool timing, cudaStream_t str
     MM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)k_rounds<kW, kStats, kPolicy>, dim3(s->grid[kW][mode]),
                                             dim3(kThreads), args, sizeof(Smem), stream),
                 "round kernel launch");
+    if (!kPolicy && prm.sym) {
+        // the finish kernel (its own barrier words), then the round kernel again
+        // for the case that the finish phase is called off; each returns at once
+        // when there is nothing left for it
+        Params fin = prm;
+        fin.bar = s->bar + kBarWords;
+        void *fargs[] = {&fin};
+        MM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)k_finish<kW, kStats>, dim3(s->fgrid[kW][kStats ? 1 : 0]),
+                                                dim3(kThreads), fargs, sizeof(Smem), stream),
+                    "finish kernel launch");
+        Params res = prm;
+        res.resume = 1;
+        void *rargs[] = {&res};
+        MM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)k_rounds<kW, kStats, kPolicy>, dim3(s->grid[kW][mode]),
+                                                dim3(kThreads), rargs, sizeof(Smem), stream),
+                    "round kernel launch (resumed)");
+    }
     return MM_OK;
 }
 
@@ -2598,7 +2684,7 @@ mm_status end_call(mm_graph *g, PushState *s, int nseeds, int *rounds_out, long 
 mm_status run_rounds(mm_graph *g, PushState *s, int type, bool stats, bool timing, cudaStream_t stream)
 {
     const bool w = is_weighted(type);
-    MM_CUDA_TRY(cudaMemsetAsync(s->bar, 0, sizeof(unsigned) * kBarWords, stream), "barrier clear");
+    MM_CUDA_TRY(cudaMemsetAsync(s->bar, 0, sizeof(unsigned) * 2 * kBarWords, stream), "barrier clear");
     if (stats)
         MM_CUDA_TRY(cudaMemsetAsync(s->stats, 0, sizeof(unsigned long long) * kMaxRounds * MM_STATS_COLS, stream),
                     "stats clear");
@@ -3019,7 +3105,7 @@ mm_status push_profile(mm_graph *g, int type, uint32_t barrier, const uint32_t *
             ms_phases[(size_t)r * MM_PROFILE_KERNELS + 3] = a + b + c;
         }
     }
-    if (launched) *launched = 1;
+    if (launched) *launched = (is_weighted(type) ? g->sym_weights : g->sym_struct) ? 3 : 1;
     return MM_OK;
 }
 
