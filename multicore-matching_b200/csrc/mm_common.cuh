@@ -104,6 +104,7 @@ struct mm_graph {
     long long *d_slot_off = nullptr;  // non-contiguous CSR: slot index of vertex v's first entry
     int2 *d_pwin = nullptr;           // weighted types: preference windows {neighbour, position | flag}
     long long *d_pwin_off = nullptr;  // weighted types: first window slot of each vertex; [n] = total
+    bool pwin_weights = false;        // d_pwin's second words hold weights (symmetric weighted path)
     int2 *win_build = nullptr;        // windows while being built (d_pwin once complete)
     int *win_big = nullptr;           // while being built: queued lists longer than a window chunk
 

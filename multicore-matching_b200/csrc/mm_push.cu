@@ -105,7 +105,8 @@ struct Params {
     const float *w;
     const unsigned long long *revkey;
     const long long *slot_off;
-    const int2 *pwin;               // weighted: preference windows {neighbour, position | flag}
+    const int2 *pwin;               // weighted: preference windows {neighbour, position | flag or weight}
+    int wwin;                       // pwin's second words are weights (symmetric weighted path)
     const long long *pwin_off;      // weighted: first window slot of each vertex (< 2^31)
     uint8_t *col;
     int2 *req;
@@ -312,6 +313,16 @@ __device__ __forceinline__ void propose_to(const Params &p, int v, int begin, in
         rk = __ldg(p.revkey + slot);
     }
     if (rk) atomicMax(&p.best[target], rk);
+    p.req[v] = make_int2(target, (int)(uint32_t)rk);
+}
+
+// Symmetric weighted path, windows carrying weights: blue v proposes to
+// `target` through an entry of weight w (w > -1); the target's entry for v has
+// the same weight, and v's id breaks ties (smaller first).
+__device__ __forceinline__ void propose_weight(const Params &p, int v, float w, int target)
+{
+    const unsigned long long rk = ((unsigned long long)weight_order(w) << 32) | (uint32_t)~v;
+    atomicMax(&p.best[target], rk);
     p.req[v] = make_int2(target, (int)(uint32_t)rk);
 }
 
@@ -589,6 +600,7 @@ __device__ void init_phase(const Params &p, Smem &sm)
 // fallback list.  Each thread walks kPerW vertices at once, two window entries
 // per vertex and step.
 constexpr int kPerW = 2;
+constexpr int kWinStep = 4;  // window entries per step after the first
 
 // Learned colouring, graphs with symmetric structure: a red vertex of at most
 // kRetireMaxDeg entries whose neighbours are all matched leaves in phase A of
@@ -651,7 +663,7 @@ __device__ void scan_window(const Params &p, int t, int par)
     for (long long i0 = (long long)blockIdx.x * kThreads + threadIdx.x; i0 < n_blue; i0 += stride * kPerW) {
         int4 it[kPerW];
         int wl[kPerW], cj[kPerW], ct[kPerW], seen[kPerW];
-        bool open[kPerW], alive[kPerW];
+        bool open[kPerW], alive[kPerW], found[kPerW];
 #pragma unroll
         for (int k = 0; k < kPerW; ++k) {
             const long long i = i0 + k * stride;
@@ -659,82 +671,91 @@ __device__ void scan_window(const Params &p, int t, int par)
             wl[k] = it[k].x >= 0 ? win_len(degree_of(it[k])) : 0;
             open[k] = wl[k] > 0;
             alive[k] = false;
+            found[k] = false;
             cj[k] = -1;
             ct[k] = 0;
             seen[k] = 0;
         }
-        for (int q = 0; q < kWin; q += 2) {
+        // the first step reads 2 entries (most vertices stop there in the first
+        // round), every later one kWinStep: at most 9 dependent steps for 32
+        for (int q = 0; q < kWin;) {
+            const int width = q == 0 ? 2 : kWinStep;
             bool any = false;
 #pragma unroll
             for (int k = 0; k < kPerW; ++k) any |= open[k];
             if (!any) break;
-            int nb0[kPerW], nb1[kPerW], j0[kPerW], j1[kPerW];
+            int nb[kPerW][kWinStep], jv[kPerW][kWinStep];
 #pragma unroll
             for (int k = 0; k < kPerW; ++k) {
-                nb0[k] = nb1[k] = 0;
-                j0[k] = j1[k] = 0;
-                if (!open[k]) continue;
-                if (kW) {
-                    const int4 e = __ldg(reinterpret_cast<const int4 *>(p.pwin + it[k].w + q));
-                    nb0[k] = e.x;
-                    j0[k] = e.y;
-                    nb1[k] = e.z;
-                    j1[k] = e.w;
-                } else {
-                    j0[k] = it[k].y + q;
-                    j1[k] = j0[k] + 1;
-                    nb0[k] = __ldg(p.nbrs + j0[k]);
-                    if (q + 1 < wl[k]) nb1[k] = __ldg(p.nbrs + j1[k]);
-                }
-            }
-            uint8_t c0[kPerW], c1[kPerW];
 #pragma unroll
-            for (int k = 0; k < kPerW; ++k) {
-                c0[k] = c1[k] = kMatched;
-                if (!open[k]) continue;
-                c0[k] = p.col[nb0[k]];
-                if (q + 1 < wl[k]) c1[k] = p.col[nb1[k]];
-            }
-#pragma unroll
-            for (int k = 0; k < kPerW; ++k) {
-                if (!open[k]) continue;
-                // entry q, then q + 1 (flag bit 31: a weight that can never be picked)
-                if (c0[k] == kRed && j0[k] >= 0) {
-                    cj[k] = j0[k];
-                    ct[k] = nb0[k];
-                    seen[k] += 1;
-                    open[k] = false;
-                    continue;
-                }
-                alive[k] |= c0[k] != kMatched;
-                seen[k] += 1;
-                if (q + 1 < wl[k]) {
-                    if (c1[k] == kRed && j1[k] >= 0) {
-                        cj[k] = j1[k];
-                        ct[k] = nb1[k];
-                        seen[k] += 1;
-                        open[k] = false;
-                        continue;
+                for (int h = 0; h < kWinStep / 2; ++h) {
+                    const int e = q + 2 * h;
+                    nb[k][2 * h] = nb[k][2 * h + 1] = 0;
+                    jv[k][2 * h] = jv[k][2 * h + 1] = 0;
+                    if (!open[k] || 2 * h >= width || e >= wl[k]) continue;
+                    if (kW) {
+                        const int4 x = __ldg(reinterpret_cast<const int4 *>(p.pwin + it[k].w + e));
+                        nb[k][2 * h] = x.x;
+                        jv[k][2 * h] = x.y;
+                        nb[k][2 * h + 1] = x.z;
+                        jv[k][2 * h + 1] = x.w;
+                    } else {
+                        jv[k][2 * h] = it[k].y + e;
+                        jv[k][2 * h + 1] = it[k].y + e + 1;
+                        nb[k][2 * h] = __ldg(p.nbrs + it[k].y + e);
+                        if (e + 1 < wl[k]) nb[k][2 * h + 1] = __ldg(p.nbrs + it[k].y + e + 1);
                     }
-                    alive[k] |= c1[k] != kMatched;
-                    seen[k] += 1;
                 }
-                if (q + 2 >= wl[k]) open[k] = false;
             }
+            uint8_t c[kPerW][kWinStep];
+#pragma unroll
+            for (int k = 0; k < kPerW; ++k) {
+#pragma unroll
+                for (int x = 0; x < kWinStep; ++x) {
+                    c[k][x] = kMatched;
+                    if (open[k] && x < width && q + x < wl[k]) c[k][x] = p.col[nb[k][x]];
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < kPerW; ++k) {
+                if (!open[k]) continue;
+#pragma unroll
+                for (int x = 0; x < kWinStep; ++x) {
+                    if (x >= width || q + x >= wl[k] || found[k]) continue;
+                    seen[k] += 1;
+                    // a window entry's second word: the weight (symmetric weighted
+                    // path), else the position with bit 31 set for a weight that
+                    // can never be picked; random types: the position
+                    const bool cand = !kW || (p.wwin ? __int_as_float(jv[k][x]) > -1.0f : jv[k][x] >= 0);
+                    if (c[k][x] == kRed && cand) {
+                        cj[k] = jv[k][x];
+                        ct[k] = nb[k][x];
+                        found[k] = true;
+                    } else {
+                        alive[k] |= c[k][x] != kMatched;
+                    }
+                }
+                if (found[k] || q + width >= wl[k]) open[k] = false;
+            }
+            q += width;
         }
 #pragma unroll
         for (int k = 0; k < kPerW; ++k) {
             if (it[k].x < 0) continue;
             const int v = it[k].x, deg = degree_of(it[k]);
             if (kStats) atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_WINDOW_ENTRIES], (unsigned long long)seen[k]);
-            if (cj[k] >= 0 || deg <= kWin) {
+            if (found[k] || deg <= kWin) {
                 if (kStats) {
                     atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_REQ_ENTRIES],
-                              request_seen<kW>(it[k].y, deg, cj[k]));
+                              request_seen<kW>(it[k].y, deg, found[k] ? cj[k] : -1));
                     atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_BLUE_DEG], (unsigned long long)deg);
                 }
-                if (cj[k] >= 0) propose_to<kW>(p, v, it[k].y, cj[k] & 0x7fffffff, ct[k]);
-                else no_proposal(p, v, alive[k]);
+                if (found[k]) {
+                    if (kW && p.wwin) propose_weight(p, v, __int_as_float(cj[k]), ct[k]);
+                    else propose_to<kW>(p, v, it[k].y, cj[k] & 0x7fffffff, ct[k]);
+                } else {
+                    no_proposal(p, v, alive[k]);
+                }
             } else {
                 // fallback: the whole list is scanned in phase A2
                 const unsigned long long old =
@@ -2549,6 +2570,7 @@ Params make_params(mm_graph *g, PushState *s, bool weighted, bool stats, bool ti
     p.revkey = g->d_revkey[weighted ? 1 : 0];
     p.slot_off = g->d_slot_off;
     p.pwin = g->d_pwin;
+    p.wwin = weighted && g->pwin_weights ? 1 : 0;
     p.pwin_off = g->d_pwin_off;
     p.col = s->col;
     p.req = s->req;
@@ -2969,9 +2991,31 @@ mm_status windows_end(mm_graph *g, cudaStream_t stream)
         return cuda_fail(e, "preference windows");
     }
     g->d_pwin = win;
+    g->pwin_weights = false;
     g->win_build = nullptr;
     return MM_OK;
 }
+
+namespace {
+
+// Symmetric weighted path: a window entry's second word becomes the entry's
+// weight, so a proposal needs no dependent load of it (the proposal key is the
+// weight and the proposer's id).  An entry flagged as never chosen keeps a
+// weight that fails the same test (<= -1 or NaN).
+__global__ void k_win_weights(const int2 *ranges, const float *w, const long long *pwin_off, int2 *pwin, int n)
+{
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const int wl = win_len(degree_of(ranges[v]));
+        const long long o = pwin_off[v];
+        for (int e = 0; e < wl; ++e) {
+            int2 x = pwin[o + e];
+            x.y = __float_as_int(__ldg(w + (x.y & 0x7fffffff)));
+            pwin[o + e] = x;
+        }
+    }
+}
+
+}  // namespace
 
 void windows_discard(mm_graph *g)
 {
@@ -3004,6 +3048,12 @@ mm_status push_prepare(mm_graph *g, int weighted, cudaStream_t stream)
     mm_status st = scan_graph(g, stream);
     if (st == MM_OK && !sym) st = build_revkey(g, weighted, stream);
     if (st == MM_OK && weighted && g->n > 0 && !g->d_pwin) st = build_windows(g, stream);
+    if (st == MM_OK && weighted && g->d_pwin && g->sym_weights && !g->pwin_weights) {
+        k_win_weights<<<grid_for(g->n, 256, 148 * 16), 256, 0, stream>>>(g->d_ranges, g->d_w, g->d_pwin_off, g->d_pwin,
+                                                                        g->n);
+        MM_CUDA_TRY(cudaGetLastError(), "window weights");
+        g->pwin_weights = true;
+    }
     return st;
 }
 
@@ -3140,6 +3190,7 @@ void push_release(mm_graph *g)
     windows_discard(g);
     dev_free(g->d_pwin, 0);
     g->d_pwin = nullptr;
+    g->pwin_weights = false;
     dev_free(g->d_pwin_off, 0);
     g->d_pwin_off = nullptr;
 }
