@@ -7,26 +7,35 @@ duplicates removed, FP32 weights in (0, 1], graph seed 1, colouring seeds from
 srand(12345) as the reference CLI draws them (bin/match.cpp:382), select
 barrier 0x88B81733 (bin/match.cpp:183).
 
-One step = one matching of the whole graph to maximality.
+One step = one matching of the whole graph to maximality: the round kernel,
+the finish kernel and (only if the finish phase is called off) the resumed
+round kernel, three launches on one stream.
 
-  value     edges traversed / s with the graph resident in HBM (the round loop
-            only: the reference's t1 -> t2 "match time", bin/match.cpp:436-437).
-            Edges traversed = adjacency entries the reference's request and
-            respond loops inspect, summed over rounds (the same count the TBB
-            matcher does), measured by an instrumented run.
+  value     edges traversed / s with the graph resident in HBM (the reference's
+            t1 -> t2 "match time", bin/match.cpp:436-437).  Edges traversed =
+            adjacency entries the reference's request and respond loops
+            inspect, summed over rounds (the count the TBB matcher does),
+            measured by an instrumented run.
   e2e       the same metric end to end through the C ABI with host buffers:
             upload + validation + preparation + matching + download + free per
             step (the reference's t0 -> t3 "total time").
-  roofline  the round kernel k_rounds, the only kernel of a matching (one
-            cooperative launch per step): achieved = its algorithmic bytes
-            (set-up, window, fallback and commit phases, from the instrumented run's
-            per-round counters) / the step's CUDA-event time, against the
-            measured HBM copy bandwidth.  The three round phases are also
-            reported separately, timed by the kernel's own barrier timestamps.
+  roofline  achieved = the reference's algorithmic bytes of one matching,
+            sum_r [24 |A_r| + 8 E_r] (weighted; 4 E_r random), over the step's
+            CUDA-event time, against the measured HBM copy bandwidth; traffic =
+            DRAM bytes of one matching's launches from an ncu capture recorded
+            in profiles/dram_traffic_<workload>.json.  The design's own byte
+            count of the kernels it runs, and per-round phase times (barrier
+            timestamps), are reported beside it.
   cpu_baseline  the reference's own GraphMatchingTBBWeighted (same algorithm,
             src/matchtbb.cu:567-623) compiled from its sources into
             oracle/_ref, on all host cores, on the same graph and seeds; its
-            match[] is also compared with the GPU result ("parity").
+            match[] is also compared with the GPU result ("parity").  Beside it
+            the same matcher on one thread, and the sequential matchers
+            (types 4 and 5 for weighted workloads, type 0 for random ones).
+  forms     (N = 1) plain vs batched vs learned: the 4096-graph batch matched
+            in one batched call and as 4096 separate calls, and the learned
+            colouring's shipped policy on the 2^22 R-MAT and RGG multilevel
+            hierarchies against the plain path.
 
 --impl reference runs only that CPU matcher, on the same metric.
 Multi-GPU (torchrun): for a single graph every rank matches its own replica
@@ -40,7 +49,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -132,29 +140,31 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons, sampled every 20 ms from before the
+    warm-up to the end of the timed steps and a hold period that keeps running
+    the same step until the sampling spans at least min_s seconds (a short timed
+    region alone would fall between two samples)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device_index: int):
+    def __init__(self, device_index: int, min_s: float = 1.0):
         self.dev = device_index
+        self.min_s = min_s
         self.proc = None
         self.lines = []
         self.started = threading.Event()
-        self.t0 = None  # samples that arrive from here on are inside the timed region
+        self.t0 = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
-            # nvidia-smi takes a moment to start: wait for its first line, so the
-            # timed region is sampled from its first step
-            self.started.wait(timeout=2.0)
+            self.started.wait(timeout=2.0)  # nvidia-smi takes a moment to start
         except (OSError, FileNotFoundError):
             self.proc = None
         self.t0 = time.perf_counter()
@@ -162,10 +172,13 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            now = time.perf_counter()
-            if self.t0 is not None and now >= self.t0:
+            if self.t0 is not None:
                 self.lines.append(line.strip())
             self.started.set()
+
+    def remaining(self) -> float:
+        """Seconds the hold period must still run."""
+        return self.min_s - (time.perf_counter() - self.t0) if self.proc else 0.0
 
     def __exit__(self, *exc):
         if self.proc:
@@ -191,7 +204,8 @@ class ClockSampler:
                 if val.lower() == "active":
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "window": f"warm-up, timed steps and a hold on the same step, >= {self.min_s:g} s"}
 
 
 def dist_setup():
@@ -286,17 +300,111 @@ def cpu_baseline(mm, g, t, gpu_match, workload, batch=None):
         wx, sx = oracle.weight(x, got)
         w_gpu += wx
         s_gpu += sx
-    # sequential weighted greedy (type 4) on one core: the reference's quality yardstick
-    seq = None
-    if oracle.ref_available() and t in (8, 9) and batch is None:
-        seq_m, seq_ms, _ = oracle.ref_run(g, 4, BARRIER, MATCH_SEED, nthreads=1)
-        w_seq, s_seq = oracle.weight(g, seq_m)
-        seq = {"type": 4, "ms": seq_ms, "weight": w_seq, "size": s_seq}
+    # the same TBB matcher on one thread (the reference's scaling normaliser,
+    # scaling.sh:17, results/randomscale.p:17-27) and the sequential matchers
+    # (bin/match.cpp:136-158: types 0, 4, 5), for one graph
+    one, seq = None, []
+    if oracle.ref_available() and batch is None:
+        _, ms1, _ = oracle.ref_run(g, ref_type, BARRIER, MATCH_SEED, nthreads=1, fixed_rounds=fixed)
+        one = {"ms": ms1, "value": edges / (ms1 / 1e3), "cores": 1}
+        for st in ((4, 5) if t in (8, 9) else (0,)):
+            seq_m, seq_ms, _ = oracle.ref_run(g, st, BARRIER, MATCH_SEED, nthreads=1)
+            w_seq, s_seq = oracle.weight(g, seq_m)
+            seq.append({"type": st, "ms": seq_ms, "weight": w_seq, "size": s_seq, "cores": 1})
     sample = (f"full {workload} graph, one matching" if batch is None else
               f"{len(items)} of the batch's {batch['count']} graphs (evenly spaced), one reference call each")
     return {"kind": kind, "cores": cores, "ms": ms_total, "value": edges / (ms_total / 1e3),
             "sample": sample, "parity": parity, "valid": valid, "maximal": maximal,
-            "gpu_weight": w_gpu, "gpu_size": s_gpu, "sequential": seq}
+            "gpu_weight": w_gpu, "gpu_size": s_gpu, "tbb_1_thread": one, "sequential": seq}
+
+
+def compare_batch(mm, local, seeds):
+    """The 4096-graph batch (BASELINE's batched configuration): one batched call
+    against the same graphs as 4096 separate plain calls, device time (CUDA
+    events) and rounds; per-graph parity with the reference on the sample."""
+    import torch
+
+    t = 9
+    u, batch = make_batch(mm, 4096, seed=3)
+    off = batch["offsets"]
+    out = torch.empty(u.n, dtype=torch.int32, device="cuda")
+    res = {"graphs": len(off) - 1, "n": u.n, "nnz": u.nnz}
+    with mm.DeviceGraph(u, device=local) as dg:
+        dg.set_batch(off)
+        dg.prepare(t)
+        for _ in range(2):
+            dg.match_batch(t, seeds, out.data_ptr())
+        torch.cuda.synchronize()
+        times = []
+        for _ in range(3):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            rounds = dg.match_batch(t, seeds, out.data_ptr())
+            b.record()
+            torch.cuda.synchronize()
+            times.append(a.elapsed_time(b))
+        got = out.cpu().numpy()
+        st_r, st = dg.stats(t, seeds, out.data_ptr())
+        edges = mm.roofline_bytes(st, True)["edges"]
+    res["batched"] = {"ms": min(times), "rounds_max": int(rounds.max()), "rounds_sum": int(rounds.sum()),
+                      "calls": 1, "edges_per_s": edges / (min(times) / 1e3)}
+    # the same graphs one call each (the plain path: what the reference's matcher, one graph per call, does)
+    ranges = np.asarray(u.ranges, dtype=np.int64).reshape(-1, 2)
+    graphs = []
+    for i in range(len(off) - 1):
+        lo, hi = int(off[i]), int(off[i + 1])
+        e0, e1 = int(ranges[lo, 0]), int(ranges[hi - 1, 1]) if hi > lo else int(ranges[lo, 0])
+        r = (ranges[lo:hi] - e0).astype(np.int32)
+        graphs.append(mm.Graph(hi - lo, r, u.nbrs[e0:e1] - lo, u.weights[e0:e1], f"batch-{i}"))
+    dgs = [mm.DeviceGraph(x, device=local) for x in graphs]
+    try:
+        for d in dgs:
+            d.prepare(t)
+        torch.cuda.synchronize()
+        rs, ms_dev = [], 0.0
+        t0 = time.perf_counter()
+        for i, d in enumerate(dgs):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            rs.append(d.match_device(t, seeds, out.data_ptr() + 4 * int(off[i])) if graphs[i].n else 0)
+            b.record()
+            b.synchronize()
+            ms_dev += a.elapsed_time(b)
+        wall = (time.perf_counter() - t0) * 1e3
+    finally:
+        for d in dgs:
+            d.close()
+    same = bool(np.array_equal(out.cpu().numpy(), got)) and [int(x) for x in rounds] == [int(x) for x in rs]
+    res["plain_calls"] = {"ms_device": ms_dev, "ms_wall": wall, "rounds_max": int(max(rs)), "rounds_sum": int(sum(rs)),
+                          "calls": len(dgs), "same_result_as_batched": same}
+    cpu = cpu_baseline(mm, u, t, got, "batch4096_weighted_maximal", batch)
+    res["parity_sample"] = {"graphs": len(batch["sample"]), "bit_exact_vs_reference": cpu["parity"],
+                            "valid": cpu["valid"], "maximal": cpu["maximal"]}
+    return res
+
+
+def compare_learned(mm, local, seeds):
+    """The learned colouring's shipped policy against the plain path on the
+    2^22 R-MAT and RGG multilevel hierarchies (BASELINE's learned configuration):
+    rounds, device time (best of 3) and matching weight summed over levels."""
+    spec = __import__("importlib.util").util.spec_from_file_location(
+        "multicore_matching_b200.policy", ROOT / "multicore-matching_b200" / "policy.py")
+    pol = __import__("importlib.util").util.module_from_spec(spec)
+    spec.loader.exec_module(pol)
+    mlp = pol.load_policy()
+    out = {}
+    for name, g in (("rmat22", mm.Graph.rmat(22, 16, 0.57, 0.19, 0.19, seed=1)),
+                    ("rgg22", mm.Graph.rgg(1 << 22, 13.0, seed=7))):
+        levels = pol.hierarchy(mm, g, 9, seeds, device=local)
+        rows = pol.evaluate(mm, levels[:-1], 9, seeds, mlp, repeats=3, device=local)
+        tot = {arm: {"rounds": int(sum(r[arm]["rounds"] for r in rows)), "ms": float(sum(r[arm]["ms"] for r in rows)),
+                     "weight": float(sum(r[arm]["weight"] for r in rows)),
+                     "valid_maximal": all(r[arm]["valid"] and r[arm]["maximal"] for r in rows)}
+               for arm in ("plain", "learned")}
+        tot["levels"] = len(rows)
+        tot["weight_change"] = tot["learned"]["weight"] / max(tot["plain"]["weight"], 1e-300) - 1.0
+        out[name] = tot
+    return out
 
 
 def main():
@@ -309,6 +417,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="rmat23_weighted_maximal", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the plain vs batched vs learned comparisons")
     ap.add_argument("--ncu-case", action="store_true",
                     help="build + prepare, then one host-stepped matching only (for ncu captures of the kernels)")
     args = ap.parse_args()
@@ -366,14 +475,14 @@ def main():
 
     # L2 is 126 MB; the CSR alone is > 1 GB, and a 512 MB write flushes L2 between steps.
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
-    for _ in range(args.warmup):
-        dg.match_device(t, seeds, out.data_ptr(), stream=sptr)
-    torch.cuda.synchronize()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
+        for _ in range(args.warmup):
+            dg.match_device(t, seeds, out.data_ptr(), stream=sptr)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
         with torch.cuda.stream(stream):
             for i in range(args.steps):
                 flush.fill_(i & 0xFF)
@@ -381,8 +490,15 @@ def main():
                 r = dg.match_device(t, seeds, out.data_ptr(), stream=sptr)
                 evs[i][1].record(stream)
         torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+        if dist:
+            dist.barrier()
+        # hold: the same step until the clock samples span at least a second
+        while clocks.remaining() > 0:
+            with torch.cuda.stream(stream):
+                for _ in range(50):
+                    flush.fill_(1)
+                    dg.match_device(t, seeds, out.data_ptr(), stream=sptr)
+            torch.cuda.synchronize()
     step_ms = [a.elapsed_time(b) for a, b in evs]
     ms = statistics.mean(step_ms)
     if dist:
@@ -394,26 +510,25 @@ def main():
     prof = []
     for _ in range(3):
         flush.fill_(1)
-        _, ms_k, _ = dg.profile(t, seeds, out.data_ptr(), stream=sptr)
+        _, ms_k, launches = dg.profile(t, seeds, out.data_ptr(), stream=sptr)
         prof.append(ms_k)
     nr = min(x.shape[0] for x in prof)
     ms_k = np.mean(np.stack([x[:nr] for x in prof]), axis=0)  # [executed rounds, (window, fallback, commit, sum)]
-    gpu_launches = args.steps * 1
+    gpu_launches = args.steps * launches
     phase_bytes = {"window": work["window_bytes"][:nr], "fallback": work["fallback_bytes"][:nr],
                    "commit": work["commit_bytes"][:nr]}
     kernel_bytes = work["kernel_bytes"]
-    # the round kernel is the only kernel of a matching: its bytes over the whole step's device time
-    achieved = kernel_bytes / (ms / 1e3) / 1e9
+    # the reference's algorithmic bytes of this rank's matching over the step's device time
+    achieved = work["reference_bytes"] / (ms / 1e3) / 1e9
     peak, peak_kind = load_peaks()
     # the scans are bound by random single-sector reads: their measured ceiling on this device
     gather_peak = mm.probe_gather_rate(local, max(g.n, 1))
     colour_gathers = float(st[:, mm.ST_WINDOW_ENTRIES].sum() + st[:, mm.ST_STAGED_DEG].sum())
-    # DRAM bytes of one k_rounds launch from an ncu capture of this workload, where one exists
+    # DRAM bytes of one matching's launches from an ncu capture of this workload, where one exists
     traffic = None
-    tfile = ROOT / "profiles" / "dram_traffic_k_rounds_rmat_weighted_maximal.md"
+    tfile = ROOT / "profiles" / f"dram_traffic_{args.workload}.json"
     if tfile.exists():
-        m = re.search(rf"dram_bytes_per_launch \({re.escape(args.workload)}\): (\d+)", tfile.read_text())
-        traffic = int(m.group(1)) if m else None
+        traffic = json.loads(tfile.read_text()).get("dram_bytes_per_step")
 
     # end to end through the C ABI with host buffers (pinned)
     ranges_h = torch.from_numpy(np.ascontiguousarray(g.ranges, dtype=np.int32)).pin_memory()
@@ -483,6 +598,13 @@ def main():
         torch.cuda.synchronize()
         cpu = cpu_baseline(mm, g, t, gpu_m.cpu().numpy(), args.workload, batch)
     dg.close()
+    del flush
+    forms = None
+    if rank == 0 and world == 1 and not args.no_forms and batch is None:
+        torch.cuda.empty_cache()
+        mm.lib().mm_release_cached_memory(local)
+        forms = {"batch4096_weighted_maximal": compare_batch(mm, local, seeds),
+                 "learned_multilevel22_weighted_maximal": compare_learned(mm, local, seeds)}
 
     if rank == 0:
         line = {
@@ -499,10 +621,18 @@ def main():
             "e2e": {"value": e2e_value, "unit": "edges/s", "ms_per_step": e2e, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_create": e2e_split[0], "ms_first_match": e2e_split[1],
                     "ms_destroy": e2e_split[2], **e2e_detail},
-            "roofline": {"bound": "hbm", "kernel": "k_rounds (whole matching: set-up, scan and commit phases)",
+            "roofline": {"bound": "hbm",
+                         "kernel": "one matching: k_rounds then k_finish (a resumed k_rounds only if the finish "
+                                   "phase is called off)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "peak_kind": peak_kind,
-                         "bytes_per_launch": kernel_bytes, "launches_per_step": 1,
+                         "bytes_per_step": work["reference_bytes"],
+                         "bytes_formula": "sum over rounds r of 24 |A_r| + (4 + 4 weighted) E_r: the reference's "
+                                          "round loop (A_r active vertices, E_r entries its request and respond "
+                                          "loops inspect)",
+                         "launches_per_step": launches,
+                         "design_bytes_per_step": kernel_bytes,
+                         "design_frac": kernel_bytes / (ms / 1e3) / 1e9 / peak,
                          "phases": {k: {"ms": float(ms_k[:, c].sum()), "bytes": float(phase_bytes[k].sum()),
                                         "gbs": float(phase_bytes[k].sum() / max(ms_k[:, c].sum(), 1e-9) / 1e6),
                                         "frac": float(phase_bytes[k].sum() / max(ms_k[:, c].sum(), 1e-9) / 1e6 / peak)}
@@ -514,7 +644,6 @@ def main():
                          "per_round_ms": {"window": [round(float(x), 4) for x in ms_k[:, 0]],
                                           "fallback": [round(float(x), 4) for x in ms_k[:, 1]],
                                           "commit": [round(float(x), 4) for x in ms_k[:, 2]]},
-                         "reference_formula_gbs": work["reference_bytes"] / (ms / 1e3) / 1e9,
                          "random_reads": {"ceiling_per_s": gather_peak, "ceiling": "mm_probe_gather_rate, table of n bytes",
                                           "colour_gathers_per_step": colour_gathers,
                                           "colour_gathers_per_s": colour_gathers / (ms / 1e3)}},
@@ -523,10 +652,13 @@ def main():
         }
         if cpu is not None:
             line["cpu_baseline"] = {"value": cpu["value"], "unit": "edges/s", "cores": cpu["cores"],
-                                    "kind": cpu["kind"], "sample": cpu["sample"], "ms": cpu["ms"]}
+                                    "kind": cpu["kind"], "sample": cpu["sample"], "ms": cpu["ms"],
+                                    "matcher": "GraphMatchingTBB (src/matchtbb.cu) on all host cores",
+                                    "tbb_1_thread": cpu["tbb_1_thread"], "sequential": cpu["sequential"]}
             line["parity"] = {"bit_exact_vs_reference": cpu["parity"], "valid": cpu["valid"],
-                              "maximal": cpu["maximal"], "weight": cpu["gpu_weight"], "size": cpu["gpu_size"],
-                              "sequential_greedy": cpu["sequential"]}
+                              "maximal": cpu["maximal"], "weight": cpu["gpu_weight"], "size": cpu["gpu_size"]}
+        if forms is not None:
+            line["forms"] = forms
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -512,6 +512,9 @@ def roofline_bytes(stats: np.ndarray, weighted: bool) -> dict:
         matched vertex (match value 4 written, no next item).
     init_bytes: the set-up pass, 33 per vertex (range 8, colour 1, best key 8,
         worklist item 16), 41 with the weighted types' window offset.
+    finish_bytes[r]: the finish phase (round r): 84 per item (worklist item 16,
+        record 64, match value 4) and 5 per adjacency entry its list scans read
+        (neighbour id 4, colour 1).
     edges: sum_r E_r (edges traversed, for TEPS).
     """
     ew = 8 if weighted else 4
@@ -525,6 +528,17 @@ def roofline_bytes(stats: np.ndarray, weighted: bool) -> dict:
     window = 32 * blue + (8 if weighted else 4) * win
     fallback = ew * fb + 36 * pieces
     commit = 41 * act - 12 * matched
+    finish = 84 * stats[:, ST_FINISH_ITEMS].astype(np.float64) + 5 * stats[:, ST_FINISH_ENTRIES].astype(np.float64)
+    # From the round in which the finish phase completed, the rounds are played
+    # inside it: no window, fallback or commit pass runs.  (A called-off attempt
+    # is followed by a window scan in the same round.)
+    ran = np.nonzero(stats[:, ST_FINISH_ITEMS] > 0)[0]
+    if len(ran):
+        r = int(ran[-1])
+        if not (stats[r:, ST_WINDOW_ENTRIES].any() or stats[r:, ST_STAGED_DEG].any()):
+            window[r:] = 0.0
+            fallback[r:] = 0.0
+            commit[r:] = 0.0
     init = (41 if weighted else 33) * float(act[0]) if len(act) else 0.0
     return {
         "edges": float(e.sum()),
@@ -532,8 +546,9 @@ def roofline_bytes(stats: np.ndarray, weighted: bool) -> dict:
         "window_bytes": window,
         "fallback_bytes": fallback,
         "commit_bytes": commit,
+        "finish_bytes": finish,
         "init_bytes": init,
-        "kernel_bytes": float(window.sum() + fallback.sum() + commit.sum() + init),
+        "kernel_bytes": float(window.sum() + fallback.sum() + commit.sum() + finish.sum() + init),
     }
 
 
