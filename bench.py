@@ -319,7 +319,8 @@ def cpu_baseline(mm, g, t, gpu_match, workload, batch=None):
 
 
 def compare_batch(mm, local, seeds):
-    """The 4096-graph batch (BASELINE's batched configuration): one batched call
+    """The 4096-graph batch workload (independent graphs, 2^10 to 2^18 vertices,
+    grid / random geometric / Erdos-Renyi, weighted maximal): one batched call
     against the same graphs as 4096 separate plain calls, device time (CUDA
     events) and rounds; per-graph parity with the reference on the sample."""
     import torch
@@ -385,7 +386,7 @@ def compare_batch(mm, local, seeds):
 
 def compare_learned(mm, local, seeds):
     """The learned colouring's shipped policy against the plain path on the
-    2^22 R-MAT and RGG multilevel hierarchies (BASELINE's learned configuration):
+    2^22 R-MAT and RGG multilevel hierarchies (coarsened to 1% of the vertices):
     rounds, device time (best of 3) and matching weight summed over levels."""
     spec = __import__("importlib.util").util.spec_from_file_location(
         "multicore_matching_b200.policy", ROOT / "multicore-matching_b200" / "policy.py")

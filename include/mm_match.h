@@ -191,10 +191,14 @@ mm_status mm_match_profile(mm_graph *g, int type, uint32_t barrier, const uint32
  * weights) and d_match_out are the caller's own DEVICE arrays on the current
  * device; seeds are host values.  Same result and round count as mm_match.
  * Scratch lives in a fixed device array inside the library: at most 1048576
- * vertices (larger n returns MM_ERR_UNSUPPORTED), held on every GPU that loads
- * the library until the process exits.  The first call on a device looks up
- * that array (make it before any stream capture).  All calls share the array:
- * calls that overlap on the GPU race.  Calls no cudaMalloc / cudaFree.
+ * vertices (larger n returns MM_ERR_UNSUPPORTED).  The array (4 MiB) is placed
+ * on a device by the first call there, which also loads the kernels and may
+ * synchronise the device, and is held until the process exits: make one call at
+ * start-up for each device and type you use.  That first call also looks up the
+ * array's address (make it before any stream capture; do not call this after a
+ * cudaDeviceReset of that device).  d_ranges must be 8-byte aligned
+ * (MM_ERR_ARG).  All calls share the array: calls that overlap on the GPU race.
+ * Calls no cudaMalloc / cudaFree.
  */
 mm_status mm_match_noalloc(int n, const int *d_ranges, long long nnz, const int *d_neighbours,
                            const float *d_weights, int type, uint32_t barrier, const uint32_t *seeds,

@@ -95,23 +95,26 @@ def build_mmgen(verbose: bool = False) -> Path:
     return out
 
 
-def build_oracle(verbose: bool = False) -> None:
-    """The CPU checker: restatement always, reference build when its sources exist."""
-    target = ["ref"] if Path("/root/reference/src/matchtbb.cu").exists() else ["all"]
+def build_oracle(verbose: bool = False, ref_src: str | None = None) -> None:
+    """The CPU checker: the restatement always; the reference's own matchers too
+    when ref_src (or the environment's MM_REFERENCE_SRC) names the reference's
+    src/ directory."""
+    ref_src = ref_src or os.environ.get("MM_REFERENCE_SRC")
+    target = ["ref"] if ref_src and (Path(ref_src) / "matchtbb.cu").exists() else ["all"]
     env = dict(os.environ)
     env.pop("CC", None)
     env.pop("CXX", None)
-    cmd = ["make", "-s", "-C", str(ROOT / "oracle"), *target]
+    cmd = ["make", "-s", "-C", str(ROOT / "oracle"), *target] + ([f"REF_SRC={ref_src}"] if target == ["ref"] else [])
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True, env=env)
 
 
-def build_all(verbose: bool = False) -> None:
+def build_all(verbose: bool = False, ref_src: str | None = None) -> None:
     build_mmatch(verbose)
     build_mtc(verbose)
     build_mmgen(verbose)
-    build_oracle(verbose)
+    build_oracle(verbose, ref_src)
 
 
 if __name__ == "__main__":

@@ -18,14 +18,21 @@
 //
 // Limits and rules:
 //   * at most kNoAllocMaxVertices vertices; larger graphs get MM_ERR_UNSUPPORTED;
-//   * the array exists once per device for the life of the process (4 MiB plus
-//     256 bytes on every GPU that loads this library);
-//   * the first call on a device looks up the array's device address (with that
-//     device current); make that first call before any stream capture;
+//   * the array takes 4 MiB plus 256 bytes on a device.  The CUDA runtime loads
+//     this library's device code lazily, so the array is placed on a device by
+//     the first call there (which also loads the kernels and may synchronise the
+//     device), then held until the process exits: a caller that must not allocate
+//     later makes one call at start-up, for each device and matching type it uses;
+//   * the first call on a device also looks up the array's device address (with
+//     that device current), kept for the life of the process: make that first call
+//     before any stream capture, and do not use this entry point on a device
+//     after cudaDeviceReset in the same process;
+//   * d_ranges is read as int2 pairs and must be 8-byte aligned (else MM_ERR_ARG);
 //   * every call shares the array and leaves its contents behind: calls that
 //     overlap on the GPU (two streams, two threads) race and must not be made.
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <mutex>
 #include <string>
 
@@ -194,6 +201,10 @@ MM_API mm_status mm_match_noalloc(int n, const int *d_ranges, long long nnz, con
     if (nnz >= (1ll << 31)) {
         set_error("mm_match_noalloc: nnz must be below 2^31");
         return MM_ERR_UNSUPPORTED;
+    }
+    if (((uintptr_t)d_ranges & 7u) != 0) {
+        set_error("mm_match_noalloc: d_ranges must be 8-byte aligned (it is read as int2 pairs)");
+        return MM_ERR_ARG;
     }
     int *scratch = nullptr;
     mm_status s = scratch_address(&scratch);

@@ -295,7 +295,7 @@ def test_errors_are_statuses(mm, orc, torch_cuda):
 
 
 def test_rgg_config_full_size(mm, orc, torch_cuda):
-    """BASELINE config 2 at full size: 2^20-vertex RGG, weighted, seed 7."""
+    """The random geometric graph at full size: 2^20 vertices, average degree 13, weighted, seed 7."""
     g = mm.Graph.rgg(1 << 20, 13.0, seed=7)
     seeds = orc.rand_seeds(12345, 256)
     with mm.DeviceGraph(g, device=0) as dg:

@@ -20,8 +20,11 @@ pytestmark = pytest.mark.gpu
 BARRIER = 0x88B81733
 
 
-def noalloc(mm, torch, g, type_, seeds, d_ranges, d_nbrs, d_w, barrier=BARRIER):
-    out = torch.full((max(g.n, 1),), -9, dtype=torch.int32, device="cuda")
+def noalloc(mm, torch, g, type_, seeds, d_ranges, d_nbrs, d_w, barrier=BARRIER, out=None):
+    if out is None:
+        out = torch.full((max(g.n, 1),), -9, dtype=torch.int32, device="cuda")
+    else:
+        out.fill_(-9)
     rounds = ctypes.c_int(0)
     seeds = np.ascontiguousarray(seeds, dtype=np.uint32)
     st = mm.lib().mm_match_noalloc(g.n, d_ranges, g.nnz, d_nbrs, d_w, type_, barrier, seeds.ctypes.data,
@@ -48,9 +51,14 @@ def test_noalloc_entry_matches_default_entry(mm, orc):
                     want_rounds = dg.match_device(t, seeds, want.data_ptr())
                     torch.cuda.synchronize()
                     want = want.cpu().numpy()
+                    out = torch.empty(max(g.n, 1), dtype=torch.int32, device="cuda")
                     for call in range(2):  # two calls in a row share the fixed scratch
+                        torch.cuda.synchronize()
+                        free0 = torch.cuda.mem_get_info()[0]
                         st, got, rounds = noalloc(mm, torch, g, t, seeds, ranges.data_ptr(), nbrs.data_ptr(),
-                                                  w.data_ptr())
+                                                  w.data_ptr(), out=out)
+                        if call == 1:  # after the first call the array is in place: nothing more is taken
+                            assert torch.cuda.mem_get_info()[0] == free0, (g.name, t, seed)
                         assert st == 0, mm.lib().mm_last_error()
                         assert rounds == want_rounds, (g.name, t, seed, call)
                         assert np.array_equal(got, want), (g.name, t, seed, call, int((got != want).sum()))
@@ -74,3 +82,8 @@ def test_noalloc_limits_and_errors(mm):
     st = lib.mm_match_noalloc(3, ranges.data_ptr(), 3, nbrs.data_ptr(), None, 7, BARRIER, seeds.ctypes.data, 255,
                               out.data_ptr(), ctypes.byref(r), None)
     assert st == 2
+    # ranges are read as int2 pairs: a misaligned view is refused before any kernel runs
+    wide = torch.zeros(8, dtype=torch.int32, device="cuda")
+    st = lib.mm_match_noalloc(3, wide.data_ptr() + 4, 3, nbrs.data_ptr(), None, 7, BARRIER, seeds.ctypes.data, 255,
+                              out.data_ptr(), ctypes.byref(r), None)
+    assert st == 1 and b"8-byte aligned" in lib.mm_last_error()
