@@ -151,6 +151,18 @@ mm_status mm_match(mm_graph *g, int type, uint32_t barrier, const uint32_t *seed
 mm_status mm_match_device(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds,
                           int nseeds, int *d_match_out, int *rounds_out, void *stream);
 
+/*
+ * As mm_match_device, but each round's seed comes from draw(ctx), called once
+ * as the round starts -- exactly once per executed round, the final round of
+ * a maximal matching included, as the reference draws host rand() values
+ * (src/matchgpu.cu:509, 609, 707, 816).  Runs the reference-structured kernels
+ * one round at a time from the host (MM_PATH_PULL), since the rounds cannot
+ * be known ahead.  For callers whose seed source cannot be read ahead, such
+ * as a rand() whose state layout is unknown.  Single graphs only.
+ */
+mm_status mm_match_drawn(mm_graph *g, int type, uint32_t barrier, uint32_t (*draw)(void *ctx), void *ctx,
+                         int *d_match_out, int *rounds_out, void *stream);
+
 /* As mm_match_device with an explicit kernel family (MM_PATH_*). */
 mm_status mm_match_ex(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds,
                       int *d_match_out, int *rounds_out, int path, void *stream);
@@ -293,6 +305,31 @@ mm_status mm_graph_contract(mm_graph *g, const int *d_match, mm_graph **coarse, 
  * bandwidth, so this is the ceiling their rate is reported against.
  */
 mm_status mm_probe_gather_rate(int device, long long table_bytes, double *gathers_per_s);
+
+/*
+ * Testing hook, no counterpart in the reference: lets tests drive the library's
+ * failure handling without any GPU fault.  Process-wide; not for production
+ * use.  *out (may be NULL) receives the previous value, or the queried one.
+ *   MM_DEBUG_SPIN_LIMIT    polls a grid-barrier wait of the round and finish
+ *                          kernels makes before giving up (0: the default,
+ *                          2^22); a wait that gives up makes the call return
+ *                          MM_ERR_DEVICE
+ *   MM_DEBUG_SKIP_BARRIER  mark of a grid barrier at which block 0 does not
+ *                          arrive, so every wait on it runs out (-1: none);
+ *                          marks: 0 after set-up, 3r + 1 after round r's
+ *                          window scan, 3r + 3 after its commit
+ *   MM_DEBUG_ALLOC_LIMIT   bytes in use in the device pool above which
+ *                          allocations fail as out of memory (-1: none)
+ *   MM_DEBUG_POOL_USED     query (value ignored): bytes in use in the current
+ *                          device's pool, after synchronising the device
+ */
+enum {
+    MM_DEBUG_SPIN_LIMIT = 1,
+    MM_DEBUG_SKIP_BARRIER = 2,
+    MM_DEBUG_ALLOC_LIMIT = 3,
+    MM_DEBUG_POOL_USED = 4
+};
+mm_status mm_debug(int key, long long value, long long *out);
 
 /* Message of the calling thread's most recent failure ("" if none). */
 const char *mm_last_error(void);

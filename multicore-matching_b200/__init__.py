@@ -83,6 +83,7 @@ _MM_SIGS = {
     "mm_match": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P]),
     "mm_match_device": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P]),
     "mm_match_ex": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _I, _P]),
+    "mm_match_drawn": (_I, [_P, _I, _U, _P, _P, _P, ctypes.POINTER(_I), _P]),
     "mm_match_stats": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P, _I, _I, _P]),
     "mm_matching_weight": (_I, [_P, _P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_LL), _P]),
     "mm_matching_check": (_I, [_P, _P, _P, ctypes.POINTER(_I), _P]),
@@ -94,6 +95,7 @@ _MM_SIGS = {
     "mm_probe_gather_rate": (_I, [_I, _LL, ctypes.POINTER(ctypes.c_double)]),
     "mm_match_profile": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P, _I, ctypes.POINTER(_I), _P]),
     "mm_match_noalloc": (_I, [_I, _P, _LL, _P, _P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P]),
+    "mm_debug": (_I, [_I, _LL, ctypes.POINTER(_LL)]),
     "mm_last_error": (ctypes.c_char_p, []),
     "mm_version": (ctypes.c_char_p, []),
 }

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <atomic>
 #include <mutex>
 #include <new>
 #include <string>
@@ -38,6 +39,10 @@ mm_status cuda_fail(cudaError_t e, const char *what)
 // mm_release_cached_memory hands the unused part back to the driver.
 
 namespace {
+// testing hooks (mm_debug)
+std::atomic<long long> g_dbg_spin_limit{0};   // 0: the kernels' own limit
+std::atomic<int> g_dbg_skip_mark{-1};
+std::atomic<long long> g_dbg_alloc_limit{-1};  // pool bytes in use above which allocations fail
 std::mutex g_pool_mu;
 constexpr int kMaxDevices = 256;
 cudaMemPool_t g_pools[kMaxDevices] = {};
@@ -82,9 +87,23 @@ cudaError_t dev_alloc(void **p, size_t bytes, cudaStream_t stream)
     cudaError_t e = cudaGetDevice(&device);
     cudaMemPool_t pool = nullptr;
     if (e == cudaSuccess) e = device_pool(device, &pool);
+    const long long limit = g_dbg_alloc_limit.load();
+    if (e == cudaSuccess && limit >= 0) {
+        uint64_t used = 0;
+        e = cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
+        if (e == cudaSuccess && (long long)(used + bytes) > limit) return cudaErrorMemoryAllocation;
+    }
     if (e == cudaSuccess) e = cudaMallocFromPoolAsync(p, bytes ? bytes : 1, pool, stream);
     return e;
 }
+
+long long debug_spin_limit()
+{
+    const long long v = g_dbg_spin_limit.load();
+    return v > 0 ? v : kSpinLimitDefault;
+}
+
+int debug_skip_mark() { return g_dbg_skip_mark.load(); }
 
 void dev_free(void *p, cudaStream_t stream)
 {
@@ -664,6 +683,25 @@ MM_API mm_status mm_match_ex(mm_graph *g, int type, uint32_t barrier, const uint
     return MM_ERR_ARG;
 }
 
+MM_API mm_status mm_match_drawn(mm_graph *g, int type, uint32_t barrier, uint32_t (*draw)(void *), void *ctx,
+                                int *d_match_out, int *rounds_out, void *stream)
+{
+    if (!draw) {
+        set_error("mm_match_drawn: draw is null");
+        return MM_ERR_ARG;
+    }
+    const uint32_t unused = 0;
+    mm_status s = check_match_args(g, type, &unused, 1, d_match_out, rounds_out);
+    if (s != MM_OK) return s;
+    if (g->ngraphs > 0) {
+        set_error("mm_match_drawn: matches single graphs only");
+        return MM_ERR_UNSUPPORTED;
+    }
+    DeviceGuard guard(g->device);
+    return pull_match(g, type, barrier, nullptr, 0, d_match_out, rounds_out, nullptr, 0, (cudaStream_t)stream, draw,
+                      ctx);
+}
+
 MM_API mm_status mm_match_device(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds,
                                  int *d_match_out, int *rounds_out, void *stream)
 {
@@ -820,6 +858,38 @@ MM_API mm_status mm_match_batch(mm_graph *g, int type, uint32_t barrier, const u
 MM_API const char *mm_last_error(void) { return g_last_error.c_str(); }
 
 MM_API const char *mm_version(void) { return "mmatch 0.1 (sm_100a)"; }
+
+MM_API mm_status mm_debug(int key, long long value, long long *out)
+{
+    long long prev = 0;
+    switch (key) {
+    case MM_DEBUG_SPIN_LIMIT:
+        prev = g_dbg_spin_limit.exchange(value < 0 ? 0 : value);
+        break;
+    case MM_DEBUG_SKIP_BARRIER:
+        prev = g_dbg_skip_mark.exchange(value < 0 ? -1 : (int)value);
+        break;
+    case MM_DEBUG_ALLOC_LIMIT:
+        prev = g_dbg_alloc_limit.exchange(value < 0 ? -1 : value);
+        break;
+    case MM_DEBUG_POOL_USED: {
+        int device = -1;
+        cudaMemPool_t pool = nullptr;
+        MM_CUDA_TRY(cudaGetDevice(&device), "mm_debug: device");
+        MM_CUDA_TRY(device_pool(device, &pool), "mm_debug: pool");
+        MM_CUDA_TRY(cudaDeviceSynchronize(), "mm_debug: synchronise");
+        uint64_t used = 0;
+        MM_CUDA_TRY(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used), "mm_debug: pool use");
+        prev = (long long)used;
+        break;
+    }
+    default:
+        set_error("mm_debug: unknown key");
+        return MM_ERR_ARG;
+    }
+    if (out) *out = prev;
+    return MM_OK;
+}
 
 MM_API mm_status mm_probe_gather_rate(int device, long long table_bytes, double *gathers_per_s)
 {

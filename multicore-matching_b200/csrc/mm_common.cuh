@@ -140,13 +140,21 @@ cudaError_t pinned_get(void **p, size_t bytes);
 void pinned_put(void *p, size_t bytes);
 mm_status release_cached(int device);
 
+// Polls a grid-barrier wait makes before it gives up (the kernel then returns
+// an error status instead of waiting on).
+constexpr long long kSpinLimitDefault = 1ll << 22;
+// Testing hooks (mm_debug): the grid barriers' poll limit and the barrier mark
+// at which block 0 does not arrive (-1: none).
+long long debug_spin_limit();
+int debug_skip_mark();
+
 // Ensure g->scratch holds at least `bytes`; returns MM_OK or an error.
 mm_status ensure_scratch(mm_graph *g, size_t bytes);
 
 // Paths.
 mm_status pull_match(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds,
                      int *d_match, int *rounds_out, long long *stats, int stats_rounds,
-                     cudaStream_t stream);
+                     cudaStream_t stream, uint32_t (*draw)(void *) = nullptr, void *draw_ctx = nullptr);
 mm_status push_prepare(mm_graph *g, int weighted, cudaStream_t stream);
 mm_status push_match(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds,
                      int *d_match, int *rounds_out, long long *stats, int stats_rounds,

@@ -175,7 +175,7 @@ void launch_round(int *match, int *req, int n, const int2 *ranges, const int *nb
 
 mm_status pull_match(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds,
                      int *d_match, int *rounds_out, long long *stats, int stats_rounds,
-                     cudaStream_t stream)
+                     cudaStream_t stream, uint32_t (*draw)(void *), void *draw_ctx)
 {
     const int n = g->n;
     const bool weighted = is_weighted(type), maximal = is_maximal(type);
@@ -193,8 +193,9 @@ mm_status pull_match(mm_graph *g, int type, uint32_t barrier, const uint32_t *se
     uint32_t *d_seeds = (uint32_t *)(base + seed_off);
     unsigned long long *d_st = (unsigned long long *)(base + st_off);
     const int nup = nseeds < cap ? nseeds : cap;
-    MM_CUDA_TRY(cudaMemcpyAsync(d_seeds, seeds, sizeof(uint32_t) * nup, cudaMemcpyHostToDevice, stream),
-                "seed upload");
+    if (!draw)
+        MM_CUDA_TRY(cudaMemcpyAsync(d_seeds, seeds, sizeof(uint32_t) * nup, cudaMemcpyHostToDevice, stream),
+                    "seed upload");
     MM_CUDA_TRY(cudaMemsetAsync(d_match, 0, sizeof(int) * (size_t)(n > 0 ? n : 1), stream), "clear match");
     if (stats) MM_CUDA_TRY(cudaMemsetAsync(d_st, 0, sizeof(unsigned long long) * kMaxRounds * MM_STATS_COLS, stream),
                            "clear stats");
@@ -202,7 +203,14 @@ mm_status pull_match(mm_graph *g, int type, uint32_t barrier, const uint32_t *se
     int rounds = 0;
     for (;;) {
         if (rounds >= cap) break;
-        if (rounds >= nseeds) {
+        if (draw) {
+            // the round's seed, drawn as the round starts (src/matchgpu.cu:609): one
+            // draw per executed round; a pageable copy is done once it returns
+            const uint32_t sd = draw(draw_ctx);
+            MM_CUDA_TRY(cudaMemcpyAsync(d_seeds + rounds, &sd, sizeof sd, cudaMemcpyHostToDevice, stream),
+                        "seed upload");
+            MM_CUDA_TRY(cudaStreamSynchronize(stream), "seed upload");
+        } else if (rounds >= nseeds) {
             set_error("mm_match: fewer seeds than rounds");
             return MM_ERR_SEEDS;
         }

@@ -122,6 +122,10 @@ struct Params {
     unsigned long long *tstamp;     // [3 * kMaxRounds + 1] barrier times (ns) or null
     unsigned *bar;                  // [kBarWords] grid barrier words, zero at launch
     int resume;                     // round kernel: continue from ctl->fin_round (finish called off)
+    // testing hooks (mm_debug): polls before a barrier wait gives up, and the
+    // mark of a barrier at which block 0 does not arrive (-1: none)
+    long long spin_limit;
+    int skip_mark;
     // A batch of independent graphs (a disjoint union, edges never cross): each
     // vertex's graph starts at vbase[v], and the graph's own numbering (v -
     // vbase[v]) drives the colouring and the match values, so every graph gets
@@ -184,12 +188,12 @@ __device__ __forceinline__ void stat_add(const P &p, int round, int col, unsigne
 // atomics per barrier.  Every word uses the same counting: the first member
 // adds 2^31 - (members - 1), every other member adds 1, so the top bit flips
 // exactly when the last member arrives and the low bits return to where they
-// were.  Each wait is still bounded: after kSpinLimit polls the block records
+// were.  Each wait is still bounded: after kSpinLimitDefault polls (a testing
+// hook, mm_debug, can set fewer) the block records
 // status 2 and the kernel returns; the other blocks then give up at their next
 // barrier.  Thread 0's fences (release before arriving, acquire after the
 // wait), with the block barriers around them, make every block's writes of
 // the phase visible to every thread of every block afterwards.
-constexpr long long kSpinLimit = 1ll << 22;
 constexpr int kBarGroup = 16;
 constexpr int kBarStride = 32;   // words per barrier line (128 bytes)
 constexpr int kBarMaxGroups = 64;
@@ -210,7 +214,8 @@ __device__ __forceinline__ unsigned long long global_ns()
     return t;
 }
 
-__device__ __noinline__ bool grid_sync(unsigned *bar, Ctl *ctl, unsigned long long *tstamp, int mark)
+__device__ __noinline__ bool grid_sync(unsigned *bar, Ctl *ctl, unsigned long long *tstamp, int mark,
+                                       long long spin_limit, int skip_mark)
 {
     __shared__ int s_ok;
     __syncthreads();
@@ -222,16 +227,19 @@ __device__ __noinline__ bool grid_sync(unsigned *bar, Ctl *ctl, unsigned long lo
         unsigned *top = bar + kBarMaxGroups * kBarStride;
         const unsigned top_before = ld_acquire(top);  // cannot flip before this block arrives
         fence_acq_rel();
-        const unsigned ginc = b % kBarGroup == 0 ? 0x80000000u - (gsize - 1u) : 1u;
-        const unsigned gold = atomicAdd(gword, ginc);
-        if (((gold + ginc) ^ gold) & 0x80000000u) {  // last of the group
-            const unsigned tinc = g == 0 ? 0x80000000u - (ngroups - 1u) : 1u;
-            atomicAdd(top, tinc);
+        // testing hook: block 0 leaves this barrier out, so every wait on it runs out
+        if (!(b == 0 && mark >= 0 && mark == skip_mark)) {
+            const unsigned ginc = b % kBarGroup == 0 ? 0x80000000u - (gsize - 1u) : 1u;
+            const unsigned gold = atomicAdd(gword, ginc);
+            if (((gold + ginc) ^ gold) & 0x80000000u) {  // last of the group
+                const unsigned tinc = g == 0 ? 0x80000000u - (ngroups - 1u) : 1u;
+                atomicAdd(top, tinc);
+            }
         }
         int ok = 1;
         long long it = 0;
         while (((top_before ^ ld_acquire(top)) & 0x80000000u) == 0u) {
-            if (++it > kSpinLimit) {
+            if (++it > spin_limit) {
                 ok = 0;
                 break;
             }
@@ -1779,7 +1787,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_rounds(Params p)
         fin_next = -1;
     } else {
         init_phase<kW, kStats, kPolicy>(p, sm);
-        if (!grid_sync(p.bar, p.ctl, p.tstamp, 0)) return;
+        if (!grid_sync(p.bar, p.ctl, p.tstamp, 0, p.spin_limit, p.skip_mark)) return;
         // active vertices at round 0; round 1 clears these counters only after
         // two more grid barriers
         active0 = (long long)__ldcg(&ctl->cnt[0][kBlue]) + __ldcg(&ctl->cnt[0][kRed]);
@@ -1808,11 +1816,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_rounds(Params p)
             if (threadIdx.x == 0) ctl->retired[par ^ 1] = 0;
         }
         scan_window<kW, kStats, kPolicy>(p, t, par);
-        if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 1)) return;
+        if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 1, p.spin_limit, p.skip_mark)) return;
         // phase A2 (all blocks see the same fallback count)
         if (__ldcg(&ctl->staged_pack) != 0ull) {
             scan_long<kW, kStats>(p, sm, t, gwarp, nwarps);
-            if (!grid_sync(p.bar, p.ctl, p.tstamp, -1)) return;
+            if (!grid_sync(p.bar, p.ctl, p.tstamp, -1, p.spin_limit, p.skip_mark)) return;
         }
         if (p.tstamp && blockIdx.x == 0 && threadIdx.x == 0) p.tstamp[3 * t + 2] = global_ns();
         // phase B; the fallback list is empty again for the next round
@@ -1821,7 +1829,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_rounds(Params p)
         if (seeds_short) has_next = false;
         commit_phase<kW, kStats, kPolicy>(p, sm, t, has_next);
         if (blockIdx.x == 0 && threadIdx.x == 0) ctl->staged_pack = 0ull;
-        if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 3)) return;
+        if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 3, p.spin_limit, p.skip_mark)) return;
         // close the round (every block decides alike)
         const long long next = (long long)__ldcg(&ctl->cnt[par ^ 1][kBlue]) + __ldcg(&ctl->cnt[par ^ 1][kRed]);
         const bool more = has_next && next > 0;
@@ -1876,26 +1884,26 @@ __global__ void __launch_bounds__(kThreads, 2) k_finish(Params p)
     if (kStats) {
         // counters must not count a called-off attempt: check, then resolve
         finish_scan<kW, kStats, false>(p, sm, t, par, c0, c1, cap, rec);
-        if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 1)) return;
+        if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 1, p.spin_limit, p.skip_mark)) return;
         done = __ldcg(&ctl->fin_abort) != t + 1;
         if (done) {
             finish_roots<kW, kStats, false, false>(p, sm, t, par, c0, c1, cap, rec);
-            if (!grid_sync(p.bar, p.ctl, p.tstamp, -1)) return;
+            if (!grid_sync(p.bar, p.ctl, p.tstamp, -1, p.spin_limit, p.skip_mark)) return;
             done = __ldcg(&ctl->fin_abort) != t + 1;
         }
         if (done) {
             finish_roots<kW, kStats, true, true>(p, sm, t, par, c0, c1, cap, rec);
-            if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 2)) return;
+            if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 2, p.spin_limit, p.skip_mark)) return;
         }
     } else {
         // speculative: a called-off attempt leaves only values that the
         // resumed rounds write again
         finish_scan<kW, kStats, true>(p, sm, t, par, c0, c1, cap, rec);
-        if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 1)) return;
+        if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 1, p.spin_limit, p.skip_mark)) return;
         done = __ldcg(&ctl->fin_abort) != t + 1;
         if (done) {
             finish_roots<kW, kStats, true, false>(p, sm, t, par, c0, c1, cap, rec);
-            if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 2)) return;
+            if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 2, p.spin_limit, p.skip_mark)) return;
             done = __ldcg(&ctl->fin_abort) != t + 1;
         }
     }
@@ -2596,6 +2604,8 @@ Params make_params(mm_graph *g, PushState *s, bool weighted, bool stats, bool ti
     p.tstamp = timing ? s->tstamp : nullptr;
     p.bar = s->bar;
     p.resume = 0;
+    p.spin_limit = debug_spin_limit();
+    p.skip_mark = debug_skip_mark();
     return p;
 }
 

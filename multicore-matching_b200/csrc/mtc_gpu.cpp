@@ -41,6 +41,16 @@ bool peek_rand(uint32_t *out, int count)
     return true;
 }
 
+uint32_t draw_rand(void *) { return (uint32_t)rand(); }
+
+// MTC_RAND_READ_AHEAD=0 makes the classes take the portable path (seeds drawn
+// from rand() one round at a time) even where the read-ahead works.
+bool read_ahead_allowed()
+{
+    const char *e = std::getenv("MTC_RAND_READ_AHEAD");
+    return !(e && e[0] == '0');
+}
+
 [[noreturn]] void fail(const char *what)
 {
     cerr << what << ": " << mm_last_error() << endl;
@@ -100,9 +110,24 @@ void GraphMatchingGPU::runMatching(vector<int> &match, cudaEvent_t &t1, cudaEven
     assert((int)match.size() == graph.nrVertices);
     const int cap = mm_max_rounds(type);
     uint32_t seeds[256];
-    if (!peek_rand(seeds, cap)) {
-        cerr << "Unable to read ahead in the rand() stream!" << endl;
-        throw exception();
+    if (!read_ahead_allowed() || !peek_rand(seeds, cap)) {
+        // rand()'s state could not be read ahead (another C library, say): the
+        // rounds run one at a time from the host, each drawing its rand() value
+        // as it starts, exactly as the reference's loop does (src/matchgpu.cu:604-615)
+        cudaEventRecord(t1, 0);
+        cudaEventSynchronize(t1);
+        int rounds = 0;
+        if (mm_match_drawn(dgraph, type, selectBarrier, draw_rand, nullptr, dmatch, &rounds, nullptr) != MM_OK)
+            fail("A CUDA error occurred during the matching process");
+        cudaEventRecord(t2, 0);
+        cudaEventSynchronize(t2);
+        if (graph.nrVertices > 0 &&
+            cudaMemcpy(&match[0], dmatch, sizeof(int) * (size_t)graph.nrVertices, cudaMemcpyDeviceToHost) !=
+                cudaSuccess) {
+            cerr << "Unable to retrieve data!" << endl;
+            throw exception();
+        }
+        return;
     }
 
     cudaEventRecord(t1, 0);

@@ -8,10 +8,13 @@ srand(seed) exactly as bin/match.cpp:382 does.  Also records the reference's
 sequential CPU matchers (types 0, 4) on the same graphs for quality
 comparisons.
 
-Output: tests/golden/golden.npz (small, committed).  Needs the reference
-sources (run here, not on the GPU machine):
+Output: tests/golden/golden.npz (small, committed), and with --full
+tests/golden/full_size.json: the SHA-256, round count and next rand() value of
+the reference's matching of the full-size R-MAT graph (2^23 vertices, edge
+factor 16, seed 1), too large to store whole.  Needs the reference build
+(oracle/_ref; run where the reference sources are, not on the GPU machine):
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [--full]
 """
 from __future__ import annotations
 
@@ -108,5 +111,29 @@ def main() -> None:
     print(f"wrote {len(index)} cases to {HERE / 'golden.npz'}")
 
 
+def full_size() -> None:
+    """The reference's matchings of the full-size R-MAT graph (GPU types 7 and 9,
+    srand(12345) as bin/match.cpp:382), recorded by hash."""
+    mm = load_package()
+    orc = load_oracle()
+    if not orc.ref_available():
+        raise SystemExit("oracle/_ref is not built (make -C oracle ref)")
+    g = mm.Graph.rmat(23, 16, 0.57, 0.19, 0.19, seed=1)
+    seeds = orc.rand_seeds(12345, 256)
+    out = {"graph": "rmat_23_ef16_s1", "n": int(g.n), "nnz": int(g.nnz), "cases": []}
+    for gpu_type, ref_type in ((7, 10), (9, 11)):
+        m, _, nxt = orc.ref_run(g, ref_type, BARRIER, 12345)
+        rounds = int(np.nonzero(seeds == nxt)[0][0])
+        valid, weight, size = orc.ref_check(g, m)
+        out["cases"].append({"type": gpu_type, "seed": 12345, "barrier": BARRIER, "rounds": rounds,
+                             "next_rand": int(nxt), "valid": bool(valid), "weight": float(weight), "size": int(size),
+                             "sha256": digest(m)})
+        print(out["cases"][-1], flush=True)
+    (HERE / "full_size.json").write_text(json.dumps(out, indent=1) + "\n")
+
+
 if __name__ == "__main__":
-    main()
+    if "--full" in sys.argv:
+        full_size()
+    else:
+        main()

@@ -163,3 +163,32 @@ def test_policy_that_ignores_its_features_is_constant(mm, orc, torch_cuda):
         ra = dg.match_policy(9, seeds, a.data_ptr(), w, 0.0)
         rb = dg.match_policy(9, seeds, b.data_ptr(), np.zeros(mm.POLICY_FLOATS, np.float32), 0.0)
         assert ra == rb and np.array_equal(a.cpu().numpy(), b.cpu().numpy())
+
+
+def test_policy_mlp_device_matches_host(mm, orc, torch_cuda):
+    """The MLP the colouring evaluates on the device gives, from the traced
+    features, the same colour as a numpy evaluation of the same weights
+    (policy.policy_prob): blue iff hash < p * 2^32, except where the hash lies
+    within a band of the threshold that fp32 rounding can cross."""
+    import importlib
+
+    pol = importlib.import_module("multicore_matching_b200.policy")
+    rng = np.random.default_rng(11)
+    mlp = (rng.standard_normal(mm.POLICY_FLOATS) * 0.6).astype(np.float32)
+    g = mm.Graph.rgg(1 << 12, 13.0, seed=3)
+    seeds = orc.rand_seeds(77, 256)
+    cap = 48
+    with mm.DeviceGraph(g, device=0) as dg:
+        tr = torch_cuda.full((cap * g.n * 8,), float("nan"), dtype=torch_cuda.float32, device="cuda")
+        out = torch_cuda.empty(g.n, dtype=torch_cuda.int32, device="cuda")
+        rounds = dg.match_policy(9, seeds, out.data_ptr(), mlp, 1.0, tr.data_ptr(), cap)
+        t = tr.view(cap, g.n, 8).cpu().numpy()[: min(rounds, cap)]
+    rr, vv = np.nonzero(~np.isnan(t[:, :, 6]))
+    rows = t[rr, vv]
+    p = pol.policy_prob(mlp.astype(np.float64), rows[:, :6].astype(np.float64))
+    thr = p * 4294967296.0
+    h = np.array([orc.colour_hash(int(v), int(seeds[r])) for r, v in zip(rr, vv)], dtype=np.float64)
+    band = np.abs(h - thr) <= 4294967296.0 * 1e-5
+    want = (h < thr).astype(np.float32)
+    assert len(rows) > 5000 and band.mean() < 0.01
+    assert np.array_equal(rows[~band, 6], want[~band]), int((rows[~band, 6] != want[~band]).sum())

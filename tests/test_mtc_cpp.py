@@ -42,8 +42,9 @@ def harness(mm, tmp_path_factory):
     return exe
 
 
-def run(exe, *args, check=True):
-    p = subprocess.run([str(exe), *map(str, args)], capture_output=True, text=True, timeout=600)
+def run(exe, *args, check=True, env=None):
+    p = subprocess.run([str(exe), *map(str, args)], capture_output=True, text=True, timeout=600,
+                       env=None if env is None else {**os.environ, **env})
     if check and p.returncode != 0:
         raise AssertionError(f"harness {args[0]} failed ({p.returncode}): {p.stdout} {p.stderr}")
     return p
@@ -222,13 +223,17 @@ def test_random_shuffle_matches_reference(mm, orc, harness, tmp_path):
 @pytest.mark.skipif(not has_gpu(), reason="needs a GPU")
 @pytest.mark.parametrize("gtype", [6, 7, 8, 9])
 @pytest.mark.parametrize("shuffle", [False, True])
-def test_cli_loop_matches_reference(mm, orc, harness, tmp_path, gtype, shuffle):
+@pytest.mark.parametrize("read_ahead", [True, False])
+def test_cli_loop_matches_reference(mm, orc, harness, tmp_path, gtype, shuffle, read_ahead):
+    """The reference's CLI loop over the GPU classes; read_ahead False forces the
+    portable path (seeds drawn from rand() one round at a time, mm_match_drawn)."""
     g = mm.Graph.rgg(6000, 10.0, seed=21)
     path = tmp_path / "g.graph"
     write_metis(path, g, True)
     reps = 3
     out = tmp_path / "m.bin"
-    p = run(harness, "match", path, gtype, 12345, int(shuffle), reps, out)
+    p = run(harness, "match", path, gtype, 12345, int(shuffle), reps, out,
+            env=None if read_ahead else {"MTC_RAND_READ_AHEAD": "0"})
     res = json.loads(p.stdout)
     got = np.fromfile(out, dtype=np.int32).reshape(reps, g.n)
     assert all(r["valid"] for r in res["runs"])
