@@ -163,6 +163,20 @@ mm_status mm_match_device(mm_graph *g, int type, uint32_t barrier, const uint32_
 mm_status mm_match_drawn(mm_graph *g, int type, uint32_t barrier, uint32_t (*draw)(void *ctx), void *ctx,
                          int *d_match_out, int *rounds_out, void *stream);
 
+/*
+ * Launch options of a graph's matchings (no counterpart in the reference),
+ * set by the autotuner (multicore-matching_b200/tune.py) or by hand; 0
+ * restores the default.  The result never depends on them, only the time.
+ *   MM_TUNE_FINISH_DIV     the finish phase (the late rounds played component by
+ *                          component) starts at the first round whose active set
+ *                          is at most 1/value of round 0's; default 12, at least
+ *                          2, -1 never
+ *   MM_TUNE_BLOCKS_PER_SM  blocks of 512 threads per multiprocessor for the round
+ *                          and finish kernels; default all that fit (2)
+ */
+enum { MM_TUNE_FINISH_DIV = 1, MM_TUNE_BLOCKS_PER_SM = 2 };
+mm_status mm_graph_tune(mm_graph *g, int key, int value);
+
 /* As mm_match_device with an explicit kernel family (MM_PATH_*). */
 mm_status mm_match_ex(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds,
                       int *d_match_out, int *rounds_out, int path, void *stream);

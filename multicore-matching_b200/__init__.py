@@ -96,6 +96,7 @@ _MM_SIGS = {
     "mm_match_profile": (_I, [_P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P, _I, ctypes.POINTER(_I), _P]),
     "mm_match_noalloc": (_I, [_I, _P, _LL, _P, _P, _I, _U, _P, _I, _P, ctypes.POINTER(_I), _P]),
     "mm_debug": (_I, [_I, _LL, ctypes.POINTER(_LL)]),
+    "mm_graph_tune": (_I, [_P, _I, _I]),
     "mm_last_error": (ctypes.c_char_p, []),
     "mm_version": (ctypes.c_char_p, []),
 }
@@ -362,6 +363,21 @@ class DeviceGraph:
         w = np.empty(max(self.nnz, 1), dtype=np.float32)
         _check(self._lib.mm_graph_copy_out(self.handle, _ptr(r), _ptr(nb), _ptr(w)))
         return r[: self.n], nb[: self.nnz], w[: self.nnz]
+
+    def tune(self, finish_div: int = 0, blocks_per_sm: int = 0) -> None:
+        """Launch options of this graph's matchings (mm_graph_tune); 0 = default."""
+        _check(self._lib.mm_graph_tune(self.handle, 1, int(finish_div)))
+        _check(self._lib.mm_graph_tune(self.handle, 2, int(blocks_per_sm)))
+
+    def tune_for(self, workload_class: str) -> dict:
+        """Apply the autotuner's choice for a workload class (tuned.json, written by
+        tune.py); unknown classes keep the defaults.  Returns the choice."""
+        import json
+
+        path = PKG / "tuned.json"
+        choice = json.loads(path.read_text()).get(workload_class, {}) if path.exists() else {}
+        self.tune(choice.get("finish_div", 0), choice.get("blocks_per_sm", 0))
+        return choice
 
     def set_batch(self, offsets: np.ndarray) -> None:
         """Mark the graph as a disjoint union of independent graphs (mm_graph_set_batch)."""

@@ -859,6 +859,29 @@ MM_API const char *mm_last_error(void) { return g_last_error.c_str(); }
 
 MM_API const char *mm_version(void) { return "mmatch 0.1 (sm_100a)"; }
 
+MM_API mm_status mm_graph_tune(mm_graph *g, int key, int value)
+{
+    if (!g) {
+        set_error("mm_graph_tune: null graph");
+        return MM_ERR_ARG;
+    }
+    switch (key) {
+    case MM_TUNE_FINISH_DIV:
+        if (value < -1 || value == 1 || value > 1 << 20) break;
+        g->opt_fin_div = value;
+        return MM_OK;
+    case MM_TUNE_BLOCKS_PER_SM:
+        if (value < 0 || value > 64) break;
+        g->opt_blocks_per_sm = value;
+        return MM_OK;
+    default:
+        set_error("mm_graph_tune: unknown key");
+        return MM_ERR_ARG;
+    }
+    set_error("mm_graph_tune: value out of range");
+    return MM_ERR_ARG;
+}
+
 MM_API mm_status mm_debug(int key, long long value, long long *out)
 {
     long long prev = 0;

@@ -110,6 +110,9 @@ struct mm_graph {
 
     // push path: per-call state of the round kernel
     void *push_exec = nullptr;  // internal (mm::PushState *)
+    // launch options (mm_graph_tune; 0 = the library's default)
+    int opt_fin_div = 0;        // finish phase from the round whose active set is <= 1/opt of round 0's; -1 never
+    int opt_blocks_per_sm = 0;  // blocks per SM of the round and finish kernels
 
     // a batch of independent graphs (mm_graph_set_batch): graph i holds
     // vertices [goff[i], goff[i + 1]); vbase[v] = goff of v's graph; last[v]

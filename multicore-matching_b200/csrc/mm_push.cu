@@ -122,6 +122,7 @@ struct Params {
     unsigned long long *tstamp;     // [3 * kMaxRounds + 1] barrier times (ns) or null
     unsigned *bar;                  // [kBarWords] grid barrier words, zero at launch
     int resume;                     // round kernel: continue from ctl->fin_round (finish called off)
+    int fin_div;                    // finish phase from the round whose active set is <= 1/fin_div of round 0's (0: never)
     // testing hooks (mm_debug): polls before a barrier wait gives up, and the
     // mark of a barrier at which block 0 does not arrive (-1: none)
     long long spin_limit;
@@ -1166,7 +1167,7 @@ constexpr int kFinMembers = 32;    // members of a component played by one warp 
 constexpr int kFinEntries = 128;   // entries between members of one component
 constexpr int kFinShort = 32;      // lists a thread scans on its own; longer ones its warp scans
 constexpr int kFinMaxDeg = 2048;   // longest list the finish phase accepts
-constexpr int kFinDiv = 12;        // first attempt once the active set is at most 1/kFinDiv of round 0's
+constexpr int kFinDiv = 12;        // default: first attempt once the active set is at most 1/kFinDiv of round 0's
 enum : int { kFinSingle = 1, kFinMember = 2, kFinRootCand = 3 };
 enum : int { kFinNotRoot = 0, kFinRoot = 1, kFinTooBig = 2 };
 
@@ -1483,7 +1484,7 @@ struct FinComp {
 
 // The finish phase's record of item i: four int4 slots, rec[4i .. 4i + 3], in
 // the worklist memory of the other parity (2n slots, which the round has not
-// written yet; an attempt has at most n / kFinDiv items): {meta, v, 0, 0},
+// written yet; an attempt has at most n / 2 items): {meta, v, 0, 0},
 // then the ids, preference-key low halves and high halves of its first
 // kFinRec entries that point at an active vertex.  meta = class | count << 8,
 // count = its active neighbours, kFinRec + 1 if more than a record holds.
@@ -1802,7 +1803,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_rounds(Params p)
         // leaves here; round t's worklists and colours are complete.
         if (!kPolicy && p.sym && t > 0) {
             const long long act = (long long)__ldcg(&ctl->cnt[par][kBlue]) + __ldcg(&ctl->cnt[par][kRed]);
-            if (act > 0 && act * kFinDiv <= active0 && act <= fin_next) {
+            if (p.fin_div > 0 && act > 0 && act * p.fin_div <= active0 && act <= fin_next) {
                 if (blockIdx.x == 0 && threadIdx.x == 0) {
                     ctl->fin_round = t;
                     ctl->fin_state = kFinStatePending;
@@ -2429,6 +2430,7 @@ struct PushState {
     unsigned *bar = nullptr;
     int grid[2][3] = {{0, 0, 0}, {0, 0, 0}};  // co-resident blocks of k_rounds by weighting and mode
     int fgrid[2][2] = {{0, 0}, {0, 0}};       // co-resident blocks of k_finish by weighting and stats
+    int sms = 0;                              // multiprocessors of the device
     float2 *wfeat = nullptr;              // learned colouring: (max, mean) incident weight per vertex
 };
 
@@ -2524,6 +2526,7 @@ mm_status alloc_state(mm_graph *g, PushState **out)
     int sms = 0, dev = 0, coop = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    s->sms = sms;
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
     s->grid[0][0] = coresident_blocks<false, false, false>(sms);
     s->grid[0][1] = coresident_blocks<false, true, false>(sms);
@@ -2604,6 +2607,8 @@ Params make_params(mm_graph *g, PushState *s, bool weighted, bool stats, bool ti
     p.tstamp = timing ? s->tstamp : nullptr;
     p.bar = s->bar;
     p.resume = 0;
+    // at least 2: the finish phase's records take 4 slots an item in 2n
+    p.fin_div = g->opt_fin_div < 0 ? 0 : (g->opt_fin_div == 0 ? kFinDiv : max(g->opt_fin_div, 2));
     p.spin_limit = debug_spin_limit();
     p.skip_mark = debug_skip_mark();
     return p;
@@ -2632,7 +2637,11 @@ mm_status launch_rounds(mm_graph *g, PushState *s, bool timing, cudaStream_t str
     }
     void *args[] = {&prm};
     const int mode = kPolicy ? 2 : (kStats ? 1 : 0);
-    MM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)k_rounds<kW, kStats, kPolicy>, dim3(s->grid[kW][mode]),
+    // blocks: all that fit at once, or the tuned number per SM (never more)
+    const int bps = g->opt_blocks_per_sm;
+    const int grid = bps > 0 ? min(s->grid[kW][mode], bps * s->sms) : s->grid[kW][mode];
+    const int fgrid = bps > 0 ? min(s->fgrid[kW][kStats ? 1 : 0], bps * s->sms) : s->fgrid[kW][kStats ? 1 : 0];
+    MM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)k_rounds<kW, kStats, kPolicy>, dim3(grid),
                                             dim3(kThreads), args, sizeof(Smem), stream),
                 "round kernel launch");
     if (!kPolicy && prm.sym) {
@@ -2642,13 +2651,13 @@ mm_status launch_rounds(mm_graph *g, PushState *s, bool timing, cudaStream_t str
         Params fin = prm;
         fin.bar = s->bar + kBarWords;
         void *fargs[] = {&fin};
-        MM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)k_finish<kW, kStats>, dim3(s->fgrid[kW][kStats ? 1 : 0]),
+        MM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)k_finish<kW, kStats>, dim3(fgrid),
                                                 dim3(kThreads), fargs, sizeof(Smem), stream),
                     "finish kernel launch");
         Params res = prm;
         res.resume = 1;
         void *rargs[] = {&res};
-        MM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)k_rounds<kW, kStats, kPolicy>, dim3(s->grid[kW][mode]),
+        MM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)k_rounds<kW, kStats, kPolicy>, dim3(grid),
                                                 dim3(kThreads), rargs, sizeof(Smem), stream),
                     "round kernel launch (resumed)");
     }

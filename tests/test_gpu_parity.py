@@ -306,3 +306,20 @@ def test_rgg_config_full_size(mm, orc, torch_cuda):
             if t == 9:
                 chk = orc.check(g, got)
                 assert chk["valid"] and chk["matchable"] == 0
+
+
+def test_launch_options_never_change_the_result(mm, orc, torch_cuda):
+    """mm_graph_tune changes only the time: every finish-phase divisor (2 tries the
+    phase so early that attempts are called off and the resumed round kernel
+    carries on; -1 never enters it) and block count gives the oracle's matching."""
+    seeds = orc.rand_seeds(12345, 256)
+    for g in (mm.Graph.rgg(1 << 14, 13.0, seed=7), mm.Graph.rmat(14, 16, seed=2), mm.Graph.grid(100, 90)):
+        with mm.DeviceGraph(g, device=0) as dg:
+            for t in (7, 9):
+                want, rounds, _ = orc.match(g, t, seeds, BARRIER)
+                for d in (-1, 2, 3, 12, 40):
+                    for b in (1, 2):
+                        dg.tune(d, b)
+                        got, r = gpu_match(mm, torch_cuda, g, t, seeds, dg=dg)
+                        assert r == rounds and np.array_equal(got, want), (g.name, t, d, b)
+            dg.tune(0, 0)
