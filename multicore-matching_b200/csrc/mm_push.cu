@@ -1597,6 +1597,8 @@ __device__ __forceinline__ void finish_scan(const Params &p, Smem &sm, int t, in
     bool abort = false;
     int last_all = -1;
     for (long long base = gw * 32; base < A; base += nw * 32) {
+        // another warp may have called the attempt off: its remaining work is wasted
+        if (__shfl_sync(kFull, lane == 0 ? __ldcg(&p.ctl->fin_abort) : 0, 0) == t + 1) break;
         const long long i = base + lane;
         const int4 it = i < A ? item_at(p, par, c0, i) : make_int4(-1, 0, 0, 0);
         const int deg = it.x >= 0 ? degree_of(it) : 0;
@@ -1653,7 +1655,10 @@ __device__ __forceinline__ void finish_scan(const Params &p, Smem &sm, int t, in
             stat_add(p, t, MM_ST_FINISH_ITEMS, it.x >= 0 ? 1ull : 0ull);
             stat_add(p, t, MM_ST_FINISH_ENTRIES, (unsigned long long)deg);
         }
-        if (__any_sync(kFull, abort)) break;  // the attempt is off
+        if (__any_sync(kFull, abort)) {  // the attempt is off: tell the other warps now
+            if (lane == 0) atomicExch(&p.ctl->fin_abort, t + 1);
+            break;
+        }
         if (kSingles) fin_singles<kStats>(p, sm.seeds, t, cap, c == kFinSingle, it.x, deg, i < c0, last_all);
     }
     if (abort && lane == 0) atomicExch(&p.ctl->fin_abort, t + 1);
@@ -1680,6 +1685,7 @@ __device__ __forceinline__ void finish_roots(const Params &p, Smem &sm, int t, i
     bool abort = false;
     int last_all = -1;
     for (long long base = gw * 32; base < A; base += nw * 32) {
+        if (__shfl_sync(kFull, lane == 0 ? __ldcg(&p.ctl->fin_abort) : 0, 0) == t + 1) break;
         const long long i = base + lane;
         const int4 r0 = i < A ? __ldcg(rec + 4 * i) : make_int4(0, -1, 0, 0);
         const int meta = r0.x;
@@ -1748,7 +1754,10 @@ __device__ __forceinline__ void finish_roots(const Params &p, Smem &sm, int t, i
             if (kPlay && r == kFinRoot) last_all = max(last_all, fin_play<kW, kStats>(p, fw, sm.seeds, t, cap, mem, k));
             __syncwarp();  // fw is reused by the next root
         }
-        if (__any_sync(kFull, abort)) break;
+        if (__any_sync(kFull, abort)) {
+            if (lane == 0) atomicExch(&p.ctl->fin_abort, t + 1);
+            break;
+        }
     }
     if (abort && lane == 0) atomicExch(&p.ctl->fin_abort, t + 1);
     if (kPlay) {
