@@ -398,6 +398,7 @@ struct Smem {
     int tile_warp[kWarps][2];             // compaction: per-warp counts, then offsets
     int tile_base[2];                     // compaction: tile bases
     uint32_t seeds[256];                  // the call's colouring seeds (finish phase)
+    int wqueue_n;                         // window scan: vertices queued for sub-pass B
 };
 
 // ---- learned colouring ----
@@ -606,10 +607,11 @@ __device__ void init_phase(const Params &p, Smem &sm)
 // fits in its window and has no red candidate is decided too (unmatchable iff
 // no entry is unmatched).  A longer list with no red candidate in its window
 // falls back to a full scan in phase A2: it is appended to the round's
-// fallback list.  Each thread walks kPerW vertices at once, two window entries
-// per vertex and step.
+// fallback list.  The first two entries of every vertex are read in one step
+// (sub-pass A below); the rest, for vertices those leave open, kWinStep at a
+// time, kPerW vertices per thread.
 constexpr int kPerW = 2;
-constexpr int kWinStep = 4;  // window entries per step after the first
+constexpr int kWinStep = 4;  // window entries per step after the first two
 
 // Learned colouring, graphs with symmetric structure: a red vertex of at most
 // kRetireMaxDeg entries whose neighbours are all matched leaves in phase A of
@@ -661,120 +663,210 @@ __device__ __forceinline__ void retire_red(const Params &p, int t, int par, int 
     }
 }
 
+// The end of a blue vertex's window scan: propose to the red candidate found,
+// or decide "no proposal" / "unmatchable" for a list that fits its window, or
+// stage a longer list with no red candidate in its window for the fallback scan.
+template <bool kW, bool kStats>
+__device__ __forceinline__ void window_done(const Params &p, int t, int4 it, bool found, int cj, int ct, bool alive,
+                                            int seen)
+{
+    Ctl *ctl = p.ctl;
+    const int v = it.x, deg = degree_of(it);
+    if (kStats) atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_WINDOW_ENTRIES], (unsigned long long)seen);
+    if (found || deg <= kWin) {
+        if (kStats) {
+            atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_REQ_ENTRIES],
+                      request_seen<kW>(it.y, deg, found ? cj : -1));
+            atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_BLUE_DEG], (unsigned long long)deg);
+        }
+        if (found) {
+            if (kW && p.wwin) propose_weight(p, v, __int_as_float(cj), ct);
+            else propose_to<kW>(p, v, it.y, cj & 0x7fffffff, ct);
+        } else {
+            no_proposal(p, v, alive);
+        }
+    } else {
+        // fallback: the whole list is scanned in phase A2
+        const unsigned long long old = atomicAdd(&ctl->staged_pack, (1ull << 32) | (unsigned long long)(unsigned)deg);
+        const int idx = (int)(old >> 32), off = (int)(old & 0xffffffffull);
+        p.staged[idx] = make_int4(v, it.y, it.z, off);
+        for (int s = (off + kSegEntries - 1) / kSegEntries; s * kSegEntries < off + deg; ++s) p.seg_first[s] = idx;
+    }
+}
+
+// Window entries q and q + 1 of a blue vertex (item it, window length wl):
+// neighbours and second words (weight, position | flag, or position).
+template <bool kW>
+__device__ __forceinline__ void window_pair(const Params &p, int4 it, int wl, int q, int &n0, int &j0, int &n1, int &j1)
+{
+    n0 = n1 = 0;
+    j0 = j1 = 0;
+    if (q >= wl) return;
+    if (kW) {
+        const int4 x = __ldg(reinterpret_cast<const int4 *>(p.pwin + it.w + q));
+        n0 = x.x;
+        j0 = x.y;
+        n1 = x.z;
+        j1 = x.w;
+    } else {
+        j0 = it.y + q;
+        j1 = j0 + 1;
+        n0 = __ldg(p.nbrs + j0);
+        if (q + 1 < wl) n1 = __ldg(p.nbrs + j1);
+    }
+}
+
+// Whether a window entry's neighbour colour c and second word j make it the
+// vertex's choice (a red candidate): on the symmetric weighted path j is the
+// weight; elsewhere for weighted types the position, bit 31 set for a weight
+// that can never be picked; random types: the position.
+template <bool kW>
+__device__ __forceinline__ bool window_choice(const Params &p, uint8_t c, int j)
+{
+    return c == kRed && (!kW || (p.wwin ? __int_as_float(j) > -1.0f : j >= 0));
+}
+
+// Phase A1.  A block takes kWinA * kThreads blue items at a time.  Sub-pass A:
+// each thread reads the first two window entries of kWinA vertices (in the
+// first rounds most vertices stop there), with all their loads in flight at
+// once, and ends every vertex those entries decide.  The others go to a queue
+// in shared memory (the fallback scan's staging area; bit 31 of the window
+// offset records whether an unmatched neighbour was seen), and sub-pass B
+// continues them two vertices a thread, kWinStep entries a step.
+constexpr int kWinA = 4;
+static_assert(kWinA * kThreads * (int)sizeof(int4) <= (int)sizeof(LongStage) * kWarps, "window queue fits the staging area");
+
 template <bool kW, bool kStats, bool kPolicy>
-__device__ void scan_window(const Params &p, int t, int par)
+__device__ void scan_window(const Params &p, Smem &sm, int t, int par)
 {
     Ctl *ctl = p.ctl;
     const int n_blue = __ldcg(&ctl->cnt[par][kBlue]);
     const int n_red = kPolicy ? __ldcg(&ctl->cnt[par][kRed]) : 0;  // read with n_blue: one round trip
     const int4 *list = p.lists[par][kBlue];
-    const long long stride = (long long)gridDim.x * kThreads;
-    for (long long i0 = (long long)blockIdx.x * kThreads + threadIdx.x; i0 < n_blue; i0 += stride * kPerW) {
-        int4 it[kPerW];
-        int wl[kPerW], cj[kPerW], ct[kPerW], seen[kPerW];
-        bool open[kPerW], alive[kPerW], found[kPerW];
+    int4 *queue = reinterpret_cast<int4 *>(&sm.stage[0]);
+    constexpr long long kChunk = (long long)kWinA * kThreads;
+    for (long long c0 = (long long)blockIdx.x * kChunk; c0 < n_blue; c0 += (long long)gridDim.x * kChunk) {
+        if (threadIdx.x == 0) sm.wqueue_n = 0;
+        __syncthreads();
+        // sub-pass A: the first two entries of kWinA vertices a thread
+        {
+            int4 it[kWinA];
+            int wl[kWinA], n0[kWinA], j0[kWinA], n1[kWinA], j1[kWinA];
 #pragma unroll
-        for (int k = 0; k < kPerW; ++k) {
-            const long long i = i0 + k * stride;
-            it[k] = i < n_blue ? __ldcg(list + i) : make_int4(-1, 0, 0, 0);
-            wl[k] = it[k].x >= 0 ? win_len(degree_of(it[k])) : 0;
-            open[k] = wl[k] > 0;
-            alive[k] = false;
-            found[k] = false;
-            cj[k] = -1;
-            ct[k] = 0;
-            seen[k] = 0;
-        }
-        // the first step reads 2 entries (most vertices stop there in the first
-        // round), every later one kWinStep: at most 9 dependent steps for 32
-        for (int q = 0; q < kWin;) {
-            const int width = q == 0 ? 2 : kWinStep;
-            bool any = false;
+            for (int k = 0; k < kWinA; ++k) {
+                const long long i = c0 + k * kThreads + threadIdx.x;
+                it[k] = i < n_blue ? __ldcg(list + i) : make_int4(-1, 0, 0, 0);
+                wl[k] = it[k].x >= 0 ? win_len(degree_of(it[k])) : 0;
+            }
 #pragma unroll
-            for (int k = 0; k < kPerW; ++k) any |= open[k];
-            if (!any) break;
-            int nb[kPerW][kWinStep], jv[kPerW][kWinStep];
+            for (int k = 0; k < kWinA; ++k) window_pair<kW>(p, it[k], wl[k], 0, n0[k], j0[k], n1[k], j1[k]);
+            uint8_t ca[kWinA], cb[kWinA];
 #pragma unroll
-            for (int k = 0; k < kPerW; ++k) {
+            for (int k = 0; k < kWinA; ++k) {
+                ca[k] = wl[k] > 0 ? p.col[n0[k]] : (uint8_t)kMatched;
+                cb[k] = wl[k] > 1 ? p.col[n1[k]] : (uint8_t)kMatched;
+            }
 #pragma unroll
-                for (int h = 0; h < kWinStep / 2; ++h) {
-                    const int e = q + 2 * h;
-                    nb[k][2 * h] = nb[k][2 * h + 1] = 0;
-                    jv[k][2 * h] = jv[k][2 * h + 1] = 0;
-                    if (!open[k] || 2 * h >= width || e >= wl[k]) continue;
-                    if (kW) {
-                        const int4 x = __ldg(reinterpret_cast<const int4 *>(p.pwin + it[k].w + e));
-                        nb[k][2 * h] = x.x;
-                        jv[k][2 * h] = x.y;
-                        nb[k][2 * h + 1] = x.z;
-                        jv[k][2 * h + 1] = x.w;
+            for (int k = 0; k < kWinA; ++k) {
+                if (it[k].x < 0) continue;
+                bool found = false, alive = false;
+                int cj = -1, ct = 0, seen = 0;
+                if (wl[k] > 0) {
+                    seen = 1;
+                    if (window_choice<kW>(p, ca[k], j0[k])) {
+                        found = true;
+                        cj = j0[k];
+                        ct = n0[k];
                     } else {
-                        jv[k][2 * h] = it[k].y + e;
-                        jv[k][2 * h + 1] = it[k].y + e + 1;
-                        nb[k][2 * h] = __ldg(p.nbrs + it[k].y + e);
-                        if (e + 1 < wl[k]) nb[k][2 * h + 1] = __ldg(p.nbrs + it[k].y + e + 1);
+                        alive = ca[k] != kMatched;
+                        if (wl[k] > 1) {
+                            seen = 2;
+                            if (window_choice<kW>(p, cb[k], j1[k])) {
+                                found = true;
+                                cj = j1[k];
+                                ct = n1[k];
+                            } else {
+                                alive |= cb[k] != kMatched;
+                            }
+                        }
                     }
                 }
-            }
-            uint8_t c[kPerW][kWinStep];
-#pragma unroll
-            for (int k = 0; k < kPerW; ++k) {
-#pragma unroll
-                for (int x = 0; x < kWinStep; ++x) {
-                    c[k][x] = kMatched;
-                    if (open[k] && x < width && q + x < wl[k]) c[k][x] = p.col[nb[k][x]];
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < kPerW; ++k) {
-                if (!open[k]) continue;
-#pragma unroll
-                for (int x = 0; x < kWinStep; ++x) {
-                    if (x >= width || q + x >= wl[k] || found[k]) continue;
-                    seen[k] += 1;
-                    // a window entry's second word: the weight (symmetric weighted
-                    // path), else the position with bit 31 set for a weight that
-                    // can never be picked; random types: the position
-                    const bool cand = !kW || (p.wwin ? __int_as_float(jv[k][x]) > -1.0f : jv[k][x] >= 0);
-                    if (c[k][x] == kRed && cand) {
-                        cj[k] = jv[k][x];
-                        ct[k] = nb[k][x];
-                        found[k] = true;
-                    } else {
-                        alive[k] |= c[k][x] != kMatched;
-                    }
-                }
-                if (found[k] || q + width >= wl[k]) open[k] = false;
-            }
-            q += width;
-        }
-#pragma unroll
-        for (int k = 0; k < kPerW; ++k) {
-            if (it[k].x < 0) continue;
-            const int v = it[k].x, deg = degree_of(it[k]);
-            if (kStats) atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_WINDOW_ENTRIES], (unsigned long long)seen[k]);
-            if (found[k] || deg <= kWin) {
-                if (kStats) {
-                    atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_REQ_ENTRIES],
-                              request_seen<kW>(it[k].y, deg, found[k] ? cj[k] : -1));
-                    atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_BLUE_DEG], (unsigned long long)deg);
-                }
-                if (found[k]) {
-                    if (kW && p.wwin) propose_weight(p, v, __int_as_float(cj[k]), ct[k]);
-                    else propose_to<kW>(p, v, it[k].y, cj[k] & 0x7fffffff, ct[k]);
+                if (found || wl[k] <= 2) {
+                    window_done<kW, kStats>(p, t, it[k], found, cj, ct, alive, seen);
                 } else {
-                    no_proposal(p, v, alive[k]);
+                    const int q = atomicAdd(&sm.wqueue_n, 1);
+                    queue[q] = make_int4(it[k].x, it[k].y, it[k].z, (int)((unsigned)it[k].w | (alive ? 0x80000000u : 0u)));
                 }
-            } else {
-                // fallback: the whole list is scanned in phase A2
-                const unsigned long long old =
-                    atomicAdd(&ctl->staged_pack, (1ull << 32) | (unsigned long long)(unsigned)deg);
-                const int idx = (int)(old >> 32), off = (int)(old & 0xffffffffull);
-                p.staged[idx] = make_int4(v, it[k].y, it[k].z, off);
-                for (int s = (off + kSegEntries - 1) / kSegEntries; s * kSegEntries < off + deg; ++s)
-                    p.seg_first[s] = idx;
             }
         }
+        __syncthreads();
+        // sub-pass B: the queued vertices from entry 2 on
+        const int qn = sm.wqueue_n;
+        for (int i0 = threadIdx.x; i0 < qn; i0 += kThreads * kPerW) {
+            int4 it[kPerW];
+            int wl[kPerW], cj[kPerW], ct[kPerW], seen[kPerW];
+            bool open[kPerW], alive[kPerW], found[kPerW];
+#pragma unroll
+            for (int k = 0; k < kPerW; ++k) {
+                const int i = i0 + k * kThreads;
+                it[k] = i < qn ? queue[i] : make_int4(-1, 0, 0, 0);
+                alive[k] = it[k].w < 0;  // bit 31
+                it[k].w &= 0x7fffffff;
+                wl[k] = it[k].x >= 0 ? win_len(degree_of(it[k])) : 0;
+                open[k] = wl[k] > 2;
+                found[k] = false;
+                cj[k] = -1;
+                ct[k] = 0;
+                seen[k] = 2;
+            }
+            for (int q = 2; q < kWin; q += kWinStep) {
+                bool any = false;
+#pragma unroll
+                for (int k = 0; k < kPerW; ++k) any |= open[k];
+                if (!any) break;
+                int nb[kPerW][kWinStep], jv[kPerW][kWinStep];
+#pragma unroll
+                for (int k = 0; k < kPerW; ++k) {
+#pragma unroll
+                    for (int h = 0; h < kWinStep / 2; ++h) {
+                        nb[k][2 * h] = nb[k][2 * h + 1] = 0;
+                        jv[k][2 * h] = jv[k][2 * h + 1] = 0;
+                        if (open[k]) window_pair<kW>(p, it[k], wl[k], q + 2 * h, nb[k][2 * h], jv[k][2 * h],
+                                                     nb[k][2 * h + 1], jv[k][2 * h + 1]);
+                    }
+                }
+                uint8_t c[kPerW][kWinStep];
+#pragma unroll
+                for (int k = 0; k < kPerW; ++k) {
+#pragma unroll
+                    for (int x = 0; x < kWinStep; ++x) {
+                        c[k][x] = kMatched;
+                        if (open[k] && q + x < wl[k]) c[k][x] = p.col[nb[k][x]];
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < kPerW; ++k) {
+                    if (!open[k]) continue;
+#pragma unroll
+                    for (int x = 0; x < kWinStep; ++x) {
+                        if (q + x >= wl[k] || found[k]) continue;
+                        seen[k] += 1;
+                        if (window_choice<kW>(p, c[k][x], jv[k][x])) {
+                            cj[k] = jv[k][x];
+                            ct[k] = nb[k][x];
+                            found[k] = true;
+                        } else {
+                            alive[k] |= c[k][x] != kMatched;
+                        }
+                    }
+                    if (found[k] || q + kWinStep >= wl[k]) open[k] = false;
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < kPerW; ++k)
+                if (it[k].x >= 0) window_done<kW, kStats>(p, t, it[k], found[k], cj[k], ct[k], alive[k], seen[k]);
+        }
+        __syncthreads();  // the queue is refilled by the next chunk
     }
     if (kPolicy && p.sym && t >= kRetireFrom) retire_red<kPolicy>(p, t, par, n_red);
 }
@@ -1825,7 +1917,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_rounds(Params p)
             ctl->cnt[par ^ 1][threadIdx.x] = 0;
             if (threadIdx.x == 0) ctl->retired[par ^ 1] = 0;
         }
-        scan_window<kW, kStats, kPolicy>(p, t, par);
+        scan_window<kW, kStats, kPolicy>(p, sm, t, par);
         if (!grid_sync(p.bar, p.ctl, p.tstamp, 3 * t + 1, p.spin_limit, p.skip_mark)) return;
         // phase A2 (all blocks see the same fallback count)
         if (__ldcg(&ctl->staged_pack) != 0ull) {
