@@ -5,7 +5,10 @@ independent graphs does: shard_batch splits the graphs into contiguous ranges of
 about equal adjacency entries, every rank computing the same split with no
 message, and bench.py's make_batch generates only the rank's own range.  These
 tests check the split, and that two gloo ranks' shards agree on it, are
-disjoint, cover the batch and concatenate to the single-process batch."""
+disjoint, cover the batch and concatenate to the single-process batch.  Each
+rank then matches the graphs of its shard (the oracle's restatement stands in
+for the kernel: no GPU here) and rank 0 gathers the results over the process
+group; they must equal the single-process batch's, graph by graph."""
 from __future__ import annotations
 
 import importlib.util
@@ -64,6 +67,26 @@ def _free_port():
         return s.getsockname()[1]
 
 
+def _match_graphs(mm, u, offsets, type_=9):
+    """Weighted maximal matching of each graph of a batch union, one graph at a
+    time (the oracle's restatement): [(match in the graph's numbering, rounds)]."""
+    import sys
+
+    sys.path.insert(0, str(ROOT))
+    import oracle
+
+    seeds = oracle.rand_seeds(12345, 256)
+    r = np.asarray(u.ranges, np.int64).reshape(-1, 2)
+    out = []
+    for i in range(len(offsets) - 1):
+        lo, hi = int(offsets[i]), int(offsets[i + 1])
+        e0, e1 = int(r[lo, 0]), int(r[hi - 1, 1])
+        x = mm.Graph(hi - lo, (r[lo:hi] - e0).astype(np.int32), u.nbrs[e0:e1] - lo, u.weights[e0:e1])
+        m, rounds, _ = oracle.match(x, type_, seeds, 0x88B81733)
+        out.append((np.asarray(m, np.int32), int(rounds)))
+    return out
+
+
 def _rank_main(rank, world, port, out_dir, count, seed):
     import torch.distributed as dist
 
@@ -91,6 +114,14 @@ def _rank_main(rank, world, port, out_dir, count, seed):
         assert all(a[1] == b[0] for a, b in zip(ranges, ranges[1:]))
         np.savez(Path(out_dir) / f"rank{rank}.npz", ranges=np.asarray(g.ranges), nbrs=np.asarray(g.nbrs),
                  weights=np.asarray(g.weights), offsets=batch["offsets"], lo_hi=np.asarray(batch["range"]))
+        # each rank matches its own graphs; rank 0 gathers every rank's results
+        matched = _match_graphs(mm, g, batch["offsets"])
+        every = [None] * world if rank == 0 else None
+        dist.gather_object(matched, every, dst=0)
+        if rank == 0:
+            flat = [x for part in every for x in part]
+            np.savez(Path(out_dir) / "gathered.npz", match=np.concatenate([m for m, _ in flat]),
+                     rounds=np.asarray([r for _, r in flat]))
         dist.barrier()
     finally:
         dist.destroy_process_group()
@@ -121,3 +152,8 @@ def test_two_gloo_ranks_shard_the_batch(mm, tmp_path):
     assert np.array_equal(np.concatenate(offs), fb["offsets"].astype(np.int64))
     lo_hi = [tuple(s["lo_hi"]) for s in shards]
     assert lo_hi[0][0] == 0 and lo_hi[0][1] == lo_hi[1][0] and lo_hi[1][1] == count * world
+    # the gathered per-rank matchings equal the single-process batch's
+    got = np.load(tmp_path / "gathered.npz")
+    want = _match_graphs(mm, full, fb["offsets"])
+    assert np.array_equal(got["match"], np.concatenate([m for m, _ in want]))
+    assert got["rounds"].tolist() == [r for _, r in want]
