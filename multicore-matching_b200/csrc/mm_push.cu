@@ -398,8 +398,12 @@ struct Smem {
     int tile_warp[kWarps][2];             // compaction: per-warp counts, then offsets
     int tile_base[2];                     // compaction: tile bases
     uint32_t seeds[256];                  // the call's colouring seeds (finish phase)
-    int wqueue_n;                         // window scan: vertices queued for sub-pass B
+    int wnext;                            // window scan: next item of the block's share
+    int stage_n;                          // window scan: fallback lists collected by the block
 };
+
+// window scan: fallback lists a block collects in its (then unused) staging area
+constexpr int kStageCap = (int)(sizeof(LongStage) * kWarps / sizeof(int4));
 
 // ---- learned colouring ----
 //
@@ -607,11 +611,7 @@ __device__ void init_phase(const Params &p, Smem &sm)
 // fits in its window and has no red candidate is decided too (unmatchable iff
 // no entry is unmatched).  A longer list with no red candidate in its window
 // falls back to a full scan in phase A2: it is appended to the round's
-// fallback list.  The first two entries of every vertex are read in one step
-// (sub-pass A below); the rest, for vertices those leave open, kWinStep at a
-// time, kPerW vertices per thread.
-constexpr int kPerW = 2;
-constexpr int kWinStep = 4;  // window entries per step after the first two
+// fallback list.
 
 // Learned colouring, graphs with symmetric structure: a red vertex of at most
 // kRetireMaxDeg entries whose neighbours are all matched leaves in phase A of
@@ -667,8 +667,8 @@ __device__ __forceinline__ void retire_red(const Params &p, int t, int par, int 
 // or decide "no proposal" / "unmatchable" for a list that fits its window, or
 // stage a longer list with no red candidate in its window for the fallback scan.
 template <bool kW, bool kStats>
-__device__ __forceinline__ void window_done(const Params &p, int t, int4 it, bool found, int cj, int ct, bool alive,
-                                            int seen)
+__device__ __forceinline__ void window_done(const Params &p, Smem &sm, int t, int4 it, bool found, int cj, int ct,
+                                            bool alive, int seen)
 {
     Ctl *ctl = p.ctl;
     const int v = it.x, deg = degree_of(it);
@@ -686,7 +686,15 @@ __device__ __forceinline__ void window_done(const Params &p, int t, int4 it, boo
             no_proposal(p, v, alive);
         }
     } else {
-        // fallback: the whole list is scanned in phase A2
+        // fallback: the whole list is scanned in phase A2.  The block collects
+        // its fallback lists in shared memory and appends them to the round's
+        // list at the end of the phase, with one global atomic; only a list
+        // that finds the block's buffer full is appended at once.
+        const int slot = atomicAdd(&sm.stage_n, 1);
+        if (slot < kStageCap) {
+            reinterpret_cast<int4 *>(&sm.stage[0])[slot] = make_int4(v, it.y, it.z, 0);
+            return;
+        }
         const unsigned long long old = atomicAdd(&ctl->staged_pack, (1ull << 32) | (unsigned long long)(unsigned)deg);
         const int idx = (int)(old >> 32), off = (int)(old & 0xffffffffull);
         p.staged[idx] = make_int4(v, it.y, it.z, off);
@@ -726,15 +734,17 @@ __device__ __forceinline__ bool window_choice(const Params &p, uint8_t c, int j)
     return c == kRed && (!kW || (p.wwin ? __int_as_float(j) > -1.0f : j >= 0));
 }
 
-// Phase A1.  A block takes kWinA * kThreads blue items at a time.  Sub-pass A:
-// each thread reads the first two window entries of kWinA vertices (in the
-// first rounds most vertices stop there), with all their loads in flight at
-// once, and ends every vertex those entries decide.  The others go to a queue
-// in shared memory (the fallback scan's staging area; bit 31 of the window
-// offset records whether an unmatched neighbour was seen), and sub-pass B
-// continues them two vertices a thread, kWinStep entries a step.
-constexpr int kWinA = 4;
-static_assert(kWinA * kThreads * (int)sizeof(int4) <= (int)sizeof(LongStage) * kWarps, "window queue fits the staging area");
+// Phase A1.  Each block takes an equal share of the round's blue items, in
+// chunks of kScanChunk interleaved with the other blocks' (ids, and with them
+// degrees, cluster in the worklists: on R-MAT graphs the hubs have small ids),
+// and hands them to its warps 32 at a time from a counter in shared memory.  A lane
+// holds one vertex at a time and reads its window two entries a step (one
+// 16-byte load, then the two colours); as soon as a lane's vertex is decided it
+// swaps in the item it prefetched and prefetches the next, so every lane keeps
+// an independent chain of loads in flight and no lane waits for the slowest
+// vertex of its warp or block.  Block barriers come only before the scan (the
+// counter) and after it (the block's fallback lists are appended at once).
+constexpr int kScanChunk = 64;
 
 template <bool kW, bool kStats, bool kPolicy>
 __device__ void scan_window(const Params &p, Smem &sm, int t, int par)
@@ -743,130 +753,128 @@ __device__ void scan_window(const Params &p, Smem &sm, int t, int par)
     const int n_blue = __ldcg(&ctl->cnt[par][kBlue]);
     const int n_red = kPolicy ? __ldcg(&ctl->cnt[par][kRed]) : 0;  // read with n_blue: one round trip
     const int4 *list = p.lists[par][kBlue];
-    int4 *queue = reinterpret_cast<int4 *>(&sm.stage[0]);
-    constexpr long long kChunk = (long long)kWinA * kThreads;
-    for (long long c0 = (long long)blockIdx.x * kChunk; c0 < n_blue; c0 += (long long)gridDim.x * kChunk) {
-        if (threadIdx.x == 0) sm.wqueue_n = 0;
-        __syncthreads();
-        // sub-pass A: the first two entries of kWinA vertices a thread
-        {
-            int4 it[kWinA];
-            int wl[kWinA], n0[kWinA], j0[kWinA], n1[kWinA], j1[kWinA];
-#pragma unroll
-            for (int k = 0; k < kWinA; ++k) {
-                const long long i = c0 + k * kThreads + threadIdx.x;
-                it[k] = i < n_blue ? __ldcg(list + i) : make_int4(-1, 0, 0, 0);
-                wl[k] = it[k].x >= 0 ? win_len(degree_of(it[k])) : 0;
-            }
-#pragma unroll
-            for (int k = 0; k < kWinA; ++k) window_pair<kW>(p, it[k], wl[k], 0, n0[k], j0[k], n1[k], j1[k]);
-            uint8_t ca[kWinA], cb[kWinA];
-#pragma unroll
-            for (int k = 0; k < kWinA; ++k) {
-                ca[k] = wl[k] > 0 ? p.col[n0[k]] : (uint8_t)kMatched;
-                cb[k] = wl[k] > 1 ? p.col[n1[k]] : (uint8_t)kMatched;
-            }
-#pragma unroll
-            for (int k = 0; k < kWinA; ++k) {
-                if (it[k].x < 0) continue;
-                bool found = false, alive = false;
-                int cj = -1, ct = 0, seen = 0;
-                if (wl[k] > 0) {
-                    seen = 1;
-                    if (window_choice<kW>(p, ca[k], j0[k])) {
-                        found = true;
-                        cj = j0[k];
-                        ct = n0[k];
-                    } else {
-                        alive = ca[k] != kMatched;
-                        if (wl[k] > 1) {
-                            seen = 2;
-                            if (window_choice<kW>(p, cb[k], j1[k])) {
-                                found = true;
-                                cj = j1[k];
-                                ct = n1[k];
-                            } else {
-                                alive |= cb[k] != kMatched;
-                            }
-                        }
-                    }
-                }
-                if (found || wl[k] <= 2) {
-                    window_done<kW, kStats>(p, t, it[k], found, cj, ct, alive, seen);
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    // this block's items: chunk c of its share is chunk c * gridDim.x + blockIdx.x of the list
+    const long long span = (long long)gridDim.x * kScanChunk;
+    const long long full = n_blue / span, rest = n_blue - full * span;
+    const int bhi = (int)(full * kScanChunk + min((long long)kScanChunk, max(0ll, rest - (long long)blockIdx.x * kScanChunk)));
+    if (threadIdx.x == 0) {
+        sm.wnext = 0;
+        sm.stage_n = 0;
+    }
+    __syncthreads();
+    bool dry = bhi == 0;  // warp-uniform: the block's share is handed out
+    // Items for the lanes in `mask`: one shared atomic per warp.  Returns this
+    // lane's item index in the list, or -1.
+    auto grab = [&](unsigned mask) -> long long {
+        const int leader = __ffs(mask) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(&sm.wnext, __popc(mask));
+        base = __shfl_sync(kFull, base, leader);
+        dry = base + __popc(mask) >= bhi;
+        const int k = base + __popc(mask & below);
+        if (!((mask >> lane) & 1u) || k >= bhi) return -1;
+        return (long long)(k / kScanChunk) * span + (long long)blockIdx.x * kScanChunk + k % kScanChunk;
+    };
+    int4 cur = make_int4(-1, 0, 0, 0), nxt = make_int4(-1, 0, 0, 0);
+    if (!dry) {
+        const long long i0 = grab(kFull);
+        if (i0 >= 0) cur = __ldcg(list + i0);
+    }
+    if (!dry) {
+        const long long i1 = grab(kFull);
+        if (i1 >= 0) nxt = __ldcg(list + i1);
+    }
+    bool has = cur.x >= 0, alive = false;
+    int q = 0, wl = has ? win_len(degree_of(cur)) : 0;
+    while (__any_sync(kFull, has)) {
+        if (has) {
+            int n0, j0, n1, j1;
+            window_pair<kW>(p, cur, wl, q, n0, j0, n1, j1);
+            const uint8_t c0 = q < wl ? p.col[n0] : (uint8_t)kMatched;
+            const uint8_t c1 = q + 1 < wl ? p.col[n1] : (uint8_t)kMatched;
+            bool found = false;
+            int cj = -1, ct = 0, seen = q;
+            if (q < wl) {
+                seen = q + 1;
+                if (window_choice<kW>(p, c0, j0)) {
+                    found = true;
+                    cj = j0;
+                    ct = n0;
                 } else {
-                    const int q = atomicAdd(&sm.wqueue_n, 1);
-                    queue[q] = make_int4(it[k].x, it[k].y, it[k].z, (int)((unsigned)it[k].w | (alive ? 0x80000000u : 0u)));
-                }
-            }
-        }
-        __syncthreads();
-        // sub-pass B: the queued vertices from entry 2 on
-        const int qn = sm.wqueue_n;
-        for (int i0 = threadIdx.x; i0 < qn; i0 += kThreads * kPerW) {
-            int4 it[kPerW];
-            int wl[kPerW], cj[kPerW], ct[kPerW], seen[kPerW];
-            bool open[kPerW], alive[kPerW], found[kPerW];
-#pragma unroll
-            for (int k = 0; k < kPerW; ++k) {
-                const int i = i0 + k * kThreads;
-                it[k] = i < qn ? queue[i] : make_int4(-1, 0, 0, 0);
-                alive[k] = it[k].w < 0;  // bit 31
-                it[k].w &= 0x7fffffff;
-                wl[k] = it[k].x >= 0 ? win_len(degree_of(it[k])) : 0;
-                open[k] = wl[k] > 2;
-                found[k] = false;
-                cj[k] = -1;
-                ct[k] = 0;
-                seen[k] = 2;
-            }
-            for (int q = 2; q < kWin; q += kWinStep) {
-                bool any = false;
-#pragma unroll
-                for (int k = 0; k < kPerW; ++k) any |= open[k];
-                if (!any) break;
-                int nb[kPerW][kWinStep], jv[kPerW][kWinStep];
-#pragma unroll
-                for (int k = 0; k < kPerW; ++k) {
-#pragma unroll
-                    for (int h = 0; h < kWinStep / 2; ++h) {
-                        nb[k][2 * h] = nb[k][2 * h + 1] = 0;
-                        jv[k][2 * h] = jv[k][2 * h + 1] = 0;
-                        if (open[k]) window_pair<kW>(p, it[k], wl[k], q + 2 * h, nb[k][2 * h], jv[k][2 * h],
-                                                     nb[k][2 * h + 1], jv[k][2 * h + 1]);
-                    }
-                }
-                uint8_t c[kPerW][kWinStep];
-#pragma unroll
-                for (int k = 0; k < kPerW; ++k) {
-#pragma unroll
-                    for (int x = 0; x < kWinStep; ++x) {
-                        c[k][x] = kMatched;
-                        if (open[k] && q + x < wl[k]) c[k][x] = p.col[nb[k][x]];
-                    }
-                }
-#pragma unroll
-                for (int k = 0; k < kPerW; ++k) {
-                    if (!open[k]) continue;
-#pragma unroll
-                    for (int x = 0; x < kWinStep; ++x) {
-                        if (q + x >= wl[k] || found[k]) continue;
-                        seen[k] += 1;
-                        if (window_choice<kW>(p, c[k][x], jv[k][x])) {
-                            cj[k] = jv[k][x];
-                            ct[k] = nb[k][x];
-                            found[k] = true;
+                    alive |= c0 != kMatched;
+                    if (q + 1 < wl) {
+                        seen = q + 2;
+                        if (window_choice<kW>(p, c1, j1)) {
+                            found = true;
+                            cj = j1;
+                            ct = n1;
                         } else {
-                            alive[k] |= c[k][x] != kMatched;
+                            alive |= c1 != kMatched;
                         }
                     }
-                    if (found[k] || q + kWinStep >= wl[k]) open[k] = false;
                 }
             }
-#pragma unroll
-            for (int k = 0; k < kPerW; ++k)
-                if (it[k].x >= 0) window_done<kW, kStats>(p, t, it[k], found[k], cj[k], ct[k], alive[k], seen[k]);
+            q += 2;
+            if (found || q >= wl) {
+                window_done<kW, kStats>(p, sm, t, cur, found, cj, ct, alive, seen);
+                has = false;
+            }
         }
-        __syncthreads();  // the queue is refilled by the next chunk
+        // lanes whose vertex is decided take their prefetched item and prefetch the next
+        const unsigned need = __ballot_sync(kFull, !has && nxt.x >= 0);
+        if (need) {
+            if (!has && nxt.x >= 0) {
+                cur = nxt;
+                nxt.x = -1;
+                has = true;
+                alive = false;
+                q = 0;
+                wl = win_len(degree_of(cur));
+            }
+            if (!dry) {
+                const long long i = grab(need);
+                if (i >= 0) nxt = __ldcg(list + i);
+            }
+        }
+    }
+    // append the block's fallback lists: one atomic for the block, item
+    // offsets by a block-wide prefix sum of their lengths
+    __syncthreads();
+    const int ns = min(sm.stage_n, kStageCap);
+    if (ns > 0) {
+        const int4 *buf = reinterpret_cast<const int4 *>(&sm.stage[0]);
+        const int warp = threadIdx.x >> 5;
+        const int per = (ns + kThreads - 1) / kThreads;
+        const int lo = min(ns, (int)threadIdx.x * per), hi = min(ns, lo + per);
+        int s = 0;
+        for (int i = lo; i < hi; ++i) s += degree_of(buf[i]);
+        const int incl = warp_incl_scan(s);
+        if (lane == 31) sm.tile_warp[warp][0] = incl;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int run = 0;
+            for (int w = 0; w < kWarps; ++w) {
+                const int x = sm.tile_warp[w][0];
+                sm.tile_warp[w][0] = run;
+                run += x;
+            }
+            const unsigned long long old =
+                atomicAdd(&ctl->staged_pack, ((unsigned long long)ns << 32) | (unsigned long long)(unsigned)run);
+            sm.tile_base[0] = (int)(old >> 32);
+            sm.tile_base[1] = (int)(old & 0xffffffffull);
+        }
+        __syncthreads();
+        int off = sm.tile_base[1] + sm.tile_warp[warp][0] + incl - s;
+        for (int i = lo; i < hi; ++i) {
+            const int4 it = buf[i];
+            const int idx = sm.tile_base[0] + i, deg = degree_of(it);
+            p.staged[idx] = make_int4(it.x, it.y, it.z, off);
+            for (int sg = (off + kSegEntries - 1) / kSegEntries; sg * kSegEntries < off + deg; ++sg) p.seg_first[sg] = idx;
+            off += deg;
+        }
+        __syncthreads();  // the buffer and the tile words are reused
     }
     if (kPolicy && p.sym && t >= kRetireFrom) retire_red<kPolicy>(p, t, par, n_red);
 }
