@@ -67,6 +67,7 @@ constexpr int kThreads = 512;            // threads per block of the round kerne
 constexpr int kWarps = kThreads / 32;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kWin = 32;                 // preference window: the first min(deg, 32) choices
+constexpr int kReqFallback = -3;         // reqi: the item's list went to the fallback scan
 constexpr int kSegEntries = 256;         // entries per fallback segment: 8 rows of 32; at most 9
                                          // pieces of lists > 32 entries overlap one segment
 
@@ -109,7 +110,9 @@ struct Params {
     int wwin;                       // pwin's second words are weights (symmetric weighted path)
     const long long *pwin_off;      // weighted: first window slot of each vertex (< 2^31)
     uint8_t *col;
-    int2 *req;
+    int2 *req;                      // per vertex: proposal of a fallback list (and the finish phase's item map)
+    int2 *reqi;                     // per blue item of the round: {target, key low half}, -1 unmatchable,
+                                    // -2 no proposal, kReqFallback: look in req
     unsigned long long *best;       // per red vertex: max proposal key this round
     unsigned long long *part_key;   // per cut fallback list: max over finished pieces
     int *part_cnt;                  // per cut fallback list: finished pieces
@@ -305,7 +308,7 @@ __device__ __forceinline__ void fold_entry(uint8_t c, float w, int j, float &bw,
 // Blue vertex v proposes to `target`, the neighbour at position j of its list
 // (begin = first position): the reverse key of that slot goes to best[target].
 template <bool kW>
-__device__ __forceinline__ void propose_to(const Params &p, int v, int begin, int j, int target)
+__device__ __forceinline__ void propose_to(const Params &p, int2 *rq, int v, int begin, int j, int target)
 {
     unsigned long long rk;
     if (p.sym) {
@@ -322,29 +325,29 @@ __device__ __forceinline__ void propose_to(const Params &p, int v, int begin, in
         rk = __ldg(p.revkey + slot);
     }
     if (rk) atomicMax(&p.best[target], rk);
-    p.req[v] = make_int2(target, (int)(uint32_t)rk);
+    *rq = make_int2(target, (int)(uint32_t)rk);
 }
 
 // Symmetric weighted path, windows carrying weights: blue v proposes to
 // `target` through an entry of weight w (w > -1); the target's entry for v has
 // the same weight, and v's id breaks ties (smaller first).
-__device__ __forceinline__ void propose_weight(const Params &p, int v, float w, int target)
+__device__ __forceinline__ void propose_weight(const Params &p, int2 *rq, int v, float w, int target)
 {
     const unsigned long long rk = ((unsigned long long)weight_order(w) << 32) | (uint32_t)~v;
     atomicMax(&p.best[target], rk);
-    p.req[v] = make_int2(target, (int)(uint32_t)rk);
+    *rq = make_int2(target, (int)(uint32_t)rk);
 }
 
 // Blue vertex v without a red choice: unmatchable if no neighbour is
 // unmatched (requests == n + 1), else no proposal this round.
-__device__ __forceinline__ void no_proposal(const Params &p, int v, bool alive)
+__device__ __forceinline__ void no_proposal(const Params &p, int2 *rq, int v, bool alive)
 {
     if (!alive) {
         p.col[v] = kDead;
         p.ctl->match[v] = 2;
-        p.req[v] = make_int2(-1, 0);
+        *rq = make_int2(-1, 0);
     } else {
-        p.req[v] = make_int2(-2, 0);
+        *rq = make_int2(-2, 0);
     }
 }
 
@@ -353,11 +356,11 @@ template <bool kW>
 __device__ __forceinline__ void propose(const Params &p, int v, int begin, unsigned long long key)
 {
     if (key < 2) {
-        no_proposal(p, v, key == 1);
+        no_proposal(p, p.req + v, v, key == 1);
         return;
     }
     const int j = (int)~(uint32_t)key;
-    propose_to<kW>(p, v, begin, j, __ldg(p.nbrs + j));
+    propose_to<kW>(p, p.req + v, v, begin, j, __ldg(p.nbrs + j));
 }
 
 // Adjacency entries the reference's request loop inspects for this vertex
@@ -667,8 +670,8 @@ __device__ __forceinline__ void retire_red(const Params &p, int t, int par, int 
 // or decide "no proposal" / "unmatchable" for a list that fits its window, or
 // stage a longer list with no red candidate in its window for the fallback scan.
 template <bool kW, bool kStats>
-__device__ __forceinline__ void window_done(const Params &p, Smem &sm, int t, int4 it, bool found, int cj, int ct,
-                                            bool alive, int seen)
+__device__ __forceinline__ void window_done(const Params &p, Smem &sm, int t, long long i, int4 it, bool found, int cj,
+                                            int ct, bool alive, int seen)
 {
     Ctl *ctl = p.ctl;
     const int v = it.x, deg = degree_of(it);
@@ -680,12 +683,14 @@ __device__ __forceinline__ void window_done(const Params &p, Smem &sm, int t, in
             atomicAdd(&p.stats[(size_t)t * MM_STATS_COLS + MM_ST_BLUE_DEG], (unsigned long long)deg);
         }
         if (found) {
-            if (kW && p.wwin) propose_weight(p, v, __int_as_float(cj), ct);
-            else propose_to<kW>(p, v, it.y, cj & 0x7fffffff, ct);
+            if (kW && p.wwin) propose_weight(p, p.reqi + i, v, __int_as_float(cj), ct);
+            else propose_to<kW>(p, p.reqi + i, v, it.y, cj & 0x7fffffff, ct);
         } else {
-            no_proposal(p, v, alive);
+            no_proposal(p, p.reqi + i, v, alive);
         }
     } else {
+        // the fallback scan proposes through req[v]
+        p.reqi[i] = make_int2(kReqFallback, 0);
         // fallback: the whole list is scanned in phase A2.  The block collects
         // its fallback lists in shared memory and appends them to the round's
         // list at the end of the phase, with one global atomic; only a list
@@ -745,6 +750,7 @@ __device__ __forceinline__ bool window_choice(const Params &p, uint8_t c, int j)
 // vertex of its warp or block.  Block barriers come only before the scan (the
 // counter) and after it (the block's fallback lists are appended at once).
 constexpr int kScanChunk = 64;
+constexpr int kWinNarrow = 4;  // window entries read two a step; later steps read four
 
 template <bool kW, bool kStats, bool kPolicy>
 __device__ void scan_window(const Params &p, Smem &sm, int t, int par)
@@ -777,48 +783,47 @@ __device__ void scan_window(const Params &p, Smem &sm, int t, int par)
         if (!((mask >> lane) & 1u) || k >= bhi) return -1;
         return (long long)(k / kScanChunk) * span + (long long)blockIdx.x * kScanChunk + k % kScanChunk;
     };
+    // the lane's vertex and its prefetched next, with their item indices
     int4 cur = make_int4(-1, 0, 0, 0), nxt = make_int4(-1, 0, 0, 0);
+    int ci = -1, ni = -1;  // item indices (a list holds at most n < 2^31 items)
     if (!dry) {
-        const long long i0 = grab(kFull);
-        if (i0 >= 0) cur = __ldcg(list + i0);
+        ci = (int)grab(kFull);
+        if (ci >= 0) cur = __ldcg(list + ci);
     }
     if (!dry) {
-        const long long i1 = grab(kFull);
-        if (i1 >= 0) nxt = __ldcg(list + i1);
+        ni = (int)grab(kFull);
+        if (ni >= 0) nxt = __ldcg(list + ni);
     }
     bool has = cur.x >= 0, alive = false;
     int q = 0, wl = has ? win_len(degree_of(cur)) : 0;
     while (__any_sync(kFull, has)) {
         if (has) {
-            int n0, j0, n1, j1;
-            window_pair<kW>(p, cur, wl, q, n0, j0, n1, j1);
-            const uint8_t c0 = q < wl ? p.col[n0] : (uint8_t)kMatched;
-            const uint8_t c1 = q + 1 < wl ? p.col[n1] : (uint8_t)kMatched;
+            // two entries a step for the first kWinNarrow, then four
+            const int width = q < kWinNarrow ? 2 : 4;
+            int nb[4], jv[4];
+            window_pair<kW>(p, cur, wl, q, nb[0], jv[0], nb[1], jv[1]);
+            nb[2] = nb[3] = jv[2] = jv[3] = 0;
+            if (width == 4) window_pair<kW>(p, cur, wl, q + 2, nb[2], jv[2], nb[3], jv[3]);
+            uint8_t c[4];
+#pragma unroll
+            for (int x = 0; x < 4; ++x) c[x] = x < width && q + x < wl ? p.col[nb[x]] : (uint8_t)kMatched;
             bool found = false;
             int cj = -1, ct = 0, seen = q;
-            if (q < wl) {
-                seen = q + 1;
-                if (window_choice<kW>(p, c0, j0)) {
+#pragma unroll
+            for (int x = 0; x < 4; ++x) {
+                if (x >= width || q + x >= wl || found) continue;
+                seen = q + x + 1;
+                if (window_choice<kW>(p, c[x], jv[x])) {
                     found = true;
-                    cj = j0;
-                    ct = n0;
+                    cj = jv[x];
+                    ct = nb[x];
                 } else {
-                    alive |= c0 != kMatched;
-                    if (q + 1 < wl) {
-                        seen = q + 2;
-                        if (window_choice<kW>(p, c1, j1)) {
-                            found = true;
-                            cj = j1;
-                            ct = n1;
-                        } else {
-                            alive |= c1 != kMatched;
-                        }
-                    }
+                    alive |= c[x] != kMatched;
                 }
             }
-            q += 2;
+            q += width;
             if (found || q >= wl) {
-                window_done<kW, kStats>(p, sm, t, cur, found, cj, ct, alive, seen);
+                window_done<kW, kStats>(p, sm, t, ci, cur, found, cj, ct, alive, seen);
                 has = false;
             }
         }
@@ -827,6 +832,7 @@ __device__ void scan_window(const Params &p, Smem &sm, int t, int par)
         if (need) {
             if (!has && nxt.x >= 0) {
                 cur = nxt;
+                ci = ni;
                 nxt.x = -1;
                 has = true;
                 alive = false;
@@ -834,8 +840,11 @@ __device__ void scan_window(const Params &p, Smem &sm, int t, int par)
                 wl = win_len(degree_of(cur));
             }
             if (!dry) {
-                const long long i = grab(need);
-                if (i >= 0) nxt = __ldcg(list + i);
+                const int i = (int)grab(need);
+                if (i >= 0) {
+                    nxt = __ldcg(list + i);
+                    ni = i;
+                }
             }
         }
     }
@@ -1103,33 +1112,49 @@ __device__ void commit_phase(const Params &p, Smem &sm, int t, bool has_next)
     const uint32_t barrier = ctl->barrier;
     const int c0 = __ldcg(&ctl->cnt[par][kBlue]), c1 = __ldcg(&ctl->cnt[par][kRed]);
     const long long total = (long long)c0 + c1;
-    const long long ntiles = (total + kTileItems - 1) / kTileItems;
+    // tiles of at most kTileItems items, as many for every block (the last tile may be short)
+    const long long per_block = (total + (long long)gridDim.x * kTileItems - 1) / ((long long)gridDim.x * kTileItems);
+    const long long tsize = per_block > 0 ? (total + (long long)gridDim.x * per_block - 1) / ((long long)gridDim.x * per_block) : 1;
+    const long long ntiles = (total + tsize - 1) / tsize;
     int *match = ctl->match;
     int retired = 0;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long long base = tile * tsize, tend = min(total, base + tsize);
+        // items, and with a blue item its request, loaded together
         int4 it[kPer];
+        int2 q[kPer];
         bool in[kPer], blue[kPer], gone[kPer];
 #pragma unroll
         for (int k = 0; k < kPer; ++k) {
-            const long long i = tile * kTileItems + k * kThreads + threadIdx.x;
-            in[k] = i < total;
+            const long long i = base + k * kThreads + threadIdx.x;
+            in[k] = i < tend;
             blue[k] = i < c0;
             it[k] = make_int4(0, 0, 0, 0);
-            if (in[k]) it[k] = blue[k] ? __ldcg(p.lists[par][kBlue] + i) : __ldcg(p.lists[par][kRed] + (i - c0));
+            q[k] = make_int2(-1, 0);
+            if (in[k]) {
+                if (blue[k]) {
+                    it[k] = __ldcg(p.lists[par][kBlue] + i);
+                } else {
+                    it[k] = __ldcg(p.lists[par][kRed] + (i - c0));
+                }
+            }
             // learned colouring: a red item retired in phase A carries its id complemented
             gone[k] = kPolicy && in[k] && !blue[k] && it[k].x < 0;
             if (gone[k]) it[k].x = ~it[k].x;
         }
-        // proposal state: blue -> its request, red -> the best proposal it received
-        int2 q[kPer];
+        // proposal state: blue -> its request (a fallback list's is in req), red -> the
+        // best proposal it received
         unsigned long long key[kPer];
 #pragma unroll
         for (int k = 0; k < kPer; ++k) {
-            q[k] = make_int2(-1, 0);
             key[k] = 0ull;
             if (in[k]) {
-                if (blue[k]) q[k] = __ldcg(p.req + it[k].x);
-                else key[k] = __ldcg(p.best + it[k].x);
+                if (blue[k]) {
+                    q[k] = __ldcg(p.reqi + (base + k * kThreads + threadIdx.x));
+                    if (q[k].x == kReqFallback) q[k] = __ldcg(p.req + it[k].x);
+                } else {
+                    key[k] = __ldcg(p.best + it[k].x);
+                }
             }
         }
 #pragma unroll
@@ -2523,6 +2548,7 @@ constexpr int kStampCount = 3 * kMaxRounds + 1;
 struct PushState {
     uint8_t *col = nullptr;
     int2 *req = nullptr;
+    int2 *reqi = nullptr;
     unsigned long long *best = nullptr;
     unsigned long long *part_key = nullptr;
     int *part_cnt = nullptr;
@@ -2548,6 +2574,7 @@ void free_state(PushState *s)
     // callers have synchronised the device (graph destroy or a failed set-up)
     dev_free(s->col, 0);
     dev_free(s->req, 0);
+    dev_free(s->reqi, 0);
     dev_free(s->best, 0);
     dev_free(s->part_key, 0);
     dev_free(s->part_cnt, 0);
@@ -2605,6 +2632,7 @@ mm_status alloc_state(mm_graph *g, PushState **out)
     cudaError_t e = cudaSuccess;
     if (e == cudaSuccess) e = dev_alloc((void **)&s->col, n, 0);
     if (e == cudaSuccess) e = dev_alloc((void **)&s->req, n * sizeof(int2), 0);
+    if (e == cudaSuccess) e = dev_alloc((void **)&s->reqi, n * sizeof(int2), 0);
     if (e == cudaSuccess) e = dev_alloc((void **)&s->best, n * sizeof(unsigned long long), 0);
     if (e == cudaSuccess) e = dev_alloc((void **)&s->part_key, n * sizeof(unsigned long long), 0);
     if (e == cudaSuccess) e = dev_alloc((void **)&s->part_cnt, n * sizeof(int), 0);
@@ -2694,6 +2722,7 @@ Params make_params(mm_graph *g, PushState *s, bool weighted, bool stats, bool ti
     p.pwin_off = g->d_pwin_off;
     p.col = s->col;
     p.req = s->req;
+    p.reqi = s->reqi;
     p.best = s->best;
     p.part_key = s->part_key;
     p.part_cnt = s->part_cnt;
