@@ -258,6 +258,33 @@ __device__ __noinline__ bool grid_sync(unsigned *bar, Ctl *ctl, unsigned long lo
     return s_ok != 0;
 }
 
+
+// L2 residency: the colour bytes, which every scan reads at random, are loaded
+// with an evict-last policy, the streamed worklists and requests with
+// evict-first (.cs) loads and stores.
+__device__ __forceinline__ unsigned long long pol_keep()
+{
+    unsigned long long p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint8_t ld_col(const uint8_t *a)
+{
+    unsigned short r;
+    asm volatile("ld.global.L2::cache_hint.u8 %0, [%1], %2;" : "=h"(r) : "l"(a), "l"(pol_keep()));
+    return (uint8_t)r;
+}
+// At the end of a matching the colour bytes go back to the normal eviction
+// priority, so that they do not crowd the L2 of the work that follows.
+template <class T>
+__device__ __forceinline__ void release_lines(const T *a, long long count)
+{
+    const uintptr_t lo = (uintptr_t)a & ~(uintptr_t)127, hi = (uintptr_t)(a + count);
+    const long long lines = (long long)((hi - lo + 127) / 128);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < lines; i += (long long)gridDim.x * blockDim.x)
+        asm volatile("applypriority.global.L2::evict_normal [%0], 128;" ::"l"(lo + (uintptr_t)i * 128) : "memory");
+}
+
 // Key under which a blue vertex ranks a red neighbour at position j
 // (gwRequest: strict > from -1, earliest j on ties; grRequest: earliest j).
 // Every candidate key is >= 2^31, so the value 1 can stand for "an unmatched
@@ -325,7 +352,7 @@ __device__ __forceinline__ void propose_to(const Params &p, int2 *rq, int v, int
         rk = __ldg(p.revkey + slot);
     }
     if (rk) atomicMax(&p.best[target], rk);
-    *rq = make_int2(target, (int)(uint32_t)rk);
+    __stcs(rq, make_int2(target, (int)(uint32_t)rk));
 }
 
 // Symmetric weighted path, windows carrying weights: blue v proposes to
@@ -335,7 +362,7 @@ __device__ __forceinline__ void propose_weight(const Params &p, int2 *rq, int v,
 {
     const unsigned long long rk = ((unsigned long long)weight_order(w) << 32) | (uint32_t)~v;
     atomicMax(&p.best[target], rk);
-    *rq = make_int2(target, (int)(uint32_t)rk);
+    __stcs(rq, make_int2(target, (int)(uint32_t)rk));
 }
 
 // Blue vertex v without a red choice: unmatchable if no neighbour is
@@ -345,9 +372,9 @@ __device__ __forceinline__ void no_proposal(const Params &p, int2 *rq, int v, bo
     if (!alive) {
         p.col[v] = kDead;
         p.ctl->match[v] = 2;
-        *rq = make_int2(-1, 0);
+        __stcs(rq, make_int2(-1, 0));
     } else {
-        *rq = make_int2(-2, 0);
+        __stcs(rq, make_int2(-2, 0));
     }
 }
 
@@ -537,7 +564,7 @@ __device__ __forceinline__ void compact_tile(const Params &p, Smem &sm, int pari
         if (l < 0) continue;
         const int idx = l == kBlue ? sm.tile_base[0] + sm.tile_warp[warp][0] + ex[0] + rc[0]++
                                    : sm.tile_base[1] + sm.tile_warp[warp][1] + ex[1] + rc[1]++;
-        p.lists[parity][l][idx] = item[k];
+        __stcs(&p.lists[parity][l][idx], item[k]);
     }
     __syncthreads();  // tile_warp / tile_base are reused by the next tile
 }
@@ -552,21 +579,36 @@ __device__ void init_phase(const Params &p, Smem &sm)
     const uint32_t seed = p.seeds[0], barrier = ctl->barrier;
     const int n = p.n;
     const int ntiles = (n + kTileItems - 1) / kTileItems;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        int dest[kPer];
-        int4 item[kPer];
-        unsigned long long act = 0, blue_n = 0;
+    // each tile's ranges and window offsets are loaded while the tile before
+    // it is coloured and compacted
+    int2 rr[kPer];
+    long long wo[kPer];
+    auto fetch = [&](int tile) {
 #pragma unroll
         for (int k = 0; k < kPer; ++k) {
             const int v = tile * kTileItems + k * kThreads + threadIdx.x;
+            rr[k] = make_int2(0, 0);
+            wo[k] = 0;
+            if (tile < ntiles && v < n) {
+                rr[k] = __ldg(p.ranges + v);
+                if (kW) wo[k] = __ldg(p.pwin_off + v);
+            }
+        }
+    };
+    fetch(blockIdx.x);
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        int dest[kPer];
+        int4 item[kPer];
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) item[k] = make_int4(tile * kTileItems + k * kThreads + threadIdx.x, rr[k].x, rr[k].y, (int)wo[k]);
+        fetch(tile + gridDim.x);
+        unsigned long long act = 0, blue_n = 0;
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            const int v = item[k].x;
             dest[k] = -1;
-            item[k] = make_int4(v, 0, 0, 0);
             if (v < n) {
-                const int2 r = __ldg(p.ranges + v);
-                item[k].y = r.x;
-                item[k].z = r.y;
-                if (kW) item[k].w = (int)__ldg(p.pwin_off + v);
-                const int deg = degree_of(r);
+                const int deg = degree_of(item[k]);
                 const float2 wf = kPolicy && policy_needs_features(p, 0) ? __ldg(p.wfeat + v) : make_float2(0.0f, 0.0f);
                 const bool blue = colour_blue<kPolicy>(p, v, deg, 0.0f, wf, 0, seed, barrier);
                 if (p.last) p.last[v] = 0;
@@ -788,11 +830,11 @@ __device__ void scan_window(const Params &p, Smem &sm, int t, int par)
     int ci = -1, ni = -1;  // item indices (a list holds at most n < 2^31 items)
     if (!dry) {
         ci = (int)grab(kFull);
-        if (ci >= 0) cur = __ldcg(list + ci);
+        if (ci >= 0) cur = __ldcs(list + ci);
     }
     if (!dry) {
         ni = (int)grab(kFull);
-        if (ni >= 0) nxt = __ldcg(list + ni);
+        if (ni >= 0) nxt = __ldcs(list + ni);
     }
     bool has = cur.x >= 0, alive = false;
     int q = 0, wl = has ? win_len(degree_of(cur)) : 0;
@@ -806,7 +848,7 @@ __device__ void scan_window(const Params &p, Smem &sm, int t, int par)
             if (width == 4) window_pair<kW>(p, cur, wl, q + 2, nb[2], jv[2], nb[3], jv[3]);
             uint8_t c[4];
 #pragma unroll
-            for (int x = 0; x < 4; ++x) c[x] = x < width && q + x < wl ? p.col[nb[x]] : (uint8_t)kMatched;
+            for (int x = 0; x < 4; ++x) c[x] = x < width && q + x < wl ? ld_col(p.col + nb[x]) : (uint8_t)kMatched;
             bool found = false;
             int cj = -1, ct = 0, seen = q;
 #pragma unroll
@@ -842,7 +884,7 @@ __device__ void scan_window(const Params &p, Smem &sm, int t, int par)
             if (!dry) {
                 const int i = (int)grab(need);
                 if (i >= 0) {
-                    nxt = __ldcg(list + i);
+                    nxt = __ldcs(list + i);
                     ni = i;
                 }
             }
@@ -1043,7 +1085,7 @@ __device__ void scan_long(const Params &p, Smem &sm, int t, int gwarp, int nwarp
                 for (int r = 0; r < kRows; ++r) {
                     const int e = i * 32 * kRows + r * 32 + lane;
                     if (e < seg_len) {
-                        const unsigned x = p.col[stg.nb[st][r * 32 + lane]];
+                        const unsigned x = ld_col(p.col + stg.nb[st][r * 32 + lane]);
                         c = (c & ~(0xffu << (8 * r))) | (x << (8 * r));
                     }
                 }
@@ -1133,9 +1175,9 @@ __device__ void commit_phase(const Params &p, Smem &sm, int t, bool has_next)
             q[k] = make_int2(-1, 0);
             if (in[k]) {
                 if (blue[k]) {
-                    it[k] = __ldcg(p.lists[par][kBlue] + i);
+                    it[k] = __ldcs(p.lists[par][kBlue] + i);
                 } else {
-                    it[k] = __ldcg(p.lists[par][kRed] + (i - c0));
+                    it[k] = __ldcs(p.lists[par][kRed] + (i - c0));
                 }
             }
             // learned colouring: a red item retired in phase A carries its id complemented
@@ -1150,7 +1192,7 @@ __device__ void commit_phase(const Params &p, Smem &sm, int t, bool has_next)
             key[k] = 0ull;
             if (in[k]) {
                 if (blue[k]) {
-                    q[k] = __ldcg(p.reqi + (base + k * kThreads + threadIdx.x));
+                    q[k] = __ldcs(p.reqi + (base + k * kThreads + threadIdx.x));
                     if (q[k].x == kReqFallback) q[k] = __ldcg(p.req + it[k].x);
                 } else {
                     key[k] = __ldcg(p.best + it[k].x);
@@ -1916,7 +1958,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_rounds(Params p)
     if (p.resume) {
         // the finish kernel called its attempt off: carry on from its round,
         // without another attempt
-        if (ctl->fin_state != kFinStateResume) return;
+        if (ctl->fin_state != kFinStateResume) {
+            release_lines(p.col, p.n);
+            return;
+        }
         t = ctl->fin_round;
         active0 = ctl->active0;
         fin_next = -1;
@@ -1990,6 +2035,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_rounds(Params p)
         const int v = i < cb ? __ldcg(p.lists[par][kBlue] + i).x : __ldcg(p.lists[par][kRed] + (i - cb)).x;
         match[v] = __ldcg(p.col + v);
     }
+    // the last launch of the matching (a finish kernel and a resumed round
+    // kernel follow only a hand-over, which returns above)
+    release_lines(p.col, p.n);
 }
 
 // The finish phase as its own cooperative launch, after k_rounds has stopped
