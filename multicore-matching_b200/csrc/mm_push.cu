@@ -92,6 +92,7 @@ struct Ctl {
     int fin_round;         // finish phase: the round it starts at (set by k_rounds)
     int fin_state;         // finish phase: kFinState*
     long long active0;     // vertices active at round 0 (for a resumed round kernel)
+    int iso_last;          // 1 + the last round in which a vertex without neighbours was active (0: none)
 };
 
 // Finish-phase hand-over between the launches of one matching.
@@ -153,6 +154,9 @@ struct Params {
     // threshold, computed once on the host, is policy_bar (policy_const = 1).
     int policy_const;
     uint32_t policy_bar;
+    // Learned colouring with a constant policy: the finish phase plays the
+    // remaining rounds under the policy's threshold and its retirement rule.
+    int fin_retire;
 };
 static_assert(sizeof(Params) <= 4096, "launch parameters stay within the classic 4 KB limit");
 
@@ -429,6 +433,8 @@ struct Smem {
     int tile_base[2];                     // compaction: tile bases
     uint32_t seeds[256];                  // the call's colouring seeds (finish phase)
     int wnext;                            // window scan: next item of the block's share
+    int iso_n;                            // set-up: queued vertices without neighbours
+    int iso_cnt[3];                       // set-up: survivors of a round of the queue (rotating)
     int stage_n;                          // window scan: fallback lists collected by the block
 };
 
@@ -569,15 +575,76 @@ __device__ __forceinline__ void compact_tile(const Params &p, Smem &sm, int pari
     __syncthreads();  // tile_warp / tile_base are reused by the next tile
 }
 
+// Vertices without neighbours on the symmetric path: no list names them, so
+// nothing depends on them but their own match value and the round count.  One
+// leaves (match value 2) in the first round in which it is blue, or stays red
+// to the cap (match value 1).  The set-up queues the ones red in round 0 in
+// shared memory and resolves the queue round by round, a hash per queued
+// vertex and round (a walk per thread would cost every lane its warp's longest
+// walk).  iso_last: the last round in which any of them is active (the cap's
+// last round if one stays red to it, nseeds if the seeds run out first: the
+// reference would draw more, and the round count then exceeds nseeds).
+constexpr int kIsoHalf = (int)(sizeof(LongStage) * kWarps / sizeof(int) / 2);  // queue capacity (two halves)
+constexpr int kIsoFlush = kIsoHalf - kTileItems;  // resolve once a tile could overflow the queue
+
+// Called by the whole block, after a barrier that follows the last append.
+// Round r reads the queue half qa and appends its survivors to the other,
+// counting them in iso_cnt[r % 3]: that counter is cleared by thread 0 in
+// round r - 1, after every thread read it (in round r - 3's closing step) and
+// before any thread appends to it, so one barrier a round suffices.
+__device__ void resolve_isolated(const Params &p, Smem &sm, int &iso_last)
+{
+    const Ctl *ctl = p.ctl;
+    int *qa = reinterpret_cast<int *>(&sm.stage[0]), *qb = qa + kIsoHalf;
+    const int cap = ctl->cap, lim = min(cap, ctl->nseeds);
+    const uint32_t barrier = ctl->barrier;
+    int nq = sm.iso_n;
+    if (threadIdx.x == 0) sm.iso_cnt[1] = 0;
+    __syncthreads();
+    for (int r = 1; nq > 0; ++r) {
+        int *cnt = &sm.iso_cnt[r % 3];
+        if (threadIdx.x == 0) sm.iso_cnt[(r + 1) % 3] = 0;
+        for (int i = threadIdx.x; i < nq; i += kThreads) {
+            const int v = qa[i];
+            if (r >= lim) {
+                // red in every round up to the limit
+                p.ctl->match[v] = 1;
+                if (p.last) p.last[v] = (uint8_t)(cap - 1);
+                iso_last = max(iso_last, lim == cap ? cap - 1 : lim);
+            } else if (colour_of((uint32_t)(v - base_of(p, v)), p.seeds[r], barrier) == kBlue) {
+                p.ctl->match[v] = 2;
+                if (p.last) p.last[v] = (uint8_t)r;
+                iso_last = max(iso_last, r);
+            } else {
+                qb[atomicAdd(cnt, 1)] = v;
+            }
+        }
+        __syncthreads();  // the survivors and their count are complete
+        nq = r >= lim ? 0 : *cnt;
+        int *x = qa;
+        qa = qb;
+        qb = x;
+    }
+    __syncthreads();  // every thread has left the loop before the queue is emptied
+    if (threadIdx.x == 0) sm.iso_n = 0;
+    __syncthreads();
+}
+
 // Set-up: colour every vertex with seeds[0] and fill the first worklists.
 // best[] starts at 0 and stays 0 for every vertex that is not matched: a red
-// vertex that receives a proposal is matched in the same round.
+// vertex that receives a proposal is matched in the same round.  On the
+// symmetric path the vertices without neighbours are resolved here, whatever
+// their colour (resolve_isolated); the instrumented kernel keeps them in the
+// rounds, whose per-round counters count them as the reference does.
 template <bool kW, bool kStats, bool kPolicy>
 __device__ void init_phase(const Params &p, Smem &sm)
 {
     const Ctl *ctl = p.ctl;
     const uint32_t seed = p.seeds[0], barrier = ctl->barrier;
     const int n = p.n;
+    int iso_last = -1;
+    if (threadIdx.x == 0) sm.iso_n = 0;
+    __syncthreads();
     const int ntiles = (n + kTileItems - 1) / kTileItems;
     // each tile's ranges and window offsets are loaded while the tile before
     // it is coloured and compacted
@@ -627,6 +694,10 @@ __device__ void init_phase(const Params &p, Smem &sm)
                     p.col[v] = kDead;
                     p.ctl->match[v] = 2;
                     trace_left<kPolicy>(p, 0, v);
+                } else if (!kPolicy && !kStats && p.sym && deg == 0) {
+                    // red in round 0: queued, resolved with the block's others
+                    p.col[v] = kDead;
+                    reinterpret_cast<int *>(&sm.stage[0])[atomicAdd(&sm.iso_n, 1)] = v;
                 } else {
                     p.col[v] = blue ? kBlue : kRed;
                     dest[k] = blue ? kBlue : kRed;
@@ -639,6 +710,19 @@ __device__ void init_phase(const Params &p, Smem &sm)
             stat_add(p, 0, MM_ST_RED, act - blue_n);
         }
         compact_tile(p, sm, 0, dest, item);
+        if (!kPolicy && !kStats && p.sym) {
+            // the tile's appends are complete (compact_tile's barriers); every
+            // thread reads the queue length before any appends for the next tile
+            const int qn = sm.iso_n;
+            __syncthreads();
+            if (qn > kIsoFlush) resolve_isolated(p, sm, iso_last);
+        }
+    }
+    if (!kPolicy && !kStats) {
+        if (sm.iso_n > 0) resolve_isolated(p, sm, iso_last);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) iso_last = max(iso_last, __shfl_xor_sync(kFull, iso_last, o));
+        if ((threadIdx.x & 31) == 0 && iso_last >= 0) atomicMax(&p.ctl->iso_last, iso_last + 1);
     }
 }
 
@@ -785,14 +869,13 @@ __device__ __forceinline__ bool window_choice(const Params &p, uint8_t c, int j)
 // chunks of kScanChunk interleaved with the other blocks' (ids, and with them
 // degrees, cluster in the worklists: on R-MAT graphs the hubs have small ids),
 // and hands them to its warps 32 at a time from a counter in shared memory.  A lane
-// holds one vertex at a time and reads its window two entries a step (one
-// 16-byte load, then the two colours); as soon as a lane's vertex is decided it
+// holds one vertex at a time and reads its window eight entries a step (four
+// 16-byte loads, then the eight colours); as soon as a lane's vertex is decided it
 // swaps in the item it prefetched and prefetches the next, so every lane keeps
 // an independent chain of loads in flight and no lane waits for the slowest
 // vertex of its warp or block.  Block barriers come only before the scan (the
 // counter) and after it (the block's fallback lists are appended at once).
 constexpr int kScanChunk = 64;
-constexpr int kWinNarrow = 4;  // window entries read two a step; later steps read four
 
 template <bool kW, bool kStats, bool kPolicy>
 __device__ void scan_window(const Params &p, Smem &sm, int t, int par)
@@ -840,19 +923,24 @@ __device__ void scan_window(const Params &p, Smem &sm, int t, int par)
     int q = 0, wl = has ? win_len(degree_of(cur)) : 0;
     while (__any_sync(kFull, has)) {
         if (has) {
-            // two entries a step for the first kWinNarrow, then four
-            const int width = q < kWinNarrow ? 2 : 4;
-            int nb[4], jv[4];
-            window_pair<kW>(p, cur, wl, q, nb[0], jv[0], nb[1], jv[1]);
-            nb[2] = nb[3] = jv[2] = jv[3] = 0;
-            if (width == 4) window_pair<kW>(p, cur, wl, q + 2, nb[2], jv[2], nb[3], jv[3]);
-            uint8_t c[4];
+            // eight entries a step (one dependent round trip for each 8: the scan
+            // is bound by the latency of its load chains); the first step of
+            // round 0, where most vertices stop at their first or second entry,
+            // reads four
+            const int width = q == 0 && t == 0 ? 4 : 8;
+            int nb[8], jv[8];
 #pragma unroll
-            for (int x = 0; x < 4; ++x) c[x] = x < width && q + x < wl ? ld_col(p.col + nb[x]) : (uint8_t)kMatched;
+            for (int h = 0; h < 4; ++h) {
+                nb[2 * h] = nb[2 * h + 1] = jv[2 * h] = jv[2 * h + 1] = 0;
+                if (2 * h < width) window_pair<kW>(p, cur, wl, q + 2 * h, nb[2 * h], jv[2 * h], nb[2 * h + 1], jv[2 * h + 1]);
+            }
+            uint8_t c[8];
+#pragma unroll
+            for (int x = 0; x < 8; ++x) c[x] = x < width && q + x < wl ? ld_col(p.col + nb[x]) : (uint8_t)kMatched;
             bool found = false;
             int cj = -1, ct = 0, seen = q;
 #pragma unroll
-            for (int x = 0; x < 4; ++x) {
+            for (int x = 0; x < 8; ++x) {
                 if (x >= width || q + x >= wl || found) continue;
                 seen = q + x + 1;
                 if (window_choice<kW>(p, c[x], jv[x])) {
@@ -1539,7 +1627,7 @@ __device__ __forceinline__ int fin_play(const Params &p, FinWarp &fw, const uint
     const int g = own ? mem : 0;
     const int base = own ? base_of(p, g) : 0;
     const uint32_t hid = (uint32_t)(g - base);
-    const uint32_t bar = p.ctl->barrier;
+    const uint32_t bar = p.fin_retire ? p.policy_bar : p.ctl->barrier;
     int eb = 0, ee = 0, deg = 0, beg = 0;
     if (own) {
         eb = fw.eoff[lane];
@@ -1548,6 +1636,8 @@ __device__ __forceinline__ int fin_play(const Params &p, FinWarp &fw, const uint
         beg = fw.mbeg[lane];
         fw.best[lane] = 0ull;
     }
+    // learned colouring: whether a red member may retire (its list is short enough)
+    const bool may_retire = p.fin_retire && own && degree_of(__ldg(p.ranges + g)) <= kRetireMaxDeg;
     bool act = own, blue = false;
     int val = 0, lastr = -1;
     __syncwarp();
@@ -1558,6 +1648,18 @@ __device__ __forceinline__ int fin_play(const Params &p, FinWarp &fw, const uint
         }
         if (own) fw.st[lane] = act ? (blue ? kBlue : kRed) : (val == 2 ? kDead : kMatched);
         __syncwarp();
+        // learned colouring: from round kRetireFrom a red member whose neighbours
+        // are all matched leaves at once (the round kernel's retire_red; its
+        // neighbours outside the component are matched)
+        bool retired = false;
+        if (may_retire && act && !blue && t >= kRetireFrom) {
+            bool alive = false;
+            for (int e = eb; e < ee; ++e) alive |= fw.st[fw.tgt[e]] != kMatched;
+            if (!alive) {
+                val = 2;
+                retired = true;
+            }
+        }
         // request: the best red neighbour among the members (matched ones
         // outside the component neither attract nor keep a vertex alive)
         unsigned long long best = 0ull;
@@ -1617,7 +1719,7 @@ __device__ __forceinline__ int fin_play(const Params &p, FinWarp &fw, const uint
         }
         __syncwarp();
         if (own) fw.best[lane] = 0ull;
-        if (matched || dead) act = false;
+        if (matched || dead || retired) act = false;
     }
     if (own) {
         // members still unmatched at the cap keep their last colour
@@ -1717,8 +1819,11 @@ template <bool kStats>
 __device__ __forceinline__ void fin_singles(const Params &p, const uint32_t *seeds, int t, int cap, bool mine, int v,
                                             int deg, bool blue0, int &last_all)
 {
-    const uint32_t bar = p.ctl->barrier;
+    const uint32_t bar = p.fin_retire ? p.policy_bar : p.ctl->barrier;
     const uint32_t hid = mine ? (uint32_t)(v - base_of(p, v)) : 0u;
+    // learned colouring: a short list retires as soon as it is red from round
+    // kRetireFrom (a singleton's neighbours are all matched)
+    const bool may_retire = p.fin_retire && deg <= kRetireMaxDeg;
     bool act = mine, blue = blue0;
     int lastr = -1;
     for (int r = t; r < cap && __any_sync(kFull, act); ++r) {
@@ -1738,7 +1843,7 @@ __device__ __forceinline__ void fin_singles(const Params &p, const uint32_t *see
             stat_add(p, r, MM_ST_REQ_ENTRIES, b ? (unsigned long long)deg : 0ull);
             stat_add(p, r, MM_ST_RESP_ENTRIES, rd ? (unsigned long long)deg : 0ull);
         }
-        if (act && blue) act = false;
+        if (act && (blue || (may_retire && r >= kRetireFrom))) act = false;
     }
     if (mine) {
         // still red at the cap: it keeps that colour
@@ -1980,7 +2085,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_rounds(Params p)
         // Hand the rest to the finish kernel (the symmetric path of the
         // reference's colouring only).  Every block reads the same counters and
         // leaves here; round t's worklists and colours are complete.
-        if (!kPolicy && p.sym && t > 0) {
+        if ((!kPolicy || p.fin_retire) && p.sym && t > 0) {
             const long long act = (long long)__ldcg(&ctl->cnt[par][kBlue]) + __ldcg(&ctl->cnt[par][kRed]);
             if (p.fin_div > 0 && act > 0 && act * p.fin_div <= active0 && act <= fin_next) {
                 if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -2022,6 +2127,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_rounds(Params p)
                 const int retired_all = __ldcg(&ctl->retired[par ^ 1]);
                 if (!maximal || next > 0) ctl->rounds = cap;
                 else ctl->rounds = min(retired_all > 0 ? t + 3 : t + 2, cap);
+                // vertices without neighbours resolved at set-up
+                const int iso = __ldcg(&ctl->iso_last) - 1;
+                if (maximal && iso >= 0) ctl->rounds = max(ctl->rounds, min(iso + 2, cap));
             }
             break;
         }
@@ -2092,7 +2200,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_finish(Params p)
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         if (done) {
-            const int last = __ldcg(&ctl->fin_last);
+            const int last = max(__ldcg(&ctl->fin_last), __ldcg(&ctl->iso_last) - 1);
             ctl->rounds = maximal ? min(last + 2, cap) : cap;
             ctl->fin_state = kFinStateDone;
             if (p.tstamp) p.tstamp[3 * t + 3] = p.tstamp[3 * t + 2];
@@ -2783,6 +2891,7 @@ Params make_params(mm_graph *g, PushState *s, bool weighted, bool stats, bool ti
     std::memset(p.mlp, 0, sizeof(p.mlp));
     p.policy_const = 0;
     p.policy_bar = 0u;
+    p.fin_retire = 0;
     p.level = 0.0f;
     p.wfeat = s->wfeat;
     p.trace = nullptr;
@@ -2820,6 +2929,8 @@ mm_status launch_rounds(mm_graph *g, PushState *s, bool timing, cudaStream_t str
         prm.level = pol->level;
         prm.trace = pol->trace;
         prm.trace_rounds = pol->trace_rounds;
+        // the finish phase knows the policy's threshold, not its features
+        prm.fin_retire = pol->constant && !pol->trace ? 1 : 0;
     }
     void *args[] = {&prm};
     const int mode = kPolicy ? 2 : (kStats ? 1 : 0);
@@ -2830,7 +2941,7 @@ mm_status launch_rounds(mm_graph *g, PushState *s, bool timing, cudaStream_t str
     MM_CUDA_TRY(cudaLaunchCooperativeKernel((void *)k_rounds<kW, kStats, kPolicy>, dim3(grid),
                                             dim3(kThreads), args, sizeof(Smem), stream),
                 "round kernel launch");
-    if (!kPolicy && prm.sym) {
+    if ((!kPolicy || prm.fin_retire) && prm.sym) {
         // the finish kernel (its own barrier words), then the round kernel again
         // for the case that the finish phase is called off; each returns at once
         // when there is nothing left for it
@@ -3304,7 +3415,7 @@ mm_status push_match_policy(mm_graph *g, int type, uint32_t barrier, const uint3
         }
         if (e != cudaSuccess) return cuda_fail(e, "policy state");
     }
-    MM_CUDA_TRY(cudaMemsetAsync(s->bar, 0, sizeof(unsigned) * kBarWords, stream), "barrier clear");
+    MM_CUDA_TRY(cudaMemsetAsync(s->bar, 0, sizeof(unsigned) * 2 * kBarWords, stream), "barrier clear");
     PolicyArgs pol;
     pol.mlp = mlp_host;
     // the output layer's weights W2 (after W1 and b1): all zero means every

@@ -192,3 +192,38 @@ def test_policy_mlp_device_matches_host(mm, orc, torch_cuda):
     want = (h < thr).astype(np.float32)
     assert len(rows) > 5000 and band.mean() < 0.01
     assert np.array_equal(rows[~band, 6], want[~band]), int((rows[~band, 6] != want[~band]).sum())
+
+
+@pytest.mark.parametrize("type_", [6, 7, 8, 9])
+def test_constant_policy_finish_phase_equals_its_rounds(mm, orc, torch_cuda, type_):
+    """A policy that ignores its features hands the late rounds to the finish
+    kernel, which plays them under the policy's threshold and the retirement
+    rule of the round kernel (a red vertex of at most 128 entries whose
+    neighbours are all matched leaves from round 3 on).  Every match value and
+    the round count must equal those of the round kernel playing every round
+    itself (finish phase off), on the symmetric graphs that take that path and
+    on a batch."""
+    import importlib
+
+    pol = importlib.import_module("multicore_matching_b200.policy")
+    seeds = orc.rand_seeds(2024, 256)
+    policies = [np.zeros(mm.POLICY_FLOATS, np.float32), pol.load_policy(), pol.constant_policy(0.7)]
+    graphs = [mm.Graph.rgg(1 << 13, 13.0, seed=21), mm.Graph.rmat(13, 16, seed=22), mm.Graph.grid(64, 48),
+              mm.Graph.er(1 << 12, 8.0, seed=23)]
+    u, off = mm.Graph.union(graphs[:3])
+    for g, batch in [(x, None) for x in graphs] + [(u, off)]:
+        with mm.DeviceGraph(g, device=0) as dg:
+            if batch is not None:
+                dg.set_batch(batch)
+            for w in policies:
+                a = torch_cuda.empty(g.n, dtype=torch_cuda.int32, device="cuda")
+                b = torch_cuda.empty(g.n, dtype=torch_cuda.int32, device="cuda")
+                dg.tune(finish_div=0)
+                ra = dg.match_policy(type_, seeds, a.data_ptr(), w, 1.0)
+                dg.tune(finish_div=-1)
+                rb = dg.match_policy(type_, seeds, b.data_ptr(), w, 1.0)
+                ma, mb = a.cpu().numpy(), b.cpu().numpy()
+                assert ra == rb and np.array_equal(ma, mb), (g.name, type_, ra, rb, int((ma != mb).sum()))
+                if batch is None:
+                    chk = orc.check(g, ma)
+                    assert chk["valid"] and (type_ in (6, 8) or chk["matchable"] == 0), (g.name, chk)
