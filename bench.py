@@ -524,6 +524,12 @@ def main():
     peak, peak_kind = load_peaks()
     # the scans are bound by random single-sector reads: their measured ceiling on this device
     gather_peak = mm.probe_gather_rate(local, max(g.n, 1))
+    # the same random one-byte gathers over a 1 GiB table: most miss L2 (and the
+    # TLB's reach), the regime of the window reads and the commit's key reads
+    try:
+        gather_dram = mm.probe_gather_rate(local, 1 << 30)
+    except mm.MatchError:
+        gather_dram = None
     colour_gathers = float(st[:, mm.ST_WINDOW_ENTRIES].sum() + st[:, mm.ST_STAGED_DEG].sum())
     # DRAM bytes of one matching's launches from an ncu capture of this workload, where one exists
     traffic = None
@@ -646,6 +652,7 @@ def main():
                                           "fallback": [round(float(x), 4) for x in ms_k[:, 1]],
                                           "commit": [round(float(x), 4) for x in ms_k[:, 2]]},
                          "random_reads": {"ceiling_per_s": gather_peak, "ceiling": "mm_probe_gather_rate, table of n bytes",
+                                          "ceiling_1gib_per_s": gather_dram,
                                           "colour_gathers_per_step": colour_gathers,
                                           "colour_gathers_per_s": colour_gathers / (ms / 1e3)}},
             "gpu_launches": gpu_launches,

@@ -581,13 +581,14 @@ __device__ __forceinline__ void compact_tile(const Params &p, Smem &sm, int pari
 // to the cap (match value 1).  The set-up queues the ones red in round 0 in
 // shared memory and resolves the queue round by round, a hash per queued
 // vertex and round (a walk per thread would cost every lane its warp's longest
-// walk).  iso_last: the last round in which any of them is active (the cap's
+// walk); a vertex that finds the queue full stays in the rounds, which give it
+// the same fate.  iso_last: the last round in which any of them is active (the cap's
 // last round if one stays red to it, nseeds if the seeds run out first: the
 // reference would draw more, and the round count then exceeds nseeds).
 constexpr int kIsoHalf = (int)(sizeof(LongStage) * kWarps / sizeof(int) / 2);  // queue capacity (two halves)
-constexpr int kIsoFlush = kIsoHalf - kTileItems;  // resolve once a tile could overflow the queue
 
-// Called by the whole block, after a barrier that follows the last append.
+// Called by the whole block once, after the set-up's last tile (whose
+// compaction ends with a barrier, after the last append).
 // Round r reads the queue half qa and appends its survivors to the other,
 // counting them in iso_cnt[r % 3]: that counter is cleared by thread 0 in
 // round r - 1, after every thread read it (in round r - 3's closing step) and
@@ -598,7 +599,7 @@ __device__ void resolve_isolated(const Params &p, Smem &sm, int &iso_last)
     int *qa = reinterpret_cast<int *>(&sm.stage[0]), *qb = qa + kIsoHalf;
     const int cap = ctl->cap, lim = min(cap, ctl->nseeds);
     const uint32_t barrier = ctl->barrier;
-    int nq = sm.iso_n;
+    int nq = min(sm.iso_n, kIsoHalf);
     if (threadIdx.x == 0) sm.iso_cnt[1] = 0;
     __syncthreads();
     for (int r = 1; nq > 0; ++r) {
@@ -675,6 +676,7 @@ __device__ void init_phase(const Params &p, Smem &sm)
             const int v = item[k].x;
             dest[k] = -1;
             if (v < n) {
+                int slot;
                 const int deg = degree_of(item[k]);
                 const float2 wf = kPolicy && policy_needs_features(p, 0) ? __ldg(p.wfeat + v) : make_float2(0.0f, 0.0f);
                 const bool blue = colour_blue<kPolicy>(p, v, deg, 0.0f, wf, 0, seed, barrier);
@@ -694,10 +696,12 @@ __device__ void init_phase(const Params &p, Smem &sm)
                     p.col[v] = kDead;
                     p.ctl->match[v] = 2;
                     trace_left<kPolicy>(p, 0, v);
-                } else if (!kPolicy && !kStats && p.sym && deg == 0) {
-                    // red in round 0: queued, resolved with the block's others
+                } else if (!kPolicy && !kStats && p.sym && deg == 0 &&
+                           (slot = atomicAdd(&sm.iso_n, 1)) < kIsoHalf) {
+                    // red in round 0: queued, resolved with the block's others (a
+                    // vertex that finds the queue full stays in the rounds)
                     p.col[v] = kDead;
-                    reinterpret_cast<int *>(&sm.stage[0])[atomicAdd(&sm.iso_n, 1)] = v;
+                    reinterpret_cast<int *>(&sm.stage[0])[slot] = v;
                 } else {
                     p.col[v] = blue ? kBlue : kRed;
                     dest[k] = blue ? kBlue : kRed;
@@ -710,13 +714,6 @@ __device__ void init_phase(const Params &p, Smem &sm)
             stat_add(p, 0, MM_ST_RED, act - blue_n);
         }
         compact_tile(p, sm, 0, dest, item);
-        if (!kPolicy && !kStats && p.sym) {
-            // the tile's appends are complete (compact_tile's barriers); every
-            // thread reads the queue length before any appends for the next tile
-            const int qn = sm.iso_n;
-            __syncthreads();
-            if (qn > kIsoFlush) resolve_isolated(p, sm, iso_last);
-        }
     }
     if (!kPolicy && !kStats) {
         if (sm.iso_n > 0) resolve_isolated(p, sm, iso_last);
@@ -2931,6 +2928,13 @@ mm_status launch_rounds(mm_graph *g, PushState *s, bool timing, cudaStream_t str
         prm.trace_rounds = pol->trace_rounds;
         // the finish phase knows the policy's threshold, not its features
         prm.fin_retire = pol->constant && !pol->trace ? 1 : 0;
+        // Retirement shrinks the active set from round kRetireFrom on, so the
+        // default threshold comes a round or two earlier than on the plain
+        // path, while components are still too large for the finish phase (on
+        // the R-MAT 2^22 hierarchy every level but the first called its attempt
+        // off, and the round kernel then played all the remaining rounds): the
+        // default divisor is doubled here.
+        if (g->opt_fin_div == 0) prm.fin_div = 2 * kFinDiv;
     }
     void *args[] = {&prm};
     const int mode = kPolicy ? 2 : (kStats ? 1 : 0);

@@ -1,8 +1,8 @@
 """Autotuner for the launch options of the matching kernels (mm_graph_tune).
 
-The kernels' shapes inside a launch (window length 32, window steps of 2 then 4
-entries, 256-entry fallback segments, two vertices per thread, 512 threads)
-were fixed by measurement.  What varies with the workload is where the round
+The kernels' shapes inside a launch (window length 32, window steps of 8
+entries, a lane per vertex refilled from 64-item chunks, 256-entry fallback
+segments, 512 threads) were fixed by measurement.  What varies with the workload is where the round
 kernel hands over to the finish phase (the first round whose active set is at
 most 1/d of round 0's: too early and components are too large, so the attempt
 is called off and its scans are wasted; too late and the grid pays for more
