@@ -169,8 +169,9 @@ mm_status mm_match_drawn(mm_graph *g, int type, uint32_t barrier, uint32_t (*dra
  * restores the default.  The result never depends on them, only the time.
  *   MM_TUNE_FINISH_DIV     the finish phase (the late rounds played component by
  *                          component) starts at the first round whose active set
- *                          is at most 1/value of round 0's; default 12, at least
- *                          2, -1 never
+ *                          is at most 1/value of round 0's; default 12 (24 for
+ *                          mm_match_policy, whose retirement shrinks the active
+ *                          set sooner), at least 2, -1 never
  *   MM_TUNE_BLOCKS_PER_SM  blocks of 512 threads per multiprocessor for the round
  *                          and finish kernels; default all that fit (2)
  */

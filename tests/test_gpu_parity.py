@@ -270,6 +270,33 @@ def test_edge_cases(mm, orc, torch_cuda):
         assert rounds == (255 if t in (7, 9) else 20)
 
 
+def test_isolated_vertices_beside_a_graph(mm, orc, torch_cuda):
+    """Vertices without neighbours (resolved at set-up on the symmetric path, a hash
+    per vertex and round): 2^20 of them after a random geometric graph, with
+    barriers that keep them red for a few rounds, for dozens, and to the cap; and
+    seed sequences one short of the rounds the reference draws, which must be an
+    error, or exactly enough."""
+    seeds = orc.rand_seeds(3, 256)
+    base = mm.Graph.rgg(1 << 12, 13.0, seed=3)
+    extra = 1 << 20
+    r = np.concatenate([np.asarray(base.ranges, np.int64),
+                        np.full((extra, 2), base.nnz, np.int64)]).astype(np.int32)
+    g = mm.Graph(base.n + extra, r, base.nbrs, base.weights, "rgg-and-isolated")
+    with mm.DeviceGraph(g, device=0) as dg:
+        for barrier in (BARRIER, 0x10000000, 0x01000000):
+            for t in mm.TYPES:
+                want, rounds, _ = orc.match(g, t, seeds, barrier)
+                got, rr = gpu_match(mm, torch_cuda, g, t, seeds, barrier=barrier, dg=dg)
+                assert rr == rounds and np.array_equal(got, want), (hex(barrier), t, rr, rounds)
+        want, rounds, _ = orc.match(g, 7, seeds, 0x10000000)
+        assert rounds < 255
+        with pytest.raises(mm.MatchError) as e:
+            dg.match(7, seeds[: rounds - 1], barrier=0x10000000)
+        assert e.value.status == 6
+        got, rr = dg.match(7, seeds[:rounds], barrier=0x10000000)
+        assert rr == rounds and np.array_equal(got, want)
+
+
 def test_errors_are_statuses(mm, orc, torch_cuda):
     seeds = orc.rand_seeds(1, 256)
     bad_id = SmallGraph(3, np.array([[0, 2], [2, 3], [3, 3]]), np.array([1, 5, 0]), None)
