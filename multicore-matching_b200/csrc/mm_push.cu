@@ -126,6 +126,7 @@ struct Params {
     unsigned long long *tstamp;     // [3 * kMaxRounds + 1] barrier times (ns) or null
     unsigned *bar;                  // [kBarWords] grid barrier words, zero at launch
     int resume;                     // round kernel: continue from ctl->fin_round (finish called off)
+    int zero_parts;                 // set-up clears part_key and part_cnt (not known to be zero)
     int fin_div;                    // finish phase from the round whose active set is <= 1/fin_div of round 0's (0: never)
     // testing hooks (mm_debug): polls before a barrier wait gives up, and the
     // mark of a barrier at which block 0 does not arrive (-1: none)
@@ -682,7 +683,8 @@ __device__ void init_phase(const Params &p, Smem &sm)
                 const bool blue = colour_blue<kPolicy>(p, v, deg, 0.0f, wf, 0, seed, barrier);
                 if (p.last) p.last[v] = 0;
                 p.best[v] = 0ull;
-                if (deg > kWin) {
+                // (every completed round leaves them zero: a cut list's last piece clears them)
+                if (deg > kWin && p.zero_parts) {
                     p.part_key[v] = 0ull;
                     p.part_cnt[v] = 0;
                 }
@@ -2719,6 +2721,11 @@ struct PushState {
     int grid[2][3] = {{0, 0, 0}, {0, 0, 0}};  // co-resident blocks of k_rounds by weighting and mode
     int fgrid[2][2] = {{0, 0}, {0, 0}};       // co-resident blocks of k_finish by weighting and stats
     int sms = 0;                              // multiprocessors of the device
+    // The last call on this state ended with every grid barrier complete (the
+    // barrier words are back at rest) and every fallback list combined (part_key
+    // and part_cnt all zero); false after a call that gave up or failed.
+    bool at_rest = false;
+    bool zero_next = true;  // the call being launched resets them (the last one did not end at rest)
     float2 *wfeat = nullptr;              // learned colouring: (max, mean) incident weight per vertex
 };
 
@@ -2802,6 +2809,8 @@ mm_status alloc_state(mm_graph *g, PushState **out)
     // two sets of barrier words: the round kernel's and the finish kernel's
     if (e == cudaSuccess) e = dev_alloc((void **)&s->bar, sizeof(unsigned) * 2 * kBarWords, 0);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->bar, 0, sizeof(unsigned) * 2 * kBarWords, 0);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->part_key, 0, n * sizeof(unsigned long long), 0);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->part_cnt, 0, n * sizeof(int), 0);
     if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) {
         cudaDeviceSynchronize();
@@ -2855,6 +2864,7 @@ mm_status alloc_state(mm_graph *g, PushState **out)
         set_error("push: the device cannot run the cooperative round kernel");
         return MM_ERR_UNSUPPORTED;
     }
+    s->at_rest = true;
     *out = s;
     return MM_OK;
 }
@@ -2899,6 +2909,7 @@ Params make_params(mm_graph *g, PushState *s, bool weighted, bool stats, bool ti
     p.tstamp = timing ? s->tstamp : nullptr;
     p.bar = s->bar;
     p.resume = 0;
+    p.zero_parts = s->zero_next ? 1 : 0;
     // at least 2: the finish phase's records take 4 slots an item in 2n
     p.fin_div = g->opt_fin_div < 0 ? 0 : (g->opt_fin_div == 0 ? kFinDiv : max(g->opt_fin_div, 2));
     p.spin_limit = debug_spin_limit();
@@ -2979,6 +2990,12 @@ mm_status begin_call(mm_graph *g, int type, uint32_t barrier, const uint32_t *se
     }
     // One pinned upload of control block + seeds.  The previous call on this
     // graph synchronised its stream before returning, so the staging buffer is free.
+    // the barrier words: reset only after a call that did not end at rest; until
+    // this call ends well, the state counts as not at rest
+    s->zero_next = !s->at_rest;
+    s->at_rest = false;
+    if (s->zero_next)
+        MM_CUDA_TRY(cudaMemsetAsync(s->bar, 0, sizeof(unsigned) * 2 * kBarWords, stream), "barrier clear");
     Ctl *ctl = reinterpret_cast<Ctl *>(s->host_stage);
     std::memset(ctl, 0, kCtlBytes);
     ctl->match = d_match;
@@ -3011,6 +3028,8 @@ mm_status end_call(mm_graph *g, PushState *s, int nseeds, int *rounds_out, long 
     MM_CUDA_TRY(cudaStreamSynchronize(stream), "round loop");
     Ctl out;
     std::memcpy(&out, s->host_back, sizeof out);
+    // every barrier completed unless one gave up (status 2)
+    s->at_rest = out.status != 2;
     if (out.status == 2) {
         set_error("mm_match: a bounded grid-barrier wait in the round kernel gave up");
         return MM_ERR_DEVICE;
@@ -3026,7 +3045,6 @@ mm_status end_call(mm_graph *g, PushState *s, int nseeds, int *rounds_out, long 
 mm_status run_rounds(mm_graph *g, PushState *s, int type, bool stats, bool timing, cudaStream_t stream)
 {
     const bool w = is_weighted(type);
-    MM_CUDA_TRY(cudaMemsetAsync(s->bar, 0, sizeof(unsigned) * 2 * kBarWords, stream), "barrier clear");
     if (stats)
         MM_CUDA_TRY(cudaMemsetAsync(s->stats, 0, sizeof(unsigned long long) * kMaxRounds * MM_STATS_COLS, stream),
                     "stats clear");
@@ -3419,7 +3437,6 @@ mm_status push_match_policy(mm_graph *g, int type, uint32_t barrier, const uint3
         }
         if (e != cudaSuccess) return cuda_fail(e, "policy state");
     }
-    MM_CUDA_TRY(cudaMemsetAsync(s->bar, 0, sizeof(unsigned) * 2 * kBarWords, stream), "barrier clear");
     PolicyArgs pol;
     pol.mlp = mlp_host;
     // the output layer's weights W2 (after W1 and b1): all zero means every
