@@ -26,29 +26,33 @@
 //     either way, so their outcome is unchanged.
 //
 // Work layout.  Vertices that can still be matched sit in worklists; an item
-// carries the vertex and its neighbour range, so the scans never read
-// neighbourRanges again.
-//   short lists (deg <= 32)   a warp takes 32 blue vertices and walks their
-//                             concatenated entries row by row, 32 consecutive
-//                             entries per load (scan_short)
-//   long lists  (deg  > 32)   blue ones are appended with their offset in the
-//                             round's concatenated long-list entry space; that
-//                             space is cut into 512-entry segments and a warp
-//                             walks one segment row by row (scan_long).
-//                             A list cut by segment edges is combined by
-//                             atomics and its last piece proposes.  Every warp
-//                             gets equal amounts of work whatever the skew.
-// Every load of neighbour ids and weights is a coalesced row of 32 consecutive
-// entries.  A list's best entry is kept as a 64-bit key (weight order << 32 |
-// ~position) max-combined in shared memory, which orders ties by position
-// exactly as the reference's strict ">" scan in list order does.
+// carries the vertex, its neighbour range and its window offset, so the scans
+// never read neighbourRanges again.
+//   windows        a blue vertex's choice is the first red candidate among its
+//                  best min(deg, 32) entries in order of preference (weight,
+//                  then position; list order for random types), stored at
+//                  preparation.  A lane holds one vertex and reads eight
+//                  window entries a step, refilled from a prefetched item as
+//                  soon as its vertex is decided (scan_window).
+//   fallback       a list longer than its window with no red candidate in it
+//                  is appended to the round's fallback list; that entry space
+//                  is cut into 256-entry segments and a warp walks one segment
+//                  in coalesced rows of 32 (scan_long).  A list cut by segment
+//                  edges is combined by atomics and its last piece proposes.
+//   finish phase   once the active set is small its components are tiny, and
+//                  a second cooperative kernel plays the remaining rounds of
+//                  each component on its own (k_finish), with no grid barrier.
+// A list's best entry is kept as a 64-bit key (weight order << 32 | ~position),
+// which orders ties by position exactly as the reference's strict ">" scan in
+// list order does.
 //
 // Loop.  k_rounds is launched cooperatively (all blocks resident) and runs
-// set-up, then per round the scan phase (A: blue scans + proposals) and the
-// commit phase (B: commit + recolour + worklist compaction), with bounded grid
-// barriers in between.  Nothing returns to the host until the matching is
-// maximal (the reference copies a flag back every round, matchgpu.cu:607-614),
-// and no round pays for kernel launches.
+// set-up, then per round the window scan (A1), the fallback scan (A2, only in
+// rounds that have fallback lists) and the commit phase (B: commit + recolour
+// + worklist compaction), with bounded grid barriers in between, until it
+// hands over to the finish kernel.  Nothing returns to the host until the
+// matching is maximal (the reference copies a flag back every round,
+// matchgpu.cu:607-614), and no round pays for kernel launches.
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
