@@ -280,8 +280,12 @@ def finish_model(n, ranges, nbrs, w, weighted, maximal, cap, seeds, barrier, col
     return min(last_all + 2, cap) if maximal else cap
 
 
-def push_match(g, type_, seeds, barrier, colour_hash, finish=None):
-    """finish: None, or the finish phase's limits {div, members, entries, maxdeg}."""
+def push_match(g, type_, seeds, barrier, colour_hash, finish=None, isolated=False):
+    """finish: None, or the finish phase's limits {div, members, entries, maxdeg}.
+    isolated: on the symmetric path, resolve the vertices without neighbours at
+    set-up, as the round kernel does (each leaves in the first round in which it
+    is blue, or stays red to the cap; the last round in which one is active
+    joins the round count), instead of carrying them through the rounds."""
     n = g.n
     ranges = np.asarray(g.ranges)
     nbrs = np.asarray(g.nbrs)
@@ -297,7 +301,30 @@ def push_match(g, type_, seeds, barrier, colour_hash, finish=None):
     best = [0] * n
     rounds = None
     t = 0
-    sym = finish is not None and is_symmetric(n, ranges, nbrs, w, weighted)
+    symmetric = is_symmetric(n, ranges, nbrs, w, weighted)
+    sym = finish is not None and symmetric
+    iso_last = -1
+    if isolated and symmetric:
+        lim = min(cap, len(seeds))
+        keep = []
+        for v in active:
+            if int(ranges[v, 1]) > int(ranges[v, 0]):
+                keep.append(v)
+                continue
+            r, blue = 0, col[v] == BLUE
+            while not blue and r + 1 < lim:
+                r += 1
+                blue = colour_hash(v, int(seeds[r])) < barrier
+            if blue:
+                match[v], last = 2, r
+            else:
+                match[v], last = 1, (cap - 1 if lim == cap else lim)
+            iso_last = max(iso_last, last)
+        active = keep
+
+    def with_isolated(r):
+        return max(r, min(iso_last + 2, cap)) if maximal and iso_last >= 0 else r
+
     act0 = len(active)
     fin_next = act0
     while True:
@@ -308,7 +335,7 @@ def push_match(g, type_, seeds, barrier, colour_hash, finish=None):
                 out = np.zeros(n, np.int32)
                 for v in range(n):
                     out[v] = match[v] if match[v] is not None else col[v]
-                return out, r
+                return out, with_isolated(r)
             fin_next = len(active) // 2
         # phase A: blue vertices scan and propose
         req = {}
@@ -371,4 +398,4 @@ def push_match(g, type_, seeds, barrier, colour_hash, finish=None):
     out = np.zeros(n, np.int32)
     for v in range(n):
         out[v] = match[v] if match[v] is not None else col[v]
-    return out, rounds
+    return out, with_isolated(rounds)

@@ -118,3 +118,30 @@ def test_finish_phase_model_equals_oracle(orc):
     finally:
         push_model.finish_model = model
     assert outcomes["done"] > 100 and outcomes["off"] > 100, outcomes
+
+
+def test_isolated_vertices_at_set_up_equal_oracle(orc):
+    """Resolving the vertices without neighbours at set-up (the round kernel's
+    rule on the symmetric path) gives the oracle's match values and round count:
+    sparse symmetric graphs with many isolated vertices, barriers that keep
+    vertices red for long (to the cap of the maximal loop), with and without the
+    finish phase."""
+    import push_model
+
+    rng = np.random.default_rng(31)
+    fin = dict(div=4, members=6, entries=16, maxdeg=12)
+    checked = 0
+    for it in range(40):
+        n = int(rng.integers(1, 60))
+        g = symmetric_graph(rng, n, float(rng.uniform(0.0, 1.5)))
+        assert push_model.is_symmetric(g.n, g.ranges, g.nbrs, g.weights, True)
+        seeds = orc.rand_seeds(int(rng.integers(1, 1000)))
+        for barrier in (0x88B81733, 0x20000000, 0x02000000):
+            for t in (6, 7, 8, 9):
+                want, rounds, _ = orc.match(g, t, seeds, barrier)
+                for f in (None, fin):
+                    got, got_rounds = push_match(g, t, seeds, barrier, orc.colour_hash, finish=f, isolated=True)
+                    assert got_rounds == rounds, (it, t, hex(barrier), f is None)
+                    assert np.array_equal(got, want), (it, t, hex(barrier), f is None)
+                    checked += 1
+    assert checked == 40 * 3 * 4 * 2
