@@ -6,8 +6,10 @@
 #include <cstring>
 #include <exception>
 #include <iostream>
+#include <vector>
 
 #include "mm_match.h"
+#include "mtc/matchcpu.h"
 #include "mtc/matchgpu.h"
 
 using namespace std;
@@ -49,6 +51,53 @@ bool read_ahead_allowed()
 {
     const char *e = std::getenv("MTC_RAND_READ_AHEAD");
     return !(e && e[0] == '0');
+}
+
+// The reference's MATCH_INTERMEDIATE_COUNT switch (src/matchcpu.h:26, used by
+// saturate.sh): its fixed-round GPU matchers print the matching's weight and
+// size after every round (src/matchgpu.cu:503-523, 701-712), "round<TAB>weight
+// <TAB>size" on standard output, starting with "0<TAB>0<TAB>0".  The same
+// switch at compile time, or MTC_MATCH_INTERMEDIATE_COUNT=1 at run time (the
+// library is built once), gives the same lines here.
+bool intermediate_count()
+{
+#ifdef MATCH_INTERMEDIATE_COUNT
+    return true;
+#else
+    const char *e = std::getenv("MTC_MATCH_INTERMEDIATE_COUNT");
+    return e && e[0] == '1';
+#endif
+}
+
+// Between rounds of the host-stepped matching (mm_match_drawn calls `draw` as
+// each round starts): the rounds done so far, their match values copied back.
+struct RoundCounts {
+    const mtc::Graph *graph;
+    const int *dmatch;
+    std::vector<int> *match;
+    int done;
+};
+
+void print_counts(RoundCounts &rc)
+{
+    if (cudaDeviceSynchronize() != cudaSuccess ||
+        (rc.graph->nrVertices > 0 && cudaMemcpy(&(*rc.match)[0], rc.dmatch, sizeof(int) * (size_t)rc.graph->nrVertices,
+                                                cudaMemcpyDeviceToHost) != cudaSuccess)) {
+        cerr << "Unable to retrieve data!" << endl;
+        throw exception();
+    }
+    double weight = 0;
+    long size = 0;
+    mtc::GraphMatching::getWeight(weight, size, *rc.match, *rc.graph);
+    cout << rc.done << "\t" << weight << "\t" << size << endl;
+}
+
+uint32_t draw_and_count(void *ctx)
+{
+    RoundCounts &rc = *(RoundCounts *)ctx;
+    if (rc.done > 0) print_counts(rc);  // after the previous round
+    ++rc.done;
+    return (uint32_t)rand();
 }
 
 [[noreturn]] void fail(const char *what)
@@ -109,6 +158,21 @@ void GraphMatchingGPU::runMatching(vector<int> &match, cudaEvent_t &t1, cudaEven
 {
     assert((int)match.size() == graph.nrVertices);
     const int cap = mm_max_rounds(type);
+    if (cap == NR_MATCH_ROUNDS && intermediate_count()) {
+        // the rounds one at a time, the counts printed between them (the
+        // reference prints inside its timed region too)
+        cudaEventRecord(t1, 0);
+        cudaEventSynchronize(t1);
+        cout << "0\t0\t0" << endl;
+        RoundCounts rc{&graph, dmatch, &match, 0};
+        int rounds = 0;
+        if (mm_match_drawn(dgraph, type, selectBarrier, draw_and_count, &rc, dmatch, &rounds, nullptr) != MM_OK)
+            fail("A CUDA error occurred during the matching process");
+        print_counts(rc);  // the last round; match now holds the result
+        cudaEventRecord(t2, 0);
+        cudaEventSynchronize(t2);
+        return;
+    }
     uint32_t seeds[256];
     if (!read_ahead_allowed() || !peek_rand(seeds, cap)) {
         // rand()'s state could not be read ahead (another C library, say): the

@@ -281,3 +281,34 @@ def test_cli_loop_matrix_market_and_empty(mm, orc, harness, tmp_path):
     p = run(harness, "match", path, 7, 1, 0, 1, out)
     res = json.loads(p.stdout)
     assert res["runs"][0]["valid"] and res["runs"][0]["size"] == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not has_gpu(), reason="needs a GPU")
+@pytest.mark.parametrize("gtype", [6, 8])
+def test_intermediate_counts(mm, orc, harness, tmp_path, gtype):
+    """MTC_MATCH_INTERMEDIATE_COUNT=1 (the reference's MATCH_INTERMEDIATE_COUNT
+    switch): the fixed-round matchers print "round, weight, size" after every
+    round, from "0 0 0" to round 20.  The sizes are the oracle's matched counts
+    summed over the rounds so far, the weights never decrease, the last line is
+    the final matching's, and the matching itself is unchanged."""
+    g = mm.Graph.rgg(6000, 10.0, seed=21)
+    path = tmp_path / "g.graph"
+    write_metis(path, g, True)
+    out = tmp_path / "m.bin"
+    p = run(harness, "match", path, gtype, 12345, 0, 1, out, env={"MTC_MATCH_INTERMEDIATE_COUNT": "1"})
+    lines = p.stdout.strip().split("\n")
+    res = json.loads(lines[-1])
+    rows = [line.split("\t") for line in lines[:-1]]
+    assert [int(r[0]) for r in rows] == list(range(21))
+    assert rows[0] == ["0", "0", "0"]
+    weights, sizes = [float(r[1]) for r in rows], [int(r[2]) for r in rows]
+    seeds = orc.rand_seeds(12345, 256)
+    want, rounds, stats = orc.match(g, gtype, seeds, BARRIER)
+    assert rounds == 20
+    assert sizes == [0] + [int(x) for x in np.cumsum(stats[:, 7])]
+    assert all(b >= a for a, b in zip(weights, weights[1:]))
+    assert sizes[-1] == res["runs"][0]["size"]
+    assert abs(weights[-1] - res["runs"][0]["weight"]) <= 1e-5 * res["runs"][0]["weight"]
+    np.testing.assert_array_equal(np.fromfile(out, dtype=np.int32), want)
+    assert res["next_rand"] == int(seeds[20])
