@@ -61,7 +61,7 @@ enum {
 enum {
     MM_PATH_AUTO = 0,
     MM_PATH_PULL = 1,  /* reference-structured select/request/respond/commit kernels */
-    MM_PATH_PUSH = 2   /* reverse-index proposals, device-resident round loop */
+    MM_PATH_PUSH = 2   /* worklists, preference windows and proposals; device-resident round loop */
 };
 
 /* Number of int64 counters per round written by mm_match_stats. */
@@ -98,9 +98,12 @@ mm_status mm_graph_create_device(int n, const int *d_ranges, long long nnz, cons
                                  const float *d_weights, mm_graph **out);
 
 /*
- * Build the per-type device structures a matching type needs (the reverse
- * proposal index of the push path) ahead of the first mm_match call, so that
- * their cost lands in set-up rather than in the timed round loop.  Optional.
+ * Build the per-type device structures a matching type needs ahead of the
+ * first mm_match call (the push path's preference windows for the weighted
+ * types, and its reverse proposal keys off the symmetric path, i.e. unless
+ * the lists are contiguous and sorted and every entry has a reverse entry of
+ * the same weight), so that their cost lands in set-up rather than in the
+ * timed round loop.  Optional.
  */
 mm_status mm_graph_prepare(mm_graph *g, int type);
 
@@ -192,16 +195,21 @@ mm_status mm_match_stats(mm_graph *g, int type, uint32_t barrier, const uint32_t
                          int stats_rounds, int path, void *stream);
 
 /*
- * Measurement entry: the same single launch of the round kernel as
- * mm_match_device, with timestamps taken by the kernel as its grid barriers
- * complete (the device's global timer, nanoseconds).
+ * Measurement entry: the same launches as mm_match_device, with timestamps
+ * taken by the kernels as their grid barriers complete (the device's global
+ * timer, nanoseconds).
  * ms_per_kernel[r * MM_PROFILE_KERNELS + k] receives, for each round r <
  * cap_rounds that the kernel executed, k = 0 the window scan (blue vertices'
  * preference windows and proposals), k = 1 the fallback scan of lists longer
  * than their window (0 in rounds without one), k = 2 the commit phase
  * (commit, recolour, worklist compaction), k = 3 their sum; rows of rounds
- * not executed are zero.  *launches receives the number of kernels launched
- * (1).  Same matching result.
+ * not executed are zero; the finish kernel's work is reported in the row of
+ * the round it took over at, its scan pass as k = 0 and the rest as k = 1.
+ * *launches receives the number of kernels launched: 3 on the symmetric path
+ * (contiguous sorted lists, every entry with a reverse entry of the same
+ * weight): the round kernel, the finish kernel and the round kernel again,
+ * each returning at once when nothing is left for it; else 1.  Same matching
+ * result.
  */
 #define MM_PROFILE_KERNELS 4
 mm_status mm_match_profile(mm_graph *g, int type, uint32_t barrier, const uint32_t *seeds, int nseeds,
