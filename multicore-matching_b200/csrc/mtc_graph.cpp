@@ -278,7 +278,11 @@ vector<int> Graph::random_shuffle()
 {
     vector<int> perm(nrVertices);
     for (int i = 0; i < nrVertices; ++i) perm[i] = i;
+    // deprecated since C++14, but the only shuffle whose draws are rand()'s
+#pragma GCC diagnostic push
+#pragma GCC diagnostic ignored "-Wdeprecated-declarations"
     std::random_shuffle(perm.begin(), perm.end());
+#pragma GCC diagnostic pop
     vector<int2> moved(nrVertices);
     for (int i = 0; i < nrVertices; ++i) moved[i] = neighbourRanges[perm[i]];
     neighbourRanges = moved;
