@@ -67,6 +67,16 @@ def tune(mm, dg, type_, seeds, batch=False, fin_divs=FIN_DIVS, blocks=BLOCKS, re
     return rows, min(rows, key=lambda x: x["ms"])
 
 
+def pick(rows, default=DEFAULT, margin=0.03):
+    """The choice for a workload class from tune()'s rows: the fastest pair if it
+    beats the library's default by more than `margin` (a fraction of the
+    default's time), else the default.  Returns (choice row, default row, tuned?)."""
+    dflt = next(r for r in rows if (r["finish_div"], r["blocks_per_sm"]) == tuple(default))
+    best = min(rows, key=lambda x: x["ms"])
+    wins = best["ms"] < (1.0 - margin) * dflt["ms"]
+    return (best if wins else dflt), dflt, wins
+
+
 def workloads(mm):
     """The workload classes: name -> (graph factory, type, batch offsets or None)."""
     sys.path.insert(0, str(ROOT))
@@ -114,9 +124,8 @@ def main():
             dg.prepare(type_)
             rows, best = tune(mm, dg, type_, seeds, batch=off is not None)
         assert all(r["same"] for r in rows), name
-        dflt = next(r for r in rows if (r["finish_div"], r["blocks_per_sm"]) == DEFAULT)
-        wins = best["ms"] < 0.97 * dflt["ms"]  # keep the default unless the tuned choice is clearly faster
-        choice = best if wins else dflt
+        # keep the default unless the tuned choice is clearly faster
+        choice, dflt, wins = pick(rows)
         tuned[name] = {"finish_div": choice["finish_div"], "blocks_per_sm": choice["blocks_per_sm"],
                        "ms": choice["ms"], "default_ms": dflt["ms"], "type": type_}
         lines += [f"## {name} (type {type_}, n = {g.n:,}, {g.nnz:,} entries)", "",
